@@ -1,0 +1,417 @@
+"""Benchmark: batched parallel-beam FBP at 2048^2 x 1800 angles.
+
+Workload (one "step"): FBP of a 512-slice volume, 2048 detector bins, 1800
+angles over [0, pi), rotation-axis offset +3.5 px, Hann filter, padding 2,
+synthetic data (50 seeded random ellipses per slice, Poisson noise at
+I0 = 1e4 photons/ray, converted to -log transmission).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours:      `value` = slices/s with the sinogram already resident in HBM
+           (raft_fbp_device), `e2e` = slices/s through the public drop-in API
+           sscRaft.fbp (-> getFBPMultiGPU) with pinned host buffers, H2D and
+           D2H inside the timed region.  Headline operator: the reference's
+           nearest-sample FBP (bit-faithful index rule), FP32.  The linear-
+           interpolation operator (FP32 and BF16 storage) is reported under
+           "variants".
+reference: the reference's own CUDA library (oracle/_ref/libraft_ref.so, built
+           from its sources for sm_100a) through its C ABI getFBPMultiGPU with
+           host buffers, on a bounded sample of the same workload.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "ssc-raft_b200"))
+
+N_RAYS, N_ANGLES, N_SLICES = 2048, 1800, 512
+OFFSET, PAD, FILTER_ID = 3.5, 2, 5          # Hann
+I0 = 1.0e4
+WORKLOAD = ("batched FBP: 512 slices x 2048^2, 1800 angles over [0,pi), 2048 bins, "
+            "axis offset +3.5 px, Hann, padding 2")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ------------------------------------------------------------------ data --
+def make_sinograms_gpu(nslices, seed_base, device):
+    """Exact ellipse projections (50 ellipses/slice) + Poisson noise, on the GPU."""
+    import torch
+    from sscRaft import synthetic as S
+    ang = S.uniform_angles(N_ANGLES)
+    th = torch.as_tensor(ang.astype(np.float64), device=device)[None, :, None]
+    R = N_RAYS / 2.0
+    c0 = (PAD * N_RAYS) // 2 - N_RAYS * (1 + PAD) / 2.0
+    t = ((torch.arange(N_RAYS, device=device, dtype=torch.float64) + c0) / R)[None, None, :]
+    cth, sth = torch.cos(th), torch.sin(th)
+    out = torch.empty((nslices, N_ANGLES, N_RAYS), dtype=torch.float32, device=device)
+    gen = torch.Generator(device=device)
+    for k in range(nslices):
+        prm = torch.as_tensor(S.ellipse_params(seed_base + k, 50), device=device)
+        x0, y0, a, b, phi, rho = [prm[:, i][:, None, None] for i in range(6)]
+        c = cth * torch.cos(phi) - sth * torch.sin(phi)
+        s = sth * torch.cos(phi) + cth * torch.sin(phi)
+        s2 = (a * c) ** 2 + (b * s) ** 2
+        tau = t - (x0 * cth - y0 * sth)
+        p = (rho * 2.0 * a * b * torch.sqrt(torch.clamp(s2 - tau * tau, min=0.0)) / s2).sum(0) * R
+        sc = 3.0 / float(p.max())
+        gen.manual_seed(seed_base + k)
+        counts = torch.poisson(I0 * torch.exp(-p * sc), generator=gen)
+        out[k] = (-torch.log(torch.clamp(counts, min=1.0) / I0)).float()
+    return out, ang
+
+
+def fbp_params(nslices, blocksize=0):
+    pi = np.array([N_RAYS, N_ANGLES, nslices, N_RAYS, PAD, 0, 0, FILTER_ID, 0, blocksize], np.int32)
+    pf = np.array([0.0, 0.0, 1.0, 0.0, 1.0, 1.0, OFFSET], np.float32)
+    return pf, pi
+
+
+# ---------------------------------------------------------------- clocks --
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            self.path = f"/tmp/raft_clocks_{os.getpid()}.csv"
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        loaded = [v for v in sm if v > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "power_w_max": max(power), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- helpers --
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("sm_max_mhz", 1965.0), "measured"
+    return 6650.0, 1965.0, "fallback"
+
+
+def gather_peak_gups(store_bytes, ops, sm_mhz, n_sm=148):
+    """Backprojection gather roofline: SMs x clock x min(smem bytes/clk / bytes
+    per update, FP32 lanes / FP32 ops per update)."""
+    per_clk = min(128.0 / store_bytes, 128.0 / ops)
+    return n_sm * sm_mhz * 1e6 * per_clk / 1e9
+
+
+def cpu_baseline(sino_host, ang):
+    """The FP32 OpenMP restatement of the same operator (oracle), on a bounded
+    sample of slices, timed on the host cores."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    oracle.build()
+    cores = os.cpu_count() or 1
+    done, t_total = 0, 0.0
+    while done < sino_host.shape[0] and (t_total < 10.0 or done == 0):
+        t0 = time.perf_counter()
+        oracle.fbp(sino_host[done:done + 1], ang, oracle.MODE_REF, FILTER_ID, PAD, offset=OFFSET, f32=True)
+        t_total += time.perf_counter() - t0
+        done += 1
+    return {"value": done / t_total, "unit": "slices/s", "cores": cores, "kind": "port",
+            "sample": f"{done} of 512 slices (2048^2 x 1800, nearest operator, FP32 OpenMP oracle port), "
+                      f"{t_total:.1f} s"}
+
+
+# -------------------------------------------------------------- our arm --
+def run_ours(args):
+    import torch
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    import sscRaft
+    from sscRaft.rafttypes import libraft, check_error, _ptr, GEOMETRY, STORE
+
+    nsl = args.slices
+    t0 = time.perf_counter()
+    sino, ang = make_sinograms_gpu(nsl, 2_000_000 + rank * nsl, dev)
+    torch.cuda.synchronize()
+    log(f"[rank {rank}] generated {nsl} sinograms in {time.perf_counter() - t0:.1f} s")
+    img = torch.empty((nsl, N_RAYS, N_RAYS), dtype=torch.float32, device=dev)
+    pf, pi = fbp_params(nsl)
+    angp = np.ascontiguousarray(ang)
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if ws == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def device_step(geometry, store):
+        st = torch.cuda.current_stream(dev).cuda_stream
+        rc = libraft.raft_fbp_device(local, ctypes.c_void_p(img.data_ptr()), ctypes.c_void_p(sino.data_ptr()),
+                                     _ptr(angp), _ptr(pf), _ptr(pi), geometry, store, ctypes.c_void_p(st))
+        if rc:
+            check_error("raft_fbp_device")
+
+    def time_device(geometry, store, K, W):
+        for _ in range(W):
+            device_step(geometry, store)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        n0 = libraft.raft_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(K):
+            device_step(geometry, store)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        launches = libraft.raft_launch_count() - n0
+        return max_over_ranks(e0.elapsed_time(e1) / K), launches
+
+    def profile_bp(geometry, store):
+        libraft.raft_profile_enable(1)
+        device_step(geometry, store)
+        torch.cuda.synchronize()
+        libraft.raft_profile_enable(0)
+        ms = (ctypes.c_double * 3)()
+        cnt = (ctypes.c_longlong * 3)()
+        libraft.raft_profile_read(ms, cnt, 3)
+        return ms[0], cnt[0], ms[1], cnt[1]
+
+    hbm_peak, sm_max, peak_kind = peaks()
+    result = {}
+    with ClockSampler(local) as clk:
+        ms_dev, launches = time_device(0, 0, args.steps, args.warmup)
+        # end-to-end through the public drop-in API with pinned host buffers
+        h_sino = torch.empty((nsl, N_ANGLES, N_RAYS), dtype=torch.float32, pin_memory=True)
+        h_sino.copy_(sino)
+        h_img = torch.empty((nsl, N_RAYS, N_RAYS), dtype=torch.float32, pin_memory=True)
+        hs, hi = h_sino.numpy(), h_img.numpy()
+        dic = {"gpu": [local], "angles[rad]": angp, "filter": "hann", "padding": PAD,
+               "rotation axis offset": OFFSET}
+        for _ in range(args.warmup):
+            sscRaft.fbp(hs, dic=dict(dic), obj=hi)
+        barrier()
+        t_e2e = []
+        for _ in range(args.steps):
+            t1 = time.perf_counter()
+            sscRaft.fbp(hs, dic=dict(dic), obj=hi)
+            t_e2e.append(time.perf_counter() - t1)
+        barrier()
+        ms_e2e = max_over_ranks(1e3 * sum(t_e2e) / len(t_e2e))
+        # parity spot check of the e2e output against the device-path output
+        spot = float((torch.from_numpy(hi[nsl // 2]).to(dev) - img[nsl // 2]).abs().max())
+        variants = {}
+        for name, g, s in (("linear_fp32", 1, 1), ("linear_bf16", 1, 2)):
+            ms_v, _ = time_device(g, s, max(1, args.steps), max(3, args.warmup))
+            variants[name] = {"value": ws * nsl / (ms_v / 1e3), "ms_per_step": ms_v}
+    clocks = clk.summary()
+
+    # dominant kernel: the backprojector; one profiled pass of the headline operator
+    f_ms, f_n, bp_ms, bp_n = profile_bp(0, 0)
+    chunk = min(nsl, 32)
+    upd_per_launch = chunk * N_RAYS * N_RAYS * N_ANGLES
+    bp_avg_s = bp_ms / bp_n / 1e3
+    # algorithmic bytes per launch: the filtered detector bins the image can
+    # reach (ceil(sqrt(2) N) per angle, 4 B) read once + the image written once
+    reach = int(math.ceil(math.sqrt(2) * N_RAYS))
+    alg_bytes = chunk * N_ANGLES * reach * 4 + chunk * N_RAYS * N_RAYS * 4
+    sm_mhz = (clocks or {}).get("sm_mhz") or sm_max
+    gups_bp = upd_per_launch / bp_avg_s / 1e9
+    peak_gups = gather_peak_gups(4, 4, sm_mhz)
+    for name, (g, s, bytes_upd, ops) in (("linear_fp32", (1, 1, 8, 5)), ("linear_bf16", (1, 2, 4, 7))):
+        _, _, vms, vn = profile_bp(g, s)
+        vg = upd_per_launch / (vms / vn / 1e3) / 1e9
+        pk = gather_peak_gups(bytes_upd, ops, sm_mhz)
+        variants[name].update({"bp_gups": vg, "gather_roofline": {"achieved_gups": vg, "peak_gups": pk,
+                                                                   "frac": vg / pk}})
+
+    if rank == 0:
+        value = ws * nsl / (ms_dev / 1e3)
+        updates_step = nsl * N_RAYS * N_RAYS * N_ANGLES
+        result = {
+            "metric": "FBP slices/s at 2048^2 x 1800 angles",
+            "value": value,
+            "unit": "slices/s",
+            "n_gpus": ws,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_dev,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic: 50 seeded random ellipses per slice, exact projections, Poisson I0=1e4, "
+                    "-log transmission (no public dataset exists for this path)",
+            "config": {"workload": WORKLOAD, "operator": "nearest-sample (reference rule), FP32",
+                       "slices_per_gpu": nsl, "parallelism": f"slab x{ws}, no collective",
+                       "l2": "inputs 7.5 GB/GPU > 126 MB L2: no flush needed"},
+            "gups": ws * updates_step / (ms_dev / 1e3) / 1e9,
+            "e2e": {"value": ws * nsl / (ms_e2e / 1e3), "unit": "slices/s", "ms_per_step": ms_e2e,
+                    "api": "sscRaft.fbp -> getFBPMultiGPU, pinned host buffers",
+                    "h2d_bytes_per_step": nsl * N_ANGLES * N_RAYS * 4,
+                    "d2h_bytes_per_step": nsl * N_RAYS * N_RAYS * 4,
+                    "max_abs_diff_vs_device_path": spot},
+            "roofline": {"bound": "hbm", "achieved": alg_bytes / bp_avg_s / 1e9, "peak": hbm_peak,
+                         "unit": "GB/s", "frac": alg_bytes / bp_avg_s / 1e9 / hbm_peak, "traffic": None,
+                         "kernel": "bp_kernel<nearest,f32>", "peak_kind": peak_kind,
+                         "note": "the backprojector is bounded by its shared-memory gather, see gather_roofline"},
+            "gather_roofline": {"achieved_gups": gups_bp, "peak_gups": peak_gups, "frac": gups_bp / peak_gups,
+                                "bytes_per_update": 4, "fp32_ops_per_update": 4, "sm_mhz": sm_mhz},
+            "kernel_ms": {"filter_per_launch": f_ms / max(1, f_n), "bp_per_launch": bp_ms / max(1, bp_n),
+                          "launches_per_step": {"filter": f_n, "bp": bp_n}},
+            "variants": variants,
+            "clocks": clocks,
+            "gpu_launches": int(launches),
+        }
+        if ws == 1 and not args.no_cpu:
+            sino_host = sino[: 4].cpu().numpy()
+            result["cpu_baseline"] = cpu_baseline(sino_host, angp)
+        print(json.dumps(result), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# -------------------------------------------------------- reference arm --
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return
+    lib_path = os.path.join(REPO, "oracle", "_ref", "libraft_ref.so")
+    if not os.path.exists(lib_path):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libraft_ref.so not built"}))
+        return
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    S = args.ref_slices
+    sino, ang = make_sinograms_gpu(S, 2_000_000, dev)
+    h_sino = sino.cpu().numpy()
+    del sino
+    torch.cuda.empty_cache()
+    lib = ctypes.CDLL(lib_path)
+    P, I = ctypes.c_void_p, ctypes.c_int
+    lib.getFBPMultiGPU.argtypes = [P, I, P, P, P, P, P]
+    g = np.array([local], np.intc)
+    pf, pi = fbp_params(S, blocksize=S)
+    obj = np.zeros((S, N_RAYS, N_RAYS), np.float32)
+    angp = np.ascontiguousarray(ang)
+
+    def p(a):
+        return a.ctypes.data_as(ctypes.c_void_p)
+
+    def step():
+        lib.getFBPMultiGPU(p(g), 1, p(obj), p(h_sino), p(angp), p(pf), p(pi))
+
+    for _ in range(args.warmup):
+        step()
+    ts = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            step()
+            ts.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(ts) / len(ts)
+    value = S / (ms / 1e3)
+    sample = (f"{S} of 512 slices per step through the reference's own getFBPMultiGPU "
+              f"(reference CUDA sources built for sm_100a, host buffers, blocksize {S})")
+    print(json.dumps({
+        "impl": "reference", "metric": "FBP slices/s at 2048^2 x 1800 angles", "value": value,
+        "unit": "slices/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (same generator and seeds as the ours arm)",
+        "config": {"workload": WORKLOAD, "operator": "reference nearest-sample FBP (padded 6144^2 grid)",
+                   "sample_slices_per_step": S},
+        "cpu_baseline": {"value": value, "unit": "slices/s", "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "slices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk.summary(),
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--slices", type=int, default=N_SLICES)
+    ap.add_argument("--ref-slices", type=int, default=4)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,119 @@
+/*
+ * raft_b200.h -- C ABI of libraft.so (ssc-raft_b200/sscRaft/lib/libraft.so),
+ * the B200 build of the ssc-raft parallel-beam reconstruction hot path.
+ *
+ * The first five functions are drop-in replacements: same names, argument
+ * lists, packed-parameter meaning and (void) return as the reference
+ * cnpem/ssc-raft library, so the reference's ctypes layer binds them
+ * unchanged.  All data pointers are HOST pointers to C-contiguous float32
+ * arrays (sinogram [slices][angles][rays], image [slices][N][N]); the
+ * library allocates, copies and frees device memory itself (device
+ * workspaces and pinned staging buffers are cached between calls).
+ *
+ * Error behaviour: the reference calls exit(-1) on any CUDA error
+ * (cuda/inc/common/logerror.hpp:59-67) and assert()s on a bad device id.
+ * Here no call exits the process; every failure is recorded in a
+ * thread-local status read with raft_last_error().  The Python layer
+ * (sscRaft) raises RuntimeError when it is set.
+ *
+ * Packed parameters (as built by sscRaft/geometries/parallel/fbp_methods.py:86-95
+ * and em_methods.py:136-145 of the reference):
+ *   FBP / lowpass  parami = {nrays, nangles, nslices, objsize, pad, 0, 0, filter, 0, blocksize}
+ *                  paramf = {1/(beta/delta) or 0, regularization, energy_eV, z2_m,
+ *                            pixel_x, pixel_y, rotation_axis_offset}
+ *   EM             parami = {nrays, nangles, nslices, objsize(=nrays), 0, 0, 0, nflats,
+ *                            iterations, blocksize}
+ *   filter ids     0 none, 1 gaussian, 2 lorentz, 3 cosine, 4 rectangle, 5 hann,
+ *                  6 hamming, 7 ramp, 8 differential, 9 shepp-logan (new)
+ */
+#ifndef RAFT_B200_H
+#define RAFT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* FBP (filter + nearest-sample backprojection, bit-faithful index rule).
+ * Replaces getFBPMultiGPU, cuda/src/geometries/parallel/reconstruction_methods/fbp.cu:238-302
+ * (ctypes prototype sscRaft/rafttypes.py:175-186).  obj [nslices][objsize][objsize] written. */
+void getFBPMultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *angles,
+                    float *paramf, int *parami);
+
+/* Filter only, in place on tomogram [nslices][nangles][nrays], axis offset 0.
+ * Replaces getFilterLowPassMultiGPU, cuda/src/processing/filters/low_pass.cu:84-141
+ * (rafttypes.py:188-198). */
+void getFilterLowPassMultiGPU(int *gpus, int ngpus, float *tomogram, float *paramf, int *parami);
+
+/* Ray-tracing Radon transform, tomogram_out [nslices][nangles][nrays] written.
+ * Replaces getRadonRTMultiGPU, cuda/src/geometries/parallel/forward_methods/radon_rt.cu:252-295
+ * (rafttypes.py:311-323). */
+void getRadonRTMultiGPU(int *gpus, int ngpus, float *tomogram_out, float *phantom, float *angles,
+                        int sizex, int sizey, int nrays, int nangles, int nslices, float ax, float ay);
+
+/* Transmission EM; obj is the initial guess and the result; count = exp(-data)
+ * (computed by the Python wrapper), flat [nslices][nrays] (the flat of each slice).
+ * Replaces get_tEM_RT_MultiGPU, cuda/src/geometries/parallel/reconstruction_methods/em_rt.cu:12-84
+ * (rafttypes.py:126-136). */
+void get_tEM_RT_MultiGPU(int *gpus, int ngpus, float *obj, float *count, float *flat, float *angles,
+                         float *paramf, int *parami);
+
+/* Emission EM; obj is the initial guess and the result.
+ * Replaces get_eEM_RT_MultiGPU, em_rt.cu:201-262 (rafttypes.py:138-147). */
+void get_eEM_RT_MultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *angles,
+                         float *paramf, int *parami);
+
+/* Adjacent reference exports kept as stubs that record "not implemented".
+ * getBSTMultiGPU: cuda/src/geometries/parallel/reconstruction_methods/bst.cu:674-734 (rafttypes.py:161-173).
+ * get_tEM_FQ_MultiGPU: .../reconstruction_methods/em_frequency.cu:339 (rafttypes.py:149-159). */
+void getBSTMultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *angles, float *paramf,
+                    int *parami, int nstreams);
+void get_tEM_FQ_MultiGPU(int *gpus, int ngpus, float *obj, float *count, float *flat, float *angles,
+                         float *paramf, int *parami);
+
+/* Status of the last call on this thread: returns 0 if it succeeded, 1 and
+ * the message (truncated to len-1 chars) otherwise.  Replaces the reference's
+ * exit(-1) (cuda/inc/common/logerror.hpp:59-67). */
+int raft_last_error(char *buf, int len);
+void raft_clear_error(void);
+int raft_abi_version(void);
+
+/* FBP with a selectable operator and sinogram storage (host buffers).
+ * geometry 0 = reference nearest-sample rule (store must be 0),
+ * geometry 1 = linear interpolation with true ramp-family filters
+ *              (store 1 = FP32 pairs, 2 = BF16 pairs; accumulation is FP32).
+ * Extends getFBPMultiGPU (fbp.cu:238-302); returns 0 on success. */
+int raft_fbp_ext(int *gpus, int ngpus, float *obj, const float *tomogram, const float *angles,
+                 const float *paramf, const int *parami, int geometry, int store);
+
+/* FBP on device-resident buffers of one GPU (d_obj, d_tomogram on `gpu`;
+ * angles host), issued on `stream` (NULL: library stream, synchronised).
+ * Same operator as raft_fbp_ext; getFBPGPU-level entry (fbp.cu:127-236). */
+int raft_fbp_device(int gpu, float *d_obj, const float *d_tomogram, const float *angles,
+                    const float *paramf, const int *parami, int geometry, int store, void *stream);
+
+/* EM (kind 0 = tEM as get_tEM_RT_MultiGPU, 1 = eEM as get_eEM_RT_MultiGPU) on one GPU with
+ * host buffers, the iteration loop replayed as one CUDA graph when use_graph != 0, and
+ * per-iteration FP64 metrics [niter][nslices][3] = {sum (model-data)^2, sum data^2,
+ * negative log-likelihood} of the iterate entering that iteration (metrics may be NULL).
+ * The reference computes no residual (em_rt.cu:154-192,316-355). Returns 0 on success. */
+int raft_em_ext(int kind, int gpu, float *obj, const float *data, const float *flat,
+                const float *angles, int nrays, int nangles, int nslices, int niter,
+                double *metrics, int use_graph);
+
+/* As raft_em_ext on device-resident buffers (metrics device pointer or NULL). */
+int raft_em_device(int kind, int gpu, float *d_obj, const float *d_data, const float *d_flat,
+                   const float *angles, int nrays, int nangles, int nslices, int niter,
+                   double *d_metrics, int use_graph, void *stream);
+
+/* Instrumentation (no reference counterpart): total kernel launches issued by
+ * this library in the process; optional CUDA-event timing of the filter (class 0),
+ * backprojector (1) and projector (2) launches, summed since the last read. */
+long long raft_launch_count(void);
+void raft_profile_enable(int on);
+int raft_profile_read(double *ms, long long *counts, int nclasses);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RAFT_B200_H */

@@ -1,0 +1,198 @@
+"""ctypes binding of the FP64 CPU oracle (oracle/raft_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py, always as the checker.  The CUDA
+product (ssc-raft_b200/sscRaft) never imports this module.
+
+Every function takes numpy arrays in the reference layouts
+(sinogram [slices, angles, rays], image [slices, N, N]) and returns float64
+results.  See raft_oracle.c for the reference file:line each routine follows.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+MODE_REF = 0
+MODE_LIN = 1
+
+
+def build(force=False):
+    """Compile raft_oracle.c into liboracle.so (gcc + OpenMP)."""
+    src = os.path.join(HERE, "raft_oracle.c")
+    if not force and os.path.exists(LIB_PATH) and os.path.getmtime(LIB_PATH) >= os.path.getmtime(src):
+        return LIB_PATH
+    cmd = ["gcc", "-O3", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off",
+           "-o", LIB_PATH, src, "-lm"]
+    subprocess.check_call(cmd)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        I = ctypes.c_int
+        D = ctypes.c_double
+        F = ctypes.c_float
+        _lib.oracle_filter_spectrum.argtypes = [I, I, I, D, D, D, D, P, P]
+        _lib.oracle_filter_rows.argtypes = [I, I, I, I, I, D, D, D, D, P, P]
+        _lib.oracle_lowpass.argtypes = [I, I, I, I, I, D, D, D, P, P]
+        _lib.oracle_fbp_backproject.argtypes = [I, I, I, I, I, F, F, P, P, P]
+        _lib.oracle_fbp_backproject_f32.argtypes = [I, I, I, I, I, F, F, P, P, P]
+        _lib.oracle_fbp.argtypes = [I, I, I, I, I, I, D, D, D, F, F, P, P, P]
+        _lib.oracle_fbp_f32.argtypes = [I, I, I, I, I, I, D, D, D, F, F, P, P, P]
+        _lib.oracle_radon_rt.argtypes = [I, I, I, I, I, F, F, P, P, P]
+        _lib.oracle_em_forward.argtypes = [I, I, I, I, P, P, P]
+        _lib.oracle_em_backproject.argtypes = [I, I, I, I, P, P, P]
+        _lib.oracle_tem.argtypes = [I, I, I, I, I, P, P, P, P]
+        _lib.oracle_eem.argtypes = [I, I, I, I, I, P, P, P]
+        _lib.oracle_tem_metrics.argtypes = [I, I, I, I, P, P, P, P, P, P]
+    return _lib
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _as3(a):
+    a = np.asarray(a)
+    return a[None] if a.ndim == 2 else a
+
+
+def filter_spectrum(mode, ftype, Np, paganin=0.0, reg=0.0, offset=0.0, pixel=1.0):
+    hre = np.zeros(Np)
+    him = np.zeros(Np)
+    lib().oracle_filter_spectrum(mode, ftype, Np, paganin, reg, offset, pixel, _p(hre), _p(him))
+    return hre + 1j * him
+
+
+def filter_rows(sino, mode, ftype, pad, paganin=0.0, reg=0.0, offset=0.0, pixel=1.0):
+    """Filtered, edge-padded rows: [..., Np] float64."""
+    s = _f32(sino)
+    N = s.shape[-1]
+    nrows = s.size // N
+    Np = N * (1 + pad)
+    q = np.zeros(s.shape[:-1] + (Np,))
+    lib().oracle_filter_rows(mode, ftype, N, nrows, pad, paganin, reg, offset, pixel, _p(s), _p(q))
+    return q
+
+
+def lowpass(sino, mode, ftype, pad, paganin=0.0, reg=0.0, pixel=1.0):
+    s = _f32(sino)
+    N = s.shape[-1]
+    out = np.zeros(s.shape)
+    lib().oracle_lowpass(mode, ftype, N, s.size // N, pad, paganin, reg, pixel, _p(s), _p(out))
+    return out
+
+
+def fbp(sino, angles, mode, ftype, pad, paganin=0.0, reg=0.0, offset=0.0, pixel=1.0,
+        f32=False):
+    """FBP of sino [B, A, N] -> [B, N, N] (float64, or float32 if f32)."""
+    s = _f32(_as3(sino))
+    B, A, N = s.shape
+    ang = _f32(angles)
+    if f32:
+        img = np.zeros((B, N, N), dtype=np.float32)
+        lib().oracle_fbp_f32(mode, ftype, N, A, B, pad, paganin, reg, offset, pixel, pixel,
+                             _p(ang), _p(s), _p(img))
+    else:
+        img = np.zeros((B, N, N))
+        lib().oracle_fbp(mode, ftype, N, A, B, pad, paganin, reg, offset, pixel, pixel,
+                         _p(ang), _p(s), _p(img))
+    return img
+
+
+def fbp_backproject(q, angles, mode, N, pad, pixel=1.0):
+    q = _f64(_as3(q))
+    B, A, Np = q.shape
+    img = np.zeros((B, N, N))
+    lib().oracle_fbp_backproject(mode, N, A, B, pad, pixel, pixel, _p(_f32(angles)), _p(q), _p(img))
+    return img
+
+
+def radon_rt(img, angles, nrays=None, ax=1.0, ay=1.0):
+    """Radon_RT_version_sscRadon (without the Python-side N*pixel/2 scale)."""
+    im = _f32(_as3(img))
+    B, ny, nx = im.shape
+    nrays = nx if nrays is None else nrays
+    ang = _f32(angles)
+    out = np.zeros((B, len(ang), nrays))
+    lib().oracle_radon_rt(nx, ny, nrays, len(ang), B, ax, ay, _p(ang), _p(im), _p(out))
+    return out
+
+
+def em_forward(img, angles, nrays):
+    im = _f64(_as3(img))
+    B, N, _ = im.shape
+    ang = _f32(angles)
+    out = np.zeros((B, len(ang), nrays))
+    lib().oracle_em_forward(N, nrays, len(ang), B, _p(ang), _p(im), _p(out))
+    return out
+
+
+def em_backproject(sino, angles, N):
+    s = None if sino is None else _f64(_as3(sino))
+    ang = _f32(angles)
+    if s is None:
+        raise ValueError("use em_backproject_ones")
+    B, A, nrays = s.shape
+    img = np.zeros((B, N, N))
+    lib().oracle_em_backproject(N, nrays, A, B, _p(ang), _p(s), _p(img))
+    return img
+
+
+def em_backproject_ones(angles, N, nrays, nslices=1):
+    ang = _f32(angles)
+    img = np.zeros((nslices, N, N))
+    lib().oracle_em_backproject(N, nrays, len(ang), nslices, _p(ang), None, _p(img))
+    return img
+
+
+def tem(counts_exp, flat, angles, niter, obj=None):
+    """tEM on counts already mapped through exp(-x) (em_methods.py:109)."""
+    c = _f32(_as3(counts_exp))
+    B, A, nrays = c.shape
+    N = nrays
+    fl = _f32(np.asarray(flat).reshape(B, nrays))
+    o = np.ones((B, N, N)) if obj is None else _f64(_as3(obj)).copy()
+    lib().oracle_tem(N, nrays, A, B, niter, _p(_f32(angles)), _p(c), _p(fl), _p(o))
+    return o
+
+
+def eem(tomo, angles, niter, obj=None):
+    t = _f32(_as3(tomo))
+    B, A, nrays = t.shape
+    N = nrays
+    o = np.ones((B, N, N)) if obj is None else _f64(_as3(obj)).copy()
+    lib().oracle_eem(N, nrays, A, B, niter, _p(_f32(angles)), _p(t), _p(o))
+    return o
+
+
+def tem_metrics(counts_exp, flat, angles, obj):
+    c = _f32(_as3(counts_exp))
+    B, A, nrays = c.shape
+    N = nrays
+    fl = _f32(np.asarray(flat).reshape(B, nrays))
+    o = _f64(_as3(obj))
+    res = np.zeros(B)
+    nll = np.zeros(B)
+    lib().oracle_tem_metrics(N, nrays, A, B, _p(_f32(angles)), _p(c), _p(fl), _p(o), _p(res), _p(nll))
+    return res, nll

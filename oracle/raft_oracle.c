@@ -1,0 +1,496 @@
+/*
+ * raft_oracle.c -- CPU restatement of the ssc-raft parallel-beam hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA product in
+ * ssc-raft_b200/csrc: tests/, __graft_entry__.smoke() and the cpu_baseline leg
+ * of bench.py are the only callers.  The product never links or calls it.
+ *
+ * Everything accumulates in FP64.  Where the reference computes an integer
+ * sample index from FP32 arithmetic (nearest-truncation operators, "ref"
+ * mode) the index is computed here with the same FP32 expression order, but
+ * with the C library's correctly rounded-ish sinf/cosf instead of the GPU's
+ * fast intrinsics, so a handful of borderline samples (fractional part within
+ * ~1e-3 of an integer) may pick the neighbouring bin.  Tests therefore compare
+ * ref-mode results in relative L2 with a stated tolerance.
+ *
+ * Reference files followed (paths inside cnpem/ssc-raft):
+ *   edge padding      cuda/src/common/padding.cu:140-178 (paddR2R)
+ *   crop              cuda/src/common/padding.cu:245-268 (remove_paddR2R)
+ *   filter weights    cuda/src/processing/filters/filters.cu:33-51 (tent + phase)
+ *                     cuda/src/processing/filters/filters.cu:395-438 (Filter::apply)
+ *   filter driver     cuda/src/processing/filters/filters.cu:163-190 (filterFBP)
+ *                     cuda/src/processing/filters/filters.cu:120-161 (filterFBPpad)
+ *   FBP backprojector cuda/src/geometries/parallel/reconstruction_methods/fbp.cu:8-76
+ *   FBP driver        cuda/src/geometries/parallel/reconstruction_methods/fbp.cu:81-236
+ *   Radon RT          cuda/src/geometries/parallel/forward_methods/radon_rt.cu:131-174
+ *   EM kernels        cuda/src/geometries/parallel/reconstruction_methods/kernels/em_RT_kernel.cu:20-351
+ *   tEM / eEM loops   cuda/src/geometries/parallel/reconstruction_methods/em_rt.cu:154-192,316-355
+ */
+#include <complex.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef double complex cplx;
+
+static const double PI_D = 3.14159265358979323846;
+
+/* ------------------------------------------------------------------------ */
+/* Mixed-radix FFT (any length; smallest-prime-factor decimation in time).   */
+/* ------------------------------------------------------------------------ */
+static int smallest_factor(int n)
+{
+    if (n % 4 == 0) return 4;
+    if (n % 2 == 0) return 2;
+    for (int p = 3; p * p <= n; p += 2)
+        if (n % p == 0) return p;
+    return n;
+}
+
+/* out[k] = sum_n in[n*stride] w^(n*k*(ntot/n)), w = exp(sign*2*pi*i/ntot);
+ * recursive decimation in time.  `root` holds the ntot roots of unity. */
+static void fft_rec(int n, const cplx *in, int stride, cplx *out, const cplx *root, int ntot,
+                    cplx *scratch)
+{
+    if (n == 1) { out[0] = in[0]; return; }
+    int p = smallest_factor(n);
+    int m = n / p;
+    for (int r = 0; r < p; r++)
+        fft_rec(m, in + (size_t)r * stride, stride * p, out + (size_t)r * m, root, ntot, scratch);
+    int step = ntot / n;      /* root index of exp(2 pi i / n) */
+    int pstep = ntot / p;     /* root index of exp(2 pi i / p) */
+    for (int k = 0; k < m; k++) {
+        for (int r = 0; r < p; r++)
+            scratch[r] = out[(size_t)r * m + k] * root[(size_t)((long long)r * k * step % ntot)];
+        for (int q = 0; q < p; q++) {
+            cplx acc = 0;
+            for (int r = 0; r < p; r++) acc += scratch[r] * root[(size_t)(((long long)r * q) % p) * pstep];
+            scratch[p + q] = acc;
+        }
+        for (int q = 0; q < p; q++) out[(size_t)q * m + k] = scratch[p + q];
+    }
+}
+
+static void fft(int n, const cplx *in, cplx *out, const cplx *root, cplx *scratch)
+{
+    fft_rec(n, in, 1, out, root, n, scratch);
+}
+
+static cplx *make_roots(int n, int sign)
+{
+    cplx *root = (cplx *)malloc(sizeof(cplx) * (size_t)n);
+    for (int m = 0; m < n; m++) {
+        double ang = sign * 2.0 * PI_D * (double)m / (double)n;
+        root[m] = cos(ang) + I * sin(ang);
+    }
+    return root;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Filter spectrum.                                                          */
+/* ------------------------------------------------------------------------ */
+
+/* Filter::apply (filters.cu:395-438).  `w` is the tent weight. */
+static double ref_apply(int type, double w, double paganin, double reg)
+{
+    double pg = 1.0 / (1.0 + paganin * w * w);
+    switch (type) {
+    case 1: return w * exp(-0.693 * reg * w * w) * pg;
+    case 2: return w * (1.0 / (1.0 + reg * w * w)) * pg;
+    case 3: return w * cos(PI_D * 0.5 * w) * pg;
+    case 4: {
+        double param = fmax(w * reg * PI_D * 0.5, 1e-4);
+        return w * (sin(param) / param) * pg;
+    }
+    case 5: return w * (0.5 + 0.5 * cos(2.0 * PI_D * w)) * pg;
+    case 6: return w * (0.54 + 0.46 * cos(2.0 * PI_D * w)) * pg;
+    case 7: return w * pg;
+    case 8: return (w > 0) ? 1.0 / (2.0 * PI_D) : 0.0; /* SIGN(0)=0: DC weight taken as 0 */
+    default: return 1.0;
+    }
+}
+
+/* Linear-interpolation ("lin") mode filters: true ramp |k|/Np times a window
+ * of nu = 2k/Np (nu = 1 at Nyquist).  Filter ids follow the reference enum
+ * (filters.hpp:26-37) plus 9 = Shepp-Logan. */
+static double lin_apply(int type, double nu, double paganin, double reg)
+{
+    double ramp = 0.5 * nu;
+    double pg = 1.0 / (1.0 + paganin * nu * nu);
+    switch (type) {
+    case 1: return ramp * exp(-0.693 * reg * nu * nu) * pg;
+    case 2: return ramp / (1.0 + reg * nu * nu) * pg;
+    case 3: return ramp * cos(0.5 * PI_D * nu) * pg;
+    case 4: {
+        double param = fmax(nu * reg * PI_D * 0.5, 1e-4);
+        return ramp * (sin(param) / param) * pg;
+    }
+    case 5: return ramp * 0.5 * (1.0 + cos(PI_D * nu)) * pg;
+    case 6: return ramp * (0.54 + 0.46 * cos(PI_D * nu)) * pg;
+    case 7: return ramp * pg;
+    case 8: return (nu > 0) ? 1.0 / (2.0 * PI_D) : 0.0;
+    case 9: {
+        double a = 0.5 * PI_D * nu;
+        return ramp * (a > 0 ? sin(a) / a : 1.0) * pg;
+    }
+    default: return 1.0;
+    }
+}
+
+/* Full-length (Hermitian-extended) filter spectrum, including the
+ * 1/(Np*pixel) normalisation of filters.cu:184-186.
+ * mode 0 = ref (tent weight 0.5*min(k,M-k)/M, M=Np/2+1, phase denominator 2M-2),
+ * mode 1 = lin (ramp |k|/Np, phase denominator Np). */
+void oracle_filter_spectrum(int mode, int type, int Np, double paganin, double reg,
+                            double offset, double pixel, double *hre, double *him)
+{
+    int M = Np / 2 + 1;
+    double norm = 1.0 / ((double)Np * pixel);
+    for (int k = 0; k < Np; k++) {
+        int kk = (k <= Np / 2) ? k : Np - k;
+        double w, phase;
+        if (mode == 0) {
+            double tent = 0.5 * fmin((double)kk, (double)(M - kk)) / (double)M;
+            w = ref_apply(type, tent, paganin, reg);
+            phase = 2.0 * PI_D / (double)(2 * M - 2) * offset * (double)kk;
+        } else {
+            w = lin_apply(type, 2.0 * (double)kk / (double)Np, paganin, reg);
+            phase = 2.0 * PI_D * offset * (double)kk / (double)Np;
+        }
+        double re = w * cos(phase), im = -w * sin(phase);
+        if (k > Np / 2) im = -im;                      /* conjugate half */
+        if ((Np % 2 == 0) && k == Np / 2) im = 0.0;      /* C2R drops Im of the Nyquist bin */
+        hre[k] = re * norm;
+        him[k] = im * norm;
+    }
+}
+
+/* Edge-replicating pad (padding.cu:140-178): out[i] = in[clamp(i - pad*N/2)]. */
+static void pad_row(const float *in, int N, int pad, int Np, double *out)
+{
+    int off = (pad * N) / 2;
+    for (int i = 0; i < Np; i++) {
+        int ii = i - off;
+        if (ii < 0) ii = 0;
+        if (ii > N - 1) ii = N - 1;
+        out[i] = in[ii];
+    }
+}
+
+/* Filtered, padded rows q[row][0..Np) for nrows rows of length N.
+ * type 0 ('none') copies the padded row unscaled, as the reference skips the
+ * filter entirely for it (fbp.cu:102-103). */
+void oracle_filter_rows(int mode, int type, int N, int nrows, int pad, double paganin,
+                        double reg, double offset, double pixel, const float *sino, double *q)
+{
+    int Np = N * (1 + pad);
+    double *hre = (double *)malloc(sizeof(double) * Np);
+    double *him = (double *)malloc(sizeof(double) * Np);
+    oracle_filter_spectrum(mode, type, Np, paganin, reg, offset, pixel, hre, him);
+    cplx *rfwd = make_roots(Np, -1), *rinv = make_roots(Np, +1);
+#pragma omp parallel
+    {
+        double *row = (double *)malloc(sizeof(double) * Np);
+        cplx *a = (cplx *)malloc(sizeof(cplx) * Np);
+        cplx *b = (cplx *)malloc(sizeof(cplx) * Np);
+        cplx *scratch = (cplx *)malloc(sizeof(cplx) * (size_t)(2 * Np + 8));
+#pragma omp for schedule(dynamic, 4)
+        for (int r = 0; r < nrows; r++) {
+            pad_row(sino + (size_t)r * N, N, pad, Np, row);
+            double *qr = q + (size_t)r * Np;
+            if (type == 0) {
+                memcpy(qr, row, sizeof(double) * Np);
+                continue;
+            }
+            for (int i = 0; i < Np; i++) a[i] = row[i];
+            fft(Np, a, b, rfwd, scratch);
+            for (int k = 0; k < Np; k++) b[k] *= (hre[k] + I * him[k]);
+            fft(Np, b, a, rinv, scratch);
+            for (int i = 0; i < Np; i++) qr[i] = creal(a[i]);
+        }
+        free(row); free(a); free(b); free(scratch);
+    }
+    free(hre); free(him); free(rfwd); free(rinv);
+}
+
+/* Lowpass (low_pass.cu:9-29 + filterFBPpad): filter with internal padding,
+ * axis offset 0, result cropped back to N (centre, offset pad*N/2). */
+void oracle_lowpass(int mode, int type, int N, int nrows, int pad, double paganin, double reg,
+                    double pixel, const float *sino, double *out)
+{
+    int Np = N * (1 + pad);
+    int off = (pad * N) / 2;
+    double *q = (double *)malloc(sizeof(double) * (size_t)nrows * Np);
+    oracle_filter_rows(mode, type, N, nrows, pad, paganin, reg, 0.0, pixel, sino, q);
+    for (int r = 0; r < nrows; r++)
+        for (int i = 0; i < N; i++) out[(size_t)r * N + i] = q[(size_t)r * Np + off + i];
+    free(q);
+}
+
+/* ------------------------------------------------------------------------ */
+/* FBP backprojection on the central N x N window of the padded grid.       */
+/* ------------------------------------------------------------------------ */
+static void angle_steps(const float *angles, int A, float *dth)
+{
+    for (int a = 0; a < A; a++) {
+        if (A == 1) { dth[a] = 1.0f; continue; }
+        dth[a] = (a == A - 1) ? angles[a] - angles[a - 1] : angles[a + 1] - angles[a];
+    }
+}
+
+static float angle_scale(const float *angles, int A)
+{
+    return (angles[A - 1] > (float)PI_D) ? (float)PI_D / angles[A - 1] : 1.0f;
+}
+
+/* mode 0: fbp.cu:38-74 truncation rule.  mode 1: linear interpolation on the
+ * same sample grid (u = (t - tmin)/dt, samples at integer u, zero outside). */
+#define DEFINE_BP(NAME, ACC)                                                                   \
+void NAME(int mode, int N, int A, int nslices, int pad, float pixel_x, float pixel_y,           \
+          const float *angles, const double *q, ACC *img)                                       \
+{                                                                                               \
+    int Np = N * (1 + pad);                                                                     \
+    int off = (pad * N) / 2;                                                                    \
+    float *cs = (float *)malloc(sizeof(float) * A), *sn = (float *)malloc(sizeof(float) * A);   \
+    float *dth = (float *)malloc(sizeof(float) * A);                                            \
+    double *cd = (double *)malloc(sizeof(double) * A), *sd = (double *)malloc(sizeof(double) * A); \
+    for (int a = 0; a < A; a++) {                                                               \
+        cs[a] = cosf(angles[a]); sn[a] = sinf(angles[a]);                                       \
+        cd[a] = cos((double)angles[a]); sd[a] = sin((double)angles[a]);                         \
+    }                                                                                           \
+    angle_steps(angles, A, dth);                                                                \
+    float scale = angle_scale(angles, A);                                                       \
+    float xmin = -pixel_x * (float)Np / 2.0f;                                                   \
+    float ymin = -pixel_y * (float)Np / 2.0f;                                                   \
+    float tmin = -pixel_x * (float)Np / 2.0f;                                                   \
+    float dt = pixel_x;                                                                         \
+    _Pragma("omp parallel for collapse(2) schedule(dynamic, 8)")                                \
+    for (int k = 0; k < nslices; k++)                                                           \
+        for (int jj = 0; jj < N; jj++) {                                                        \
+            const double *qk = q + (size_t)k * A * Np;                                          \
+            for (int ii = 0; ii < N; ii++) {                                                    \
+                int i = ii + off, j = jj + off;                                                 \
+                ACC sum = 0;                                                                    \
+                if (mode == 0) {                                                                \
+                    float x = xmin + (float)i * pixel_x;                                        \
+                    float y = ymin + (float)j * pixel_y;                                        \
+                    for (int a = 0; a < A; a++) {                                               \
+                        float t = x * cs[a] - y * sn[a];                                        \
+                        int ti = (int)((t - tmin) / dt);                                        \
+                        if (ti > -1 && ti < Np) sum += (ACC)qk[(size_t)a * Np + ti] * (ACC)dth[a]; \
+                    }                                                                           \
+                } else {                                                                        \
+                    double x = ((double)i - 0.5 * Np) * pixel_x;                                \
+                    double y = ((double)j - 0.5 * Np) * pixel_y;                                \
+                    for (int a = 0; a < A; a++) {                                               \
+                        double u = (x * cd[a] - y * sd[a]) / pixel_x + 0.5 * Np;                \
+                        double fl = floor(u);                                                   \
+                        int b0 = (int)fl;                                                       \
+                        double f = u - fl;                                                      \
+                        double v0 = (b0 >= 0 && b0 < Np) ? qk[(size_t)a * Np + b0] : 0.0;      \
+                        double v1 = (b0 + 1 >= 0 && b0 + 1 < Np) ? qk[(size_t)a * Np + b0 + 1] : 0.0; \
+                        sum += (ACC)(((1.0 - f) * v0 + f * v1) * (double)dth[a]);              \
+                    }                                                                           \
+                }                                                                               \
+                img[((size_t)k * N + jj) * N + ii] = sum * (ACC)scale;                          \
+            }                                                                                   \
+        }                                                                                       \
+    free(cs); free(sn); free(dth); free(cd); free(sd);                                           \
+}
+
+DEFINE_BP(oracle_fbp_backproject, double)
+DEFINE_BP(oracle_fbp_backproject_f32, float)
+
+/* Full FBP: filter (unless type 'none') then backproject.  img is [nslices,N,N]. */
+void oracle_fbp(int mode, int type, int N, int A, int nslices, int pad, double paganin,
+                double reg, double offset, float pixel_x, float pixel_y, const float *angles,
+                const float *sino, double *img)
+{
+    int Np = N * (1 + pad);
+    double *q = (double *)malloc(sizeof(double) * (size_t)nslices * A * Np);
+    oracle_filter_rows(mode, type, N, nslices * A, pad, paganin, reg, offset, pixel_x, sino, q);
+    oracle_fbp_backproject(mode, N, A, nslices, pad, pixel_x, pixel_y, angles, q, img);
+    free(q);
+}
+
+/* FP32-accumulating variant used as the timed CPU baseline. */
+void oracle_fbp_f32(int mode, int type, int N, int A, int nslices, int pad, double paganin,
+                    double reg, double offset, float pixel_x, float pixel_y, const float *angles,
+                    const float *sino, float *img)
+{
+    int Np = N * (1 + pad);
+    double *q = (double *)malloc(sizeof(double) * (size_t)nslices * A * Np);
+    oracle_filter_rows(mode, type, N, nslices * A, pad, paganin, reg, offset, pixel_x, sino, q);
+    oracle_fbp_backproject_f32(mode, N, A, nslices, pad, pixel_x, pixel_y, angles, q, img);
+    free(q);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Radon RT (radon_rt.cu:131-174).  out[k][a][i]                            */
+/* ------------------------------------------------------------------------ */
+void oracle_radon_rt(int nx, int ny, int nrays, int A, int nslices, float ax, float ay,
+                     const float *angles, const float *img, double *out)
+{
+    float dx = 2.0f * ax / (float)(nx - 1);
+    float dy = 2.0f * ay / (float)(ny - 1);
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+    for (int k = 0; k < nslices; k++)
+        for (int a = 0; a < A; a++) {
+            float c = cosf(angles[a]), s = sinf(angles[a]);
+            for (int i = 0; i < nrays; i++) {
+                float t = -ax + (float)i * dx;
+                double sum = 0;
+                for (int r = 0; r < ny; r++) {
+                    float sr = -ay + (float)r * dy;
+                    float x = t * c - sr * s;
+                    float y = t * s + sr * c;
+                    int ix = (int)((x + 1) / dx);
+                    int iy = (int)((y + 1) / dy);
+                    if (ix >= 0 && ix < nx && iy >= 0 && iy < ny)
+                        sum += img[((size_t)k * ny + iy) * nx + ix];
+                }
+                out[((size_t)k * A + a) * nrays + i] = sum * (double)dy;
+            }
+        }
+}
+
+/* ------------------------------------------------------------------------ */
+/* EM operators (em_RT_kernel.cu).                                           */
+/* ------------------------------------------------------------------------ */
+
+/* kernel_radon (em_RT_kernel.cu:145-185), a = 1: out[k][a][r] */
+void oracle_em_forward(int N, int nrays, int A, int nslices, const float *angles,
+                       const double *img, double *out)
+{
+    float a1 = 1.0f;
+    float dt = (float)(2.0 * a1 / (nrays - 1));
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
+    for (int k = 0; k < nslices; k++)
+        for (int a = 0; a < A; a++) {
+            float c = cosf(angles[a]), s = sinf(angles[a]);
+            for (int r = 0; r < nrays; r++) {
+                float t = -a1 + (float)r * dt;
+                double sum = 0;
+                for (int m = 0; m < nrays; m++) {
+                    float sm = -a1 + (float)m * dt;
+                    float x = t * c - sm * s;
+                    float y = t * s + sm * c;
+                    int X = (int)((x + 1) / dt);
+                    int Y = (int)((y + 1) / dt);
+                    if (X >= 0 && X < N && Y >= 0 && Y < N)
+                        sum += img[((size_t)k * N + Y) * N + X];
+                }
+                out[((size_t)k * A + a) * nrays + r] = sum * (double)dt;
+            }
+        }
+}
+
+/* kernel_backprojection (em_RT_kernel.cu:92-142); sino==NULL gives the
+ * back-projection of ones (kernel_backprojectionOfOnes, :303-351). */
+void oracle_em_backproject(int N, int nrays, int A, int nslices, const float *angles,
+                           const double *sino, double *img)
+{
+    float dxy = (float)(2.0 / (N - 1));
+    float dt = (float)(2.0 / (nrays - 1));
+    float *cs = (float *)malloc(sizeof(float) * A), *sn = (float *)malloc(sizeof(float) * A);
+    float *dth = (float *)malloc(sizeof(float) * A);
+    for (int a = 0; a < A; a++) { cs[a] = cosf(angles[a]); sn[a] = sinf(angles[a]); }
+    angle_steps(angles, A, dth);
+#pragma omp parallel for collapse(2) schedule(dynamic, 8)
+    for (int k = 0; k < nslices; k++)
+        for (int j = 0; j < N; j++)
+            for (int i = 0; i < N; i++) {
+                float x = -1.0f + (float)i * dxy;
+                float y = -1.0f + (float)j * dxy;
+                double sum = 0;
+                for (int a = 0; a < A; a++) {
+                    float t = x * cs[a] + y * sn[a];
+                    int T = (int)((t + 1.0f) / dt);
+                    if (T > -1 && T < nrays)
+                        sum += (sino ? sino[((size_t)k * A + a) * nrays + T] : 1.0) * (double)dth[a];
+                }
+                img[((size_t)k * N + j) * N + i] = sum;
+            }
+    free(cs); free(sn); free(dth);
+}
+
+/* tEM (em_rt.cu:154-192).  counts = exp(-data) already applied (as the
+ * Python wrapper does, em_methods.py:109).  flat is [nslices][nrays]
+ * (intended semantics: flat of the slice, not of the angle row). */
+void oracle_tem(int N, int nrays, int A, int nslices, int niter, const float *angles,
+                const float *counts, const float *flat, double *obj)
+{
+    size_t ns = (size_t)nslices * A * nrays, ni = (size_t)nslices * N * N;
+    double *c = (double *)malloc(sizeof(double) * ns);
+    double *p = (double *)malloc(sizeof(double) * ns);
+    double *bc = (double *)malloc(sizeof(double) * ni);
+    double *b = (double *)malloc(sizeof(double) * ni);
+    for (size_t i = 0; i < ns; i++) c[i] = counts[i];
+    oracle_em_backproject(N, nrays, A, nslices, angles, c, bc);
+    for (int it = 0; it < niter; it++) {
+        oracle_em_forward(N, nrays, A, nslices, angles, obj, p);
+        for (int k = 0; k < nslices; k++)
+            for (int a = 0; a < A; a++)
+                for (int r = 0; r < nrays; r++) {
+                    size_t ix = ((size_t)k * A + a) * nrays + r;
+                    p[ix] = (double)flat[(size_t)k * nrays + r] * exp(-p[ix]);
+                }
+        oracle_em_backproject(N, nrays, A, nslices, angles, p, b);
+        for (size_t i = 0; i < ni; i++) obj[i] = obj[i] * b[i] / bc[i];
+    }
+    free(c); free(p); free(bc); free(b);
+}
+
+/* eEM (em_rt.cu:316-355; kernel_radonWithDivision em_RT_kernel.cu:188-246). */
+void oracle_eem(int N, int nrays, int A, int nslices, int niter, const float *angles,
+                const float *tomo, double *obj)
+{
+    size_t ns = (size_t)nslices * A * nrays, ni = (size_t)nslices * N * N;
+    double *p = (double *)malloc(sizeof(double) * ns);
+    double *bo = (double *)malloc(sizeof(double) * ni);
+    double *b = (double *)malloc(sizeof(double) * ni);
+    oracle_em_backproject(N, nrays, A, nslices, angles, NULL, bo);
+    for (int it = 0; it < niter; it++) {
+        oracle_em_forward(N, nrays, A, nslices, angles, obj, p);
+        for (size_t i = 0; i < ns; i++) {
+            double v = p[i];
+            double sg = (v > 0) ? 1.0 : ((v < 0) ? -1.0 : 0.0);
+            double r = (double)tomo[i] * sg / sqrt(1e-8 + v * v);
+            p[i] = r < 0 ? 0.0 : r;
+        }
+        oracle_em_backproject(N, nrays, A, nslices, angles, p, b);
+        for (size_t i = 0; i < ni; i++) obj[i] = obj[i] * b[i] / bo[i];
+    }
+    free(p); free(bo); free(b);
+}
+
+/* Transmission data residual ||flat*exp(-Ax) - y|| / ||y|| and Poisson
+ * negative log-likelihood sum(flat*exp(-Ax) + y*Ax), both per slice. */
+void oracle_tem_metrics(int N, int nrays, int A, int nslices, const float *angles,
+                        const float *counts, const float *flat, const double *obj,
+                        double *residual, double *nll)
+{
+    size_t ns = (size_t)nslices * A * nrays;
+    double *p = (double *)malloc(sizeof(double) * ns);
+    oracle_em_forward(N, nrays, A, nslices, angles, obj, p);
+    for (int k = 0; k < nslices; k++) {
+        double num = 0, den = 0, l = 0;
+        for (int a = 0; a < A; a++)
+            for (int r = 0; r < nrays; r++) {
+                size_t ix = ((size_t)k * A + a) * nrays + r;
+                double m = (double)flat[(size_t)k * nrays + r] * exp(-p[ix]);
+                double y = counts[ix];
+                num += (m - y) * (m - y);
+                den += y * y;
+                l += m + y * p[ix];
+            }
+        residual[k] = sqrt(num) / (den > 0 ? sqrt(den) : 1.0);
+        nll[k] = l;
+    }
+    free(p);
+}

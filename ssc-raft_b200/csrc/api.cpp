@@ -1,0 +1,414 @@
+// api.cpp -- the C ABI of libraft.so.
+//
+// The five reference entry points keep their exact names and signatures
+// (void return, packed int/float parameter arrays, host pointers), so the
+// ssc-raft ctypes layer binds them unchanged.  They never exit the process:
+// failures are recorded and read back with raft_last_error().  Extensions
+// (operator mode, sinogram storage precision, device-resident buffers, EM
+// residual metrics) are separate exports; see include/raft_b200.h.
+#include "engine.hpp"
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace raft {
+
+// --------------------------------------------------------------- status --
+static thread_local std::string t_error;
+
+void set_error(const std::string &msg)
+{
+    if (t_error.empty()) t_error = msg;
+}
+bool has_error() { return !t_error.empty(); }
+std::string get_error() { return t_error; }
+void clear_error() { t_error.clear(); }
+
+// ----------------------------------------------------------- parameters --
+// setFBPParameters, cuda/src/geometries/parallel/reconstruction_methods/parameters.cu:131-219
+static bool parse_fbp_arrays(const float *paramf, const int *parami, FbpConfig &c, bool need_obj)
+{
+    if (!paramf || !parami) {
+        set_error("null parameter array");
+        return false;
+    }
+    c.nrays = parami[0];
+    c.nangles = parami[1];
+    c.nslices = parami[2];
+    c.objsize = parami[3];
+    c.pad = parami[4];
+    c.filter = parami[7];
+    c.blocksize = parami[9];
+    c.beta_delta = paramf[0];
+    c.reg = paramf[1];
+    c.energy = paramf[2];
+    c.z2 = paramf[3];
+    c.pixel_x = paramf[4];
+    c.pixel_y = paramf[5];
+    c.offset = paramf[6];
+    // parameters.cu:201-203 (float arithmetic; plank*vc in double as there)
+    const float plank = 4.135667696E-15f;
+    (void)plank;
+    float wavelength = (c.beta_delta == 0.0f) ? 1.0f : (float)((4.135667696E-15 * 299792458) / c.energy);
+    c.paganin = wavelength * c.z2 * float(M_PI) * c.beta_delta / (c.pixel_x * c.pixel_x);
+    if (c.nrays < 2 || c.nangles < 1 || c.nslices < 0 || c.pad < 0 || c.pad > 64) {
+        set_error("invalid sizes: need nrays >= 2, nangles >= 1, nslices >= 0, 0 <= pad <= 64");
+        return false;
+    }
+    if (need_obj && c.objsize < 1) {
+        set_error("invalid object size");
+        return false;
+    }
+    if (c.filter < 0 || c.filter > 9) {
+        set_error("invalid filter type (valid: 0..9)");
+        return false;
+    }
+    if (!(c.pixel_x > 0.f) || !(c.pixel_y > 0.f) || !std::isfinite(c.pixel_x) || !std::isfinite(c.pixel_y)) {
+        set_error("invalid pixel size");
+        return false;
+    }
+    return true;
+}
+
+// setEMRTParameters, parameters.cu:8-59
+static bool parse_em_arrays(const float *paramf, const int *parami, EmConfig &c)
+{
+    (void)paramf;
+    if (!parami) {
+        set_error("null parameter array");
+        return false;
+    }
+    c.nrays = parami[0];
+    c.nangles = parami[1];
+    c.nslices = parami[2];
+    c.objsize = parami[3];
+    c.nflats = parami[7];
+    c.niter = parami[8];
+    c.blocksize = parami[9];
+    if (c.nrays < 2 || c.nangles < 2 || c.nslices < 0 || c.objsize < 2 || c.niter < 0) {
+        set_error("invalid EM sizes: need nrays >= 2, nangles >= 2, objsize >= 2, iterations >= 0");
+        return false;
+    }
+    if (c.objsize != c.nrays) {
+        set_error("EM requires objsize == nrays (em_methods.py:31,107)");
+        return false;
+    }
+    return true;
+}
+
+static bool check_gpus(const int *gpus, int ngpus)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("no CUDA device available");
+        return false;
+    }
+    if (!gpus || ngpus < 1) {
+        set_error("empty GPU list");
+        return false;
+    }
+    for (int i = 0; i < ngpus; i++)
+        if (gpus[i] < 0 || gpus[i] >= count) {
+            set_error("invalid device number " + std::to_string(gpus[i]));
+            return false;
+        }
+    return true;
+}
+
+// Contiguous z-slabs, one host thread per device (fbp.cu:267-301); errors
+// from worker threads are carried back into the caller's status.
+template <class F>
+static void split_slabs(const int *gpus, int ngpus, int nslices, F work)
+{
+    const int sub = (nslices + ngpus - 1) / ngpus;
+    if (ngpus == 1) {
+        try {
+            work(gpus[0], 0, nslices);
+        } catch (const CudaFail &) {
+        } catch (const std::exception &e) {
+            set_error(e.what());
+        }
+        return;
+    }
+    std::vector<std::thread> th;
+    std::vector<std::string> errs(ngpus);
+    int ptr = 0;
+    for (int i = 0; i < ngpus; i++) {
+        const int n = std::max(0, std::min(nslices - ptr, sub));
+        const int start = ptr;
+        th.emplace_back([&, i, start, n] {
+            try {
+                work(gpus[i], start, n);
+            } catch (const CudaFail &) {
+            } catch (const std::exception &e) {
+                set_error(e.what());
+            }
+            errs[i] = get_error();
+        });
+        ptr += n;
+    }
+    for (auto &t : th) t.join();
+    for (auto &e : errs)
+        if (!e.empty()) {
+            set_error(e);
+            break;
+        }
+}
+
+}  // namespace raft
+
+using namespace raft;
+
+extern "C" {
+
+int raft_last_error(char *buf, int len)
+{
+    const std::string &e = t_error;
+    if (buf && len > 0) {
+        const int n = (int)std::min<size_t>(e.size(), (size_t)len - 1);
+        std::memcpy(buf, e.data(), n);
+        buf[n] = 0;
+    }
+    return e.empty() ? 0 : 1;
+}
+
+void raft_clear_error(void) { clear_error(); }
+
+int raft_abi_version(void) { return 1; }
+
+// --- FBP ------------------------------------------------------------------
+static void fbp_common(int *gpus, int ngpus, float *obj, const float *tomogram, const float *angles,
+                       const float *paramf, const int *parami, int geometry, int store)
+{
+    clear_error();
+    FbpConfig cfg;
+    if (!parse_fbp_arrays(paramf, parami, cfg, true)) return;
+    if (!check_gpus(gpus, ngpus)) return;
+    if (!obj || !tomogram || !angles) {
+        set_error("null data pointer");
+        return;
+    }
+    cfg.geometry = geometry;
+    cfg.store = store;
+    const size_t obj_ps = (size_t)cfg.objsize * cfg.objsize, tomo_ps = (size_t)cfg.nangles * cfg.nrays;
+    split_slabs(gpus, ngpus, cfg.nslices, [&](int dev, int start, int n) {
+        fbp_host_slab(cfg, dev, obj + obj_ps * start, tomogram + tomo_ps * start, angles, n);
+    });
+}
+
+// Reference: getFBPMultiGPU, cuda/src/geometries/parallel/reconstruction_methods/fbp.cu:238-302
+void getFBPMultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *angles, float *paramf, int *parami)
+{
+    fbp_common(gpus, ngpus, obj, tomogram, angles, paramf, parami, GEOM_FBP_REF, STORE_F32);
+}
+
+int raft_fbp_ext(int *gpus, int ngpus, float *obj, const float *tomogram, const float *angles, const float *paramf,
+                 const int *parami, int geometry, int store)
+{
+    if (geometry != GEOM_FBP_REF && geometry != GEOM_FBP_LIN) {
+        clear_error();
+        set_error("raft_fbp_ext: geometry must be 0 (nearest, reference) or 1 (linear)");
+        return 1;
+    }
+    if (store < 0 || store > 2 || (geometry == GEOM_FBP_REF && store != STORE_F32) ||
+        (geometry == GEOM_FBP_LIN && store == STORE_F32)) {
+        clear_error();
+        set_error("raft_fbp_ext: store must be 0 with geometry 0, 1 (fp32) or 2 (bf16) with geometry 1");
+        return 1;
+    }
+    fbp_common(gpus, ngpus, obj, tomogram, angles, paramf, parami, geometry, store);
+    return has_error() ? 1 : 0;
+}
+
+// Device-resident FBP on one GPU: d_obj / d_tomogram are device pointers on
+// `gpu`, angles is host.  Runs on `stream` (0 = the library's own stream,
+// synchronised before returning).
+int raft_fbp_device(int gpu, float *d_obj, const float *d_tomogram, const float *angles, const float *paramf,
+                    const int *parami, int geometry, int store, void *stream)
+{
+    clear_error();
+    FbpConfig cfg;
+    if (!parse_fbp_arrays(paramf, parami, cfg, true)) return 1;
+    if (!check_gpus(&gpu, 1)) return 1;
+    cfg.geometry = geometry;
+    cfg.store = store;
+    try {
+        DeviceState &ds = device_state(gpu);
+        std::lock_guard<std::mutex> lk(ds.mtx);
+        RAFT_CUDA(cudaSetDevice(gpu));
+        ds.ensure();
+        cudaStream_t st = stream ? (cudaStream_t)stream : ds.s_comp;
+        FbpPrepared fp = prepare_fbp(cfg, gpu);
+        FbpTables tb = fbp_tables(ds, fp, angles, st);
+        const size_t tomo_ps = (size_t)cfg.nangles * cfg.nrays;
+        const int chunk = std::max(1, std::min(cfg.nslices, cfg.blocksize > 0 ? cfg.blocksize : 32));
+        void *rows = ds.rows.get(fbp_rows_bytes(fp, chunk));
+        for (int s0 = 0; s0 < cfg.nslices; s0 += chunk) {
+            const int ns = std::min(chunk, cfg.nslices - s0);
+            fbp_chunk(ds, fp, tb, d_tomogram + tomo_ps * s0, d_obj + (size_t)fp.No * fp.No * s0, ns, rows, st);
+        }
+        if (!stream) RAFT_CUDA(cudaStreamSynchronize(st));
+    } catch (const CudaFail &) {
+    }
+    return has_error() ? 1 : 0;
+}
+
+// --- lowpass --------------------------------------------------------------
+// Reference: getFilterLowPassMultiGPU, cuda/src/processing/filters/low_pass.cu:84-141
+void getFilterLowPassMultiGPU(int *gpus, int ngpus, float *tomogram, float *paramf, int *parami)
+{
+    clear_error();
+    FbpConfig cfg;
+    if (!parse_fbp_arrays(paramf, parami, cfg, false)) return;
+    if (!check_gpus(gpus, ngpus)) return;
+    if (!tomogram) {
+        set_error("null data pointer");
+        return;
+    }
+    const size_t ps = (size_t)cfg.nangles * cfg.nrays;
+    split_slabs(gpus, ngpus, cfg.nslices,
+                [&](int dev, int start, int n) { lowpass_host_slab(cfg, dev, tomogram + ps * start, n); });
+}
+
+// --- Radon ----------------------------------------------------------------
+// Reference: getRadonRTMultiGPU, cuda/src/geometries/parallel/forward_methods/radon_rt.cu:252-295
+void getRadonRTMultiGPU(int *gpus, int ngpus, float *tomogram, float *phantom, float *angles, int sizex, int sizey,
+                        int nrays, int nangles, int nslices, float ax, float ay)
+{
+    clear_error();
+    if (sizex < 2 || sizey < 2 || nrays < 1 || nangles < 1 || nslices < 0) {
+        set_error("invalid Radon sizes");
+        return;
+    }
+    if (!check_gpus(gpus, ngpus)) return;
+    if (!tomogram || !phantom || !angles) {
+        set_error("null data pointer");
+        return;
+    }
+    split_slabs(gpus, ngpus, nslices, [&](int dev, int start, int n) {
+        radon_host_slab(dev, tomogram + (size_t)start * nrays * nangles, phantom + (size_t)start * sizex * sizey,
+                        angles, sizex, sizey, nrays, nangles, n, ax, ay);
+    });
+}
+
+// --- EM -------------------------------------------------------------------
+static void em_common(int kind, int *gpus, int ngpus, float *obj, const float *data, const float *flat,
+                      const float *angles, const float *paramf, const int *parami)
+{
+    clear_error();
+    EmConfig cfg;
+    if (!parse_em_arrays(paramf, parami, cfg)) return;
+    if (!check_gpus(gpus, ngpus)) return;
+    if (!obj || !data || !angles || (kind == 0 && !flat)) {
+        set_error("null data pointer");
+        return;
+    }
+    const size_t ops = (size_t)cfg.objsize * cfg.objsize, dps = (size_t)cfg.nangles * cfg.nrays;
+    split_slabs(gpus, ngpus, cfg.nslices, [&](int dev, int start, int n) {
+        em_host_slab(cfg, kind, dev, obj + ops * start, data + dps * start,
+                     flat ? flat + (size_t)cfg.nrays * start : nullptr, angles, n, false);
+    });
+}
+
+// Reference: get_tEM_RT_MultiGPU, cuda/src/geometries/parallel/reconstruction_methods/em_rt.cu:12-84
+void get_tEM_RT_MultiGPU(int *gpus, int ngpus, float *obj, float *count, float *flat, float *angles, float *paramf,
+                         int *parami)
+{
+    em_common(0, gpus, ngpus, obj, count, flat, angles, paramf, parami);
+}
+
+// Reference: get_eEM_RT_MultiGPU, em_rt.cu:201-262
+void get_eEM_RT_MultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *angles, float *paramf,
+                         int *parami)
+{
+    em_common(1, gpus, ngpus, obj, tomogram, nullptr, angles, paramf, parami);
+}
+
+// Single-GPU EM with per-iteration FP64 metrics [niter][nslices][3]
+// (sum (model-data)^2, sum data^2, negative log-likelihood) copied to the
+// host buffer `metrics` (may be NULL).  kind 0 = tEM, 1 = eEM.
+int raft_em_ext(int kind, int gpu, float *obj, const float *data, const float *flat, const float *angles, int nrays,
+                int nangles, int nslices, int niter, double *metrics, int use_graph)
+{
+    clear_error();
+    int parami[10] = {nrays, nangles, nslices, nrays, 0, 0, 0, 1, niter, 0};
+    EmConfig cfg;
+    if (!parse_em_arrays(nullptr, parami, cfg)) return 1;
+    if (!check_gpus(&gpu, 1)) return 1;
+    if (kind != 0 && kind != 1) {
+        set_error("raft_em_ext: kind must be 0 (tEM) or 1 (eEM)");
+        return 1;
+    }
+    try {
+        DeviceState &ds = device_state(gpu);
+        std::lock_guard<std::mutex> lk(ds.mtx);
+        RAFT_CUDA(cudaSetDevice(gpu));
+        ds.ensure();
+        EmPrepared ep = prepare_em(cfg);
+        cudaStream_t st = ds.s_comp;
+        const size_t dps = (size_t)nangles * nrays, ops = (size_t)nrays * nrays;
+        float *d_data = (float *)ds.sino[0].get(dps * nslices * sizeof(float));
+        float *d_obj = (float *)ds.img[0].get(ops * nslices * sizeof(float));
+        float *d_flat = (float *)ds.flat.get((size_t)nrays * nslices * sizeof(float) + 16);
+        double *d_met = metrics ? (double *)ds.metrics.get(sizeof(double) * 3 * (size_t)nslices * niter + 8) : nullptr;
+        RAFT_CUDA(cudaMemcpyAsync(d_data, data, dps * nslices * sizeof(float), cudaMemcpyHostToDevice, st));
+        RAFT_CUDA(cudaMemcpyAsync(d_obj, obj, ops * nslices * sizeof(float), cudaMemcpyHostToDevice, st));
+        if (kind == 0)
+            RAFT_CUDA(cudaMemcpyAsync(d_flat, flat, (size_t)nrays * nslices * sizeof(float), cudaMemcpyHostToDevice,
+                                      st));
+        em_chunk(ds, ep, kind, d_data, d_flat, angles, d_obj, nslices, d_met, use_graph != 0, st);
+        RAFT_CUDA(cudaMemcpyAsync(obj, d_obj, ops * nslices * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (metrics)
+            RAFT_CUDA(cudaMemcpyAsync(metrics, d_met, sizeof(double) * 3 * (size_t)nslices * niter,
+                                      cudaMemcpyDeviceToHost, st));
+        RAFT_CUDA(cudaStreamSynchronize(st));
+    } catch (const CudaFail &) {
+    }
+    return has_error() ? 1 : 0;
+}
+
+// Device-resident EM on one GPU (all pointers device, angles host).
+int raft_em_device(int kind, int gpu, float *d_obj, const float *d_data, const float *d_flat, const float *angles,
+                   int nrays, int nangles, int nslices, int niter, double *d_metrics, int use_graph, void *stream)
+{
+    clear_error();
+    int parami[10] = {nrays, nangles, nslices, nrays, 0, 0, 0, 1, niter, 0};
+    EmConfig cfg;
+    if (!parse_em_arrays(nullptr, parami, cfg)) return 1;
+    if (!check_gpus(&gpu, 1)) return 1;
+    try {
+        DeviceState &ds = device_state(gpu);
+        std::lock_guard<std::mutex> lk(ds.mtx);
+        RAFT_CUDA(cudaSetDevice(gpu));
+        ds.ensure();
+        EmPrepared ep = prepare_em(cfg);
+        cudaStream_t st = stream ? (cudaStream_t)stream : ds.s_comp;
+        em_chunk(ds, ep, kind, d_data, d_flat, angles, d_obj, nslices, d_metrics, use_graph != 0, st);
+    } catch (const CudaFail &) {
+    }
+    return has_error() ? 1 : 0;
+}
+
+// Adjacent reference exports that this library does not implement: they
+// record an error instead of running (rafttypes.py binds them if present).
+void getBSTMultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *angles, float *paramf, int *parami,
+                    int nstreams)
+{
+    (void)gpus; (void)ngpus; (void)obj; (void)tomogram; (void)angles; (void)paramf; (void)parami; (void)nstreams;
+    clear_error();
+    set_error("getBSTMultiGPU is not implemented by this library (use method='RT')");
+}
+
+void get_tEM_FQ_MultiGPU(int *gpus, int ngpus, float *obj, float *count, float *flat, float *angles, float *paramf,
+                         int *parami)
+{
+    (void)gpus; (void)ngpus; (void)obj; (void)count; (void)flat; (void)angles; (void)paramf; (void)parami;
+    clear_error();
+    set_error("get_tEM_FQ_MultiGPU is not implemented by this library (use method='tEMRT')");
+}
+
+}  // extern "C"

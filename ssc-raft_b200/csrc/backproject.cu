@@ -1,0 +1,446 @@
+// backproject.cu -- the backprojector for FBP and for the EM iterations.
+//
+// Reference kernels restated (cnpem/ssc-raft):
+//   * FBP  BackProjection_SS, cuda/src/geometries/parallel/reconstruction_methods/fbp.cu:8-76
+//     x = xmin + i*dx, t = x*cos - y*sin, sample = sino[(int)((t - tmin)/dt)]
+//     on the padded (N*(1+pad))^2 grid, then the centre N x N is cropped
+//     (padding.cu:245-268).  Here only the centre window is computed; for
+//     those pixels the arithmetic is identical.
+//   * EM   kernel_backprojection / kernel_backprojectionWithUpdate,
+//     cuda/src/geometries/parallel/reconstruction_methods/kernels/em_RT_kernel.cu:92-142,249-300
+//     x = -1 + i*2/(N-1), t = x*cos + y*sin, T = (int)((t + 1)/dt),
+//     optional update x <- x * BP / den.
+//   * FBP with linear interpolation (north-star operator): same pixel and
+//     detector grid, the sample at fractional bin u = (t - tmin)/dt is
+//     interpolated between bins floor(u) and floor(u)+1 (zero outside).
+//
+// B200 design.  A CTA owns a 64 x 32 pixel tile of one slice (256 threads,
+// 8 pixels per thread spread so that every warp touches an 8 x 4 pixel
+// block -> one shared-memory wavefront per gather).  Angles stream through a
+// two-stage pipeline of 32-angle blocks: for every angle, warp 0 computes the
+// detector window the tile can reach and one lane issues a 1-D bulk copy
+// (cp.async.bulk, the TMA engine) of that window from the filtered rows in
+// HBM/L2 into shared memory, completing on an mbarrier; while block s is
+// gathered, block s+1 is in flight.  The filtered rows already carry the
+// angle step, so the inner loop is: position, round, gather, interpolate,
+// accumulate.  All waits are bounded and report through a device flag.
+#include "raft.hpp"
+#include "ptx.hpp"
+#include "profile.hpp"
+
+#include <cmath>
+#include <algorithm>
+
+namespace raft {
+
+struct __align__(16) AngleParam {
+    float a, b, c;
+    int d;
+};
+
+struct BpArgs {
+    const unsigned char *filt;   // window rows [nslices*nangles][Wg] elements
+    float *img;                  // [nslices][No][No]
+    const float *den;            // update denominator (EM), same layout as img
+    int No, nangles, nslices;
+    int wlo, Wg, W, esize;
+    // FBP reference arithmetic
+    float xmin, ymin, dx, dy, tmin, dt;
+    int offo;
+    // EM reference arithmetic
+    float xymin, dxy;
+    // linear geometry
+    double c0, ratio, u0;
+    const float *cs, *sn;        // FP32 tables (fast intrinsics, as the reference)
+    const double *csd, *snd;     // FP64 tables
+    int *err;
+    int update;                  // 0: store, 1: img = img * acc / den
+};
+
+constexpr uint32_t kWaitLimit = 1u << 24;
+constexpr int kParamBytes = 2 * BP_AB * (int)sizeof(AngleParam);
+constexpr int kWinOffset = 128 + kParamBytes;   // bytes before the windows
+
+static_assert(kWinOffset % 128 == 0, "window area alignment");
+
+// ------------------------------------------------------------------------
+// per-angle window base (warp 0, one lane per angle)
+// ------------------------------------------------------------------------
+template <int GEOM>
+__device__ __forceinline__ void angle_param(const BpArgs &p, int a, int x0, int y0, AngleParam &ap, int &base)
+{
+    const int align = 16 / p.esize;
+    int lo;
+    if constexpr (GEOM == GEOM_FBP_LIN) {
+        const double c = p.csd[a], s = -p.snd[a] * p.ratio;
+        const double v00 = ((double)x0 + p.c0) * c + ((double)y0 + p.c0) * s + p.u0;
+        const double vmin = v00 + fmin(0.0, (BP_TX - 1) * c) + fmin(0.0, (BP_TY - 1) * s);
+        lo = (int)floor(vmin) - 1;
+        int b = lo - ((lo % align) + align) % align;
+        b = max(0, min(b, p.Wg - p.W));
+        base = b;
+        ap.a = (float)(v00 - (double)b);
+        ap.b = (float)c;
+        ap.c = (float)s;
+        ap.d = b;
+    } else {
+        const float c = p.cs[a], s = p.sn[a];
+        int tmin_i = 0x7fffffff;
+#pragma unroll
+        for (int cy = 0; cy < 2; cy++)
+#pragma unroll
+            for (int cx = 0; cx < 2; cx++) {
+                const int i = x0 + cx * (BP_TX - 1), j = y0 + cy * (BP_TY - 1);
+                int ti;
+                if constexpr (GEOM == GEOM_FBP_REF) {
+                    const int ip = i + p.offo, jp = j + p.offo;
+                    float x = p.xmin + ip * p.dx;
+                    float y = p.ymin + jp * p.dy;
+                    float t = x * c - y * s;
+                    ti = (int)((t - p.tmin) / p.dt);
+                } else {
+                    float x = p.xymin + i * p.dxy;
+                    float y = p.xymin + j * p.dxy;
+                    float t = x * c + y * s;
+                    ti = (int)((t - p.tmin) / p.dt);
+                }
+                tmin_i = min(tmin_i, ti);
+            }
+        lo = tmin_i - 1 - p.wlo;
+        int b = lo - ((lo % align) + align) % align;
+        b = max(0, min(b, p.Wg - p.W));
+        base = b;
+        ap.a = c;
+        ap.b = s;
+        ap.c = 0.f;
+        ap.d = p.wlo + b;   // padded-bin index of window element 0
+    }
+}
+
+// ------------------------------------------------------------------------
+// element fetch
+// ------------------------------------------------------------------------
+template <int STORE>
+__device__ __forceinline__ float lerp_fetch(const unsigned char *w, int k, float f)
+{
+    if constexpr (STORE == STORE_PAIR_F32) {
+        const float2 sd = reinterpret_cast<const float2 *>(w)[k];
+        return fmaf(f, sd.y, sd.x);
+    } else {
+        const uint32_t bits = reinterpret_cast<const uint32_t *>(w)[k];
+        const float mid = __uint_as_float(bits << 16);
+        const float dif = __uint_as_float(bits & 0xffff0000u);
+        return fmaf(f, dif, mid);
+    }
+}
+
+// ------------------------------------------------------------------------
+// kernel
+// ------------------------------------------------------------------------
+template <int GEOM, int STORE>
+__global__ void __launch_bounds__(BP_THREADS)
+bp_kernel(const BpArgs p)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    AngleParam *prm = reinterpret_cast<AngleParam *>(smem + 128);
+    unsigned char *win = smem + kWinOffset;
+    const int esize = (STORE == STORE_PAIR_F32) ? 8 : 4;
+    const int W = p.W;
+    const int stage_bytes = BP_AB * W * esize;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int x0 = blockIdx.x * BP_TX, y0 = blockIdx.y * BP_TY, slice = blockIdx.z;
+    const int A = p.nangles;
+    const int nst = (A + BP_AB - 1) / BP_AB;
+
+    // thread -> pixels: warp covers an 8 x 4 block per (i, j)
+    const int lx = lane & 7, ly = lane >> 3;
+    const int wx = warp & 1, wy = warp >> 1;
+    int li[4], lj[2];
+#pragma unroll
+    for (int i = 0; i < 4; i++) li[i] = wx * 32 + lx + 8 * i;
+#pragma unroll
+    for (int j = 0; j < 2; j++) lj[j] = wy * 8 + ly + 4 * j;
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    const unsigned char *rows = p.filt + (size_t)slice * A * p.Wg * esize;
+
+    auto issue = [&](int s, int b) {
+        // warp 0 only
+        const int a = s * BP_AB + lane;
+        const int na = min(BP_AB, A - s * BP_AB);
+        int base = 0;
+        if (lane < na) {
+            AngleParam ap;
+            angle_param<GEOM>(p, a, x0, y0, ap, base);
+            prm[b * BP_AB + lane] = ap;
+        }
+        if (lane == 0) {
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&bars[b], (uint32_t)(na * W * esize));
+        }
+        __syncwarp();
+        if (lane < na)
+            bulk_g2s(win + (size_t)b * stage_bytes + (size_t)lane * W * esize,
+                     rows + ((size_t)a * p.Wg + base) * esize, (uint32_t)(W * esize), &bars[b]);
+    };
+
+    if (warp == 0) issue(0, 0);
+    __syncthreads();
+
+    float acc[2][4];
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) acc[j][i] = 0.f;
+
+    // per-thread coordinates in the reference's float arithmetic
+    float xr[4], yr[2];
+    if constexpr (GEOM == GEOM_FBP_REF) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) { const int ip = x0 + li[i] + p.offo; xr[i] = p.xmin + ip * p.dx; }
+#pragma unroll
+        for (int j = 0; j < 2; j++) { const int jp = y0 + lj[j] + p.offo; yr[j] = p.ymin + jp * p.dy; }
+    } else if constexpr (GEOM == GEOM_EM_REF) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) { const int ip = x0 + li[i]; xr[i] = p.xymin + ip * p.dxy; }
+#pragma unroll
+        for (int j = 0; j < 2; j++) { const int jp = y0 + lj[j]; yr[j] = p.xymin + jp * p.dxy; }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; i++) xr[i] = (float)li[i];
+#pragma unroll
+        for (int j = 0; j < 2; j++) yr[j] = (float)lj[j];
+    }
+
+    bool ok = true;
+    for (int s = 0; s < nst && ok; s++) {
+        const int b = s & 1;
+        if (s + 1 < nst && warp == 0) issue(s + 1, b ^ 1);
+        if (!mbar_wait_bounded(&bars[b], (uint32_t)((s >> 1) & 1), kWaitLimit)) {
+            ok = false;
+            if (p.err) atomicExch(p.err, 1);
+            break;
+        }
+        const int na = min(BP_AB, A - s * BP_AB);
+        const unsigned char *wb = win + (size_t)b * stage_bytes;
+        const AngleParam *pb = prm + b * BP_AB;
+        for (int al = 0; al < na; al++) {
+            const AngleParam ap = pb[al];
+            const unsigned char *w = wb + (size_t)al * W * esize;
+            if constexpr (GEOM == GEOM_FBP_LIN) {
+                const float MAGIC = 12582912.0f;   // 1.5 * 2^23: fadd rounds to an integer
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const float vrow = fmaf(yr[j], ap.c, ap.a);
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const float v = fmaf(xr[i], ap.b, vrow);
+                        const float m = __fadd_rn(v, MAGIC);
+                        const int k = __float_as_int(m) - 0x4B400000;
+                        const float f = __fsub_rn(v, __fsub_rn(m, MAGIC));
+                        acc[j][i] += lerp_fetch<STORE>(w, min((unsigned)k, (unsigned)(W - 1)), f);
+                    }
+                }
+            } else if constexpr (GEOM == GEOM_FBP_REF) {
+                const float c = ap.a, sn = ap.b;
+                const int wbase = ap.d;
+                const float *wf = reinterpret_cast<const float *>(w);
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        float t = xr[i] * c - yr[j] * sn;
+                        int ti = (int)((t - p.tmin) / p.dt);
+                        acc[j][i] += wf[min((unsigned)(ti - wbase), (unsigned)(W - 1))];
+                    }
+            } else {
+                const float c = ap.a, sn = ap.b;
+                const int wbase = ap.d;
+                const float *wf = reinterpret_cast<const float *>(w);
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        float t = xr[i] * c + yr[j] * sn;
+                        int ti = (int)((t - p.tmin) / p.dt);
+                        acc[j][i] += wf[min((unsigned)(ti - wbase), (unsigned)(W - 1))];
+                    }
+            }
+        }
+        __syncthreads();
+    }
+    if (!ok) return;
+
+    float *out = p.img + (size_t)slice * p.No * p.No;
+    const float *den = p.den ? p.den + (size_t)slice * p.No * p.No : nullptr;
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int X = x0 + li[i], Y = y0 + lj[j];
+            if (X < p.No && Y < p.No) {
+                const size_t o = (size_t)Y * p.No + X;
+                if (p.update) out[o] = out[o] * acc[j][i] / den[o];
+                else out[o] = acc[j][i];
+            }
+        }
+}
+
+// ------------------------------------------------------------------------
+// angle tables: the reference computes sin/cos with the fast intrinsics,
+// __sinf/__cosf for FBP (opt.cu:187-194) and __sincosf for EM
+// (em_RT_kernel.cu:120); angle steps as em_RT_kernel.cu:122-126 / fbp.cu:61-64.
+// ------------------------------------------------------------------------
+__global__ void angle_table_kernel(const float *angles, int A, float *cs, float *sn, float *wt, int em)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= A) return;
+    if (em) {
+        float s, c;
+        __sincosf(angles[k], &s, &c);
+        cs[k] = c;
+        sn[k] = s;
+    } else {
+        sn[k] = __sinf(angles[k]);
+        cs[k] = __cosf(angles[k]);
+    }
+    if (wt) {
+        float d;
+        if (A == 1) d = 1.0f;
+        else if (k == A - 1) d = angles[k] - angles[k - 1];
+        else d = angles[k + 1] - angles[k];
+        // FBP angular correction for scans beyond pi (fbp.cu:24-28); EM has none
+        float scale = 1.0f;
+        if (!em && angles[A - 1] > float(M_PI)) scale = float(M_PI) / angles[A - 1];
+        wt[k] = d * scale;
+    }
+}
+
+void launch_angle_tables(const float *d_angles, int nangles, float *d_cos, float *d_sin, float *d_wt,
+                         int em_sincos, cudaStream_t st)
+{
+    count_launch();
+    angle_table_kernel<<<(nangles + 127) / 128, 128, 0, st>>>(d_angles, nangles, d_cos, d_sin, d_wt,
+                                                               em_sincos);
+    RAFT_CUDA(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------
+// host: window planning and launch
+// ------------------------------------------------------------------------
+static int floor_to(int v, int a) { return v - (((v % a) + a) % a); }
+static int ceil_to(int v, int a) { return floor_to(v + a - 1, a); }
+
+WindowLayout plan_window(const BpPlanInput &in)
+{
+    WindowLayout L;
+    const int esize = store_bytes(in.store);
+    const int align = 16 / esize;
+    L.align = align;
+    const int Xext = ((in.No + BP_TX - 1) / BP_TX) * BP_TX;
+    const int Yext = ((in.No + BP_TY - 1) / BP_TY) * BP_TY;
+    double span, lo, hi;
+    if (in.geometry == GEOM_EM_REF) {
+        const double dxy = in.dxy, dt = in.dt;
+        const double xm = std::max(1.0, std::fabs(-1.0 + (Xext - 1) * dxy));
+        const double ym = std::max(1.0, std::fabs(-1.0 + (Yext - 1) * dxy));
+        const double Rt = std::sqrt(xm * xm + ym * ym);
+        lo = (-Rt + 1.0) / dt;
+        hi = (Rt + 1.0) / dt;
+        span = std::sqrt(std::pow((BP_TX - 1) * dxy, 2) + std::pow((BP_TY - 1) * dxy, 2)) / dt;
+    } else {
+        // x = xmin + (i + offo) * dx for i in [0, Xext)
+        const double xa = std::fabs(in.xmin + (double)in.offo * in.dx);
+        const double xb = std::fabs(in.xmin + (double)(in.offo + Xext - 1) * in.dx);
+        const double ya = std::fabs(in.ymin + (double)in.offo * in.dy);
+        const double yb = std::fabs(in.ymin + (double)(in.offo + Yext - 1) * in.dy);
+        const double xm = std::max(xa, xb), ym = std::max(ya, yb);
+        const double Rt = std::sqrt(xm * xm + ym * ym);
+        lo = (-Rt - in.tmin) / in.dt;
+        hi = (Rt - in.tmin) / in.dt;
+        span = std::sqrt(std::pow((BP_TX - 1) * in.dx, 2) + std::pow((BP_TY - 1) * in.dy, 2)) / in.dt;
+    }
+    // staged window: tile span, +1 inclusive, 1 bin margin each side,
+    // rounding of the aligned start, 1 extra for the lin pair index rounding
+    L.W = ceil_to((int)std::ceil(span) + 1 + 2 + (align - 1) + 2, align);
+    L.wlo = floor_to((int)std::floor(lo) - 4 - align, align);
+    const int whi = (int)std::ceil(hi) + 4 + L.W + align;
+    L.Wg = ceil_to(whi - L.wlo, align);
+    return L;
+}
+
+template <int GEOM, int STORE>
+static void launch_bp_t(const BpArgs &a, int nslices, cudaStream_t st)
+{
+    const int esize = (STORE == STORE_PAIR_F32) ? 8 : 4;
+    const size_t smem = kWinOffset + 2 * (size_t)BP_AB * a.W * esize;
+    static thread_local int configured = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured != dev) {
+        RAFT_CUDA(cudaFuncSetAttribute(bp_kernel<GEOM, STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       200 * 1024));
+        configured = dev;
+    }
+    RAFT_CHECK(smem <= 200 * 1024, "backprojector: staged window too large");
+    dim3 grid((a.No + BP_TX - 1) / BP_TX, (a.No + BP_TY - 1) / BP_TY, nslices);
+    ProfScope ps(PROF_BACKPROJECT, st);
+    bp_kernel<GEOM, STORE><<<grid, BP_THREADS, smem, st>>>(a);
+    RAFT_CUDA(cudaGetLastError());
+}
+
+void launch_backproject(const BpLaunch &bl, cudaStream_t st)
+{
+    if (bl.nslices <= 0 || bl.nangles <= 0) return;
+    BpArgs a;
+    a.filt = reinterpret_cast<const unsigned char *>(bl.filt);
+    a.img = bl.img;
+    a.den = bl.den;
+    a.No = bl.No;
+    a.nangles = bl.nangles;
+    a.nslices = bl.nslices;
+    a.wlo = bl.win.wlo;
+    a.Wg = bl.win.Wg;
+    a.W = bl.win.W;
+    a.esize = store_bytes(bl.store);
+    a.xmin = bl.geo.xmin;
+    a.ymin = bl.geo.ymin;
+    a.dx = bl.geo.dx;
+    a.dy = bl.geo.dy;
+    a.tmin = bl.geo.tmin;
+    a.dt = bl.geo.dt;
+    a.offo = bl.geo.offo;
+    a.xymin = -1.0f;
+    a.dxy = bl.geo.dxy;
+    a.c0 = bl.geo.c0;
+    a.ratio = bl.geo.ratio;
+    a.u0 = bl.geo.u0;
+    a.cs = bl.cs;
+    a.sn = bl.sn;
+    a.csd = bl.csd;
+    a.snd = bl.snd;
+    a.err = bl.err;
+    a.update = bl.den ? 1 : 0;
+    switch (bl.geometry) {
+    case GEOM_FBP_REF:
+        launch_bp_t<GEOM_FBP_REF, STORE_F32>(a, bl.nslices, st);
+        break;
+    case GEOM_EM_REF:
+        launch_bp_t<GEOM_EM_REF, STORE_F32>(a, bl.nslices, st);
+        break;
+    default:
+        if (bl.store == STORE_PAIR_BF16) launch_bp_t<GEOM_FBP_LIN, STORE_PAIR_BF16>(a, bl.nslices, st);
+        else launch_bp_t<GEOM_FBP_LIN, STORE_PAIR_F32>(a, bl.nslices, st);
+        break;
+    }
+}
+
+}  // namespace raft

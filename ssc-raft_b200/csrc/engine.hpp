@@ -1,0 +1,103 @@
+// engine.hpp -- per-device execution engine: cached device workspaces,
+// pinned staging, filter plans, and the chunked FBP / EM / Radon / lowpass
+// pipelines behind the C-ABI.
+#pragma once
+#include "raft.hpp"
+
+#include <mutex>
+#include <vector>
+
+namespace raft {
+
+// Grow-only device buffer owned by a per-device workspace.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    void *get(size_t need);      // (re)allocates when too small; contents undefined
+    void release();
+};
+
+struct PinBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    void *get(size_t need);
+    void release();
+};
+
+// Everything one device keeps between calls.  Calls on the same device are
+// serialised by `mtx` (the reference is not re-entrant per device either).
+struct DeviceState {
+    int device = 0;
+    std::mutex mtx;
+    cudaStream_t s_comp = nullptr, s_h2d = nullptr, s_d2h = nullptr;
+    DevBuf sino[2], img[2], rows, den, flat, data, angles, tabs, metrics, err;
+    PinBuf pin_in[2], pin_out[2];
+    cudaEvent_t ev_h2d[2] = {}, ev_comp[2] = {}, ev_d2h[2] = {};
+    bool init = false;
+    void ensure();
+};
+
+DeviceState &device_state(int device);
+
+// Filter plan cache (per device, keyed by every spectrum input).
+const FilterPlan &cached_filter_plan(int device, int geometry, int ftype, int N, int pad, double paganin,
+                                     double reg, double offset, double pixel);
+
+// Host memcpy with a few threads (staging to / from pinned buffers).
+void parallel_memcpy(void *dst, const void *src, size_t bytes);
+
+// --- FBP ---------------------------------------------------------------
+struct FbpPrepared {
+    FbpConfig cfg;
+    int No = 0, Np = 0, Npo = 0;
+    WindowLayout win;
+    BpGeo geo;
+    const FilterPlan *plan = nullptr;
+};
+
+FbpPrepared prepare_fbp(const FbpConfig &cfg, int device);
+
+// Device-resident FBP of `nslices` slices (filter + backprojection), using
+// the device workspace for the window rows; tables must be set up by
+// fbp_tables().  d_sino [nslices][A][N] -> d_img [nslices][No][No].
+struct FbpTables {
+    float *cs = nullptr, *sn = nullptr, *wt = nullptr;
+    double *csd = nullptr, *snd = nullptr;
+    int *err = nullptr;
+};
+FbpTables fbp_tables(DeviceState &ds, const FbpPrepared &fp, const float *h_angles, cudaStream_t st);
+void fbp_chunk(DeviceState &ds, const FbpPrepared &fp, const FbpTables &tb, const float *d_sino, float *d_img,
+               int nslices, void *d_rows, cudaStream_t st);
+size_t fbp_rows_bytes(const FbpPrepared &fp, int nslices);
+
+// Host-buffer FBP of one slab on one device (the body of getFBPMultiGPU).
+void fbp_host_slab(const FbpConfig &cfg, int device, float *obj, const float *tomo, const float *angles,
+                   int nslices);
+
+// --- lowpass -------------------------------------------------------------
+void lowpass_host_slab(const FbpConfig &cfg, int device, float *tomo, int nslices);
+
+// --- Radon ---------------------------------------------------------------
+void radon_host_slab(int device, float *proj, const float *img, const float *angles, int nx, int ny,
+                     int nrays, int nangles, int nslices, float ax, float ay);
+
+// --- EM ------------------------------------------------------------------
+struct EmPrepared {
+    EmConfig cfg;
+    WindowLayout win;
+    BpGeo geo;
+};
+EmPrepared prepare_em(const EmConfig &cfg);
+
+// Device-resident EM of one chunk.  kind 0 = tEM (data = exp(-input) counts,
+// flat [nslices][nrays]), 1 = eEM.  obj is in/out.  metrics (optional) is a
+// device array [niter][nslices][3] of FP64 sums, filled per iteration.
+// use_graph captures the iteration loop as one CUDA graph.
+void em_chunk(DeviceState &ds, const EmPrepared &ep, int kind, const float *d_data, const float *d_flat,
+              const float *h_angles, float *d_obj, int nslices, double *d_metrics, bool use_graph,
+              cudaStream_t st);
+
+void em_host_slab(const EmConfig &cfg, int kind, int device, float *obj, const float *data, const float *flat,
+                  const float *angles, int nslices, bool flat_by_angle);
+
+}  // namespace raft

@@ -1,0 +1,206 @@
+// raft.hpp -- shared host/device definitions of the B200 parallel-beam
+// reconstruction library (libraft.so).
+//
+// Layouts (all C-contiguous, as in ssc-raft):
+//   sinogram  [slices][angles][rays]   float32
+//   image     [slices][N][N]           float32
+//   window rows [slices*angles][Wg]    the detector bins that one slice's
+//             image can reach, with zero margins, each element already
+//             multiplied by the angle step dtheta_a (and by the >pi angular
+//             rescale), stored as float32 (nearest-sample operators), as
+//             (mid, diff) float2 pairs or as (mid, diff) bf16x2 pairs
+//             (linear interpolation: value(u) = mid + (u - k - 1/2) * diff).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cstdint>
+#include <cstddef>
+#include <string>
+
+namespace raft {
+
+// ----------------------------------------------------------------- status --
+// The reference library calls exit(-1) on any CUDA error
+// (cuda/inc/common/logerror.hpp:59-67).  Here every failure is recorded in a
+// thread-local status that raft_last_error() returns; nothing exits.
+void set_error(const std::string &msg);
+bool has_error();
+std::string get_error();
+void clear_error();
+
+struct CudaFail {};
+
+#define RAFT_CUDA(call)                                                         \
+    do {                                                                        \
+        cudaError_t _e = (call);                                                \
+        if (_e != cudaSuccess) {                                                \
+            ::raft::set_error(std::string(#call) + ": " + cudaGetErrorString(_e) \
+                              + " (" + __FILE__ + ":" + std::to_string(__LINE__) + ")"); \
+            throw ::raft::CudaFail();                                           \
+        }                                                                       \
+    } while (0)
+
+#define RAFT_CHECK(cond, msg)                                                   \
+    do {                                                                        \
+        if (!(cond)) {                                                          \
+            ::raft::set_error(std::string(msg));                                \
+            throw ::raft::CudaFail();                                           \
+        }                                                                       \
+    } while (0)
+
+// ----------------------------------------------------------------- enums --
+enum Geometry : int {
+    GEOM_FBP_REF = 0,   // fbp.cu:38-72: nearest sample by truncation, pixel units
+    GEOM_FBP_LIN = 1,   // same grid, linear interpolation (north-star operator)
+    GEOM_EM_REF  = 2,   // em_RT_kernel.cu:92-142: [-1,1] grid, truncation
+};
+
+enum Store : int {
+    STORE_F32       = 0,  // one float per bin (nearest-sample operators)
+    STORE_PAIR_F32  = 1,  // (mid, diff) float2 per bin (linear interpolation)
+    STORE_PAIR_BF16 = 2,  // (mid, diff) bf16x2 per bin (linear interpolation)
+};
+
+inline int store_bytes(int store) { return store == STORE_PAIR_F32 ? 8 : 4; }
+
+// Filter ids: the reference enum (cuda/inc/processing/filters.hpp:26-37)
+// plus 9 = Shepp-Logan for the linear-interpolation mode.
+enum FilterType : int {
+    FILTER_NONE = 0, FILTER_GAUSSIAN = 1, FILTER_LORENTZ = 2, FILTER_COSINE = 3,
+    FILTER_RECTANGLE = 4, FILTER_HANN = 5, FILTER_HAMMING = 6, FILTER_RAMP = 7,
+    FILTER_DIFFERENTIAL = 8, FILTER_SHEPP_LOGAN = 9,
+};
+
+// ----------------------------------------------------------- filter plan --
+struct FilterPlan {
+    int N = 0, Np = 0, pad = 0, off = 0;
+    int fft = 0;                 // 1: mixed-radix FFT path, 0: direct circular convolution
+    int nradix = 0;
+    int radix[24] = {};
+    int threads = 0;             // CTA size of the FFT kernel
+    float2 *d_H = nullptr;       // full Hermitian-extended spectrum incl. 1/(Np*pixel)
+    float2 *d_tw = nullptr;      // exp(-2 pi i m / Np)
+    float *d_h = nullptr;        // impulse response (direct path)
+    bool skip = false;           // reference 'none' filter: pad + copy only
+};
+
+bool build_filter_plan(FilterPlan &plan, int geometry, int ftype, int N, int pad, double paganin,
+                       double reg, double offset, double pixel, int device);
+void release_filter_plan(FilterPlan &plan);
+void filter_spectrum_host(int geometry, int ftype, int Np, double paganin, double reg,
+                          double offset, double pixel, double *hre, double *him);
+
+struct FilterLaunch {
+    const float *sino = nullptr;   // [nrows][N]
+    void *out = nullptr;           // [nrows][Wg] window rows, or [nrows][N] (lowpass)
+    const float *wt = nullptr;     // per-angle weight, indexed row % nangles
+    int nrows = 0, nangles = 1;
+    int wlo = 0, Wg = 0;
+    int store = STORE_F32;
+    int out_padded = 0;            // lowpass: centre N bins, unweighted float
+};
+
+void launch_filter(const FilterPlan &plan, const FilterLaunch &fl, cudaStream_t st);
+
+// ------------------------------------------------------- window layout --
+// Which stored bins a backprojection needs, and how a CTA tile stages them.
+struct WindowLayout {
+    int wlo = 0;      // padded-bin index of stored element 0
+    int Wg = 0;       // stored elements per row (multiple of the 16-byte granule)
+    int W = 0;        // staged elements per angle per tile
+    int align = 4;    // element alignment of a staged window start
+};
+
+// Launch-time tile configuration of the backprojector.
+constexpr int BP_THREADS = 256;
+constexpr int BP_TX = 64;     // tile width  (pixels)
+constexpr int BP_TY = 32;     // tile height (pixels)
+constexpr int BP_AB = 32;     // angles per pipeline stage
+
+// Geometry constants of one backprojection, in the reference's FP32
+// arithmetic (FBP: fbp.cu:38-44; EM: em_RT_kernel.cu:97-102).
+struct BpGeo {
+    float xmin = 0, ymin = 0, dx = 1, dy = 1, tmin = 0, dt = 1;  // FBP; EM uses tmin=-1, dt=2/(n-1)
+    int offo = 0;          // padded-grid index of output pixel 0 (FBP)
+    float dxy = 0;         // EM pixel step 2/(N-1)
+    double c0 = 0;         // linear geometry: pixel i sits at (i + c0)*pixel_x
+    double ratio = 1;      // pixel_y / pixel_x
+    double u0 = 0;         // Np/2 - wlo - 0.5
+};
+
+struct BpPlanInput {
+    int geometry = GEOM_FBP_REF, store = STORE_F32, No = 0;
+    float xmin = 0, ymin = 0, dx = 1, dy = 1, tmin = 0, dt = 1;
+    int offo = 0;
+    float dxy = 0;
+};
+
+WindowLayout plan_window(const BpPlanInput &in);
+
+struct BpLaunch {
+    const void *filt = nullptr;   // window rows [nslices*nangles][Wg]
+    float *img = nullptr;         // [nslices][No][No]
+    const float *den = nullptr;   // EM update denominator; nullptr = plain store
+    int No = 0, nangles = 0, nslices = 0;
+    int geometry = GEOM_FBP_REF, store = STORE_F32;
+    WindowLayout win;
+    BpGeo geo;
+    const float *cs = nullptr, *sn = nullptr;     // FP32 angle tables
+    const double *csd = nullptr, *snd = nullptr;  // FP64 angle tables
+    int *err = nullptr;                           // device error flag
+};
+
+void launch_backproject(const BpLaunch &bl, cudaStream_t st);
+
+// sin/cos with the reference's fast intrinsics (__sinf/__cosf for FBP,
+// opt.cu:187-194; __sincosf for EM, em_RT_kernel.cu:120) and the per-angle
+// weight dtheta_a (times pi/theta_last beyond pi for FBP).
+void launch_angle_tables(const float *d_angles, int nangles, float *d_cos, float *d_sin,
+                         float *d_wt, int em_sincos, cudaStream_t st);
+
+// ------------------------------------------------------------ projector --
+struct ProjLaunch {
+    const float *img = nullptr;     // [nslices][ny][nx]
+    float *out = nullptr;           // plain [nslices][nangles][nrays] or window rows
+    const float *angles = nullptr;
+    int nx = 0, ny = 0, nrays = 0, nangles = 0, nslices = 0;
+    float ax = 1.f, ay = 1.f;
+    int em = 0;                     // 1: kernel_radon geometry, 0: Radon_RT_version_sscRadon
+    int epilogue = 0;               // 0 plain, 1 tEM flat*exp(-p), 2 eEM ratio
+    const float *flat = nullptr;    // tEM: [nslices][nrays]
+    const float *data = nullptr;    // tEM counts / eEM tomogram [nslices][nangles][nrays]
+    const float *wt = nullptr;      // per-angle weight applied when writing window rows
+    int windowed = 0, wlo = 0, Wg = 0;
+    double *metrics = nullptr;      // optional FP64 sums [nslices][3]
+};
+
+void launch_project(const ProjLaunch &pl, cudaStream_t st);
+
+// Copy a plain sinogram into weighted window rows (EM: BP of the counts).
+void launch_to_window(const float *sino, float *rows, const float *wt, int nrows, int nangles,
+                      int nrays, int wlo, int Wg, cudaStream_t st);
+
+// ----------------------------------------------------------- parameters --
+// FBP configuration as unpacked from the reference's packed arrays
+// (setFBPParameters, cuda/src/geometries/parallel/reconstruction_methods/parameters.cu:131-219).
+struct FbpConfig {
+    int nrays = 0, nangles = 0, nslices = 0, objsize = 0;
+    int pad = 0;
+    int filter = FILTER_RAMP;
+    int blocksize = 0;
+    float beta_delta = 0.f, reg = 0.f, energy = 1.f, z2 = 0.f;
+    float pixel_x = 1.f, pixel_y = 1.f, offset = 0.f;
+    float paganin = 0.f;           // derived, parameters.cu:201-203
+    int geometry = GEOM_FBP_REF;   // GEOM_FBP_REF or GEOM_FBP_LIN
+    int store = STORE_F32;
+};
+
+// EM configuration (setEMRTParameters, parameters.cu:8-59).
+struct EmConfig {
+    int nrays = 0, nangles = 0, nslices = 0, objsize = 0;
+    int niter = 0, blocksize = 0;
+    int nflats = 1;
+};
+
+}  // namespace raft

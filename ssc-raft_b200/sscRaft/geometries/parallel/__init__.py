@@ -1,0 +1,3 @@
+from .fbp_methods import *
+from .radon_methods import *
+from .em_methods import *

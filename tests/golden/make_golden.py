@@ -1,0 +1,148 @@
+"""Generate golden fixtures by running the REFERENCE ssc-raft CUDA library.
+
+Runs on a GPU box: loads oracle/_ref/libraft_ref.so (built from the
+reference sources by oracle/build_ref.sh) and calls its own C ABI
+(getFBPMultiGPU, getFilterLowPassMultiGPU, getRadonRTMultiGPU,
+get_tEM_RT_MultiGPU, get_eEM_RT_MultiGPU) with the packing of the reference
+Python wrappers, on small seeded inputs.  Inputs and outputs are saved
+together in tests/golden/ref_<case>.npz (or under --out).
+
+    python tests/golden/make_golden.py [--out DIR]
+"""
+import argparse
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "ssc-raft_b200"))
+sys.path.insert(0, os.path.join(REPO, "tests"))
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+
+from helpers import fbp_params, phantom_case, sino_case  # noqa: E402
+
+
+def ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def load_ref():
+    lib = ctypes.CDLL(os.path.join(REPO, "oracle", "_ref", "libraft_ref.so"))
+    P, I, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    lib.getFBPMultiGPU.argtypes = [P, I, P, P, P, P, P]
+    lib.getFilterLowPassMultiGPU.argtypes = [P, I, P, P, P]
+    lib.getRadonRTMultiGPU.argtypes = [P, I, P, P, P, I, I, I, I, I, F, F]
+    lib.get_tEM_RT_MultiGPU.argtypes = [P, I, P, P, P, P, P, P]
+    lib.get_eEM_RT_MultiGPU.argtypes = [P, I, P, P, P, P, P]
+    return lib
+
+
+GPUS = np.array([0], np.intc)
+
+# (name, N, A, nslices, pad, ftype, pixel, offset, reg, angle_span)
+FBP_CASES = [
+    ("fbp_ramp_n64", 64, 90, 2, 2, 7, 1.0, 0.0, 0.0, np.pi),
+    ("fbp_hann_off", 96, 120, 2, 2, 5, 1.0, 3.5, 0.0, np.pi),
+    ("fbp_hamming_px", 50, 64, 1, 2, 6, 0.5, 1.25, 0.0, np.pi),
+    ("fbp_ramp_pad1_2pi", 80, 100, 1, 1, 7, 1.0, 0.0, 0.0, 2 * np.pi),
+    ("fbp_none", 64, 60, 1, 2, 0, 1.0, 0.0, 0.0, np.pi),
+    ("fbp_gaussian", 64, 45, 1, 2, 1, 1.0, 0.0, 2.0, np.pi),
+    ("fbp_lorentz", 64, 45, 1, 2, 2, 1.0, -2.0, 3.0, np.pi),
+    ("fbp_cosine", 64, 45, 1, 2, 3, 1.0, 0.0, 0.0, np.pi),
+    ("fbp_rectangle", 64, 45, 1, 2, 4, 1.0, 0.0, 1.5, np.pi),
+    ("fbp_ramp_pad0_odd", 63, 37, 1, 0, 7, 1.0, 0.0, 0.0, np.pi),
+    ("fbp_ramp_n200", 200, 180, 1, 2, 7, 1.0, 0.0, 0.0, np.pi),
+]
+
+
+def fbp_case(lib, name, N, A, B, pad, ftype, pixel, offset, reg, span, seed):
+    ang = (np.arange(A, dtype=np.float64) * (span / A)).astype(np.float32)
+    sino, _ = sino_case(N, A, B, seed=seed, pixel=pixel, angles=ang)
+    pf, pi = fbp_params(N, A, B, pad=pad, ftype=ftype, pixel=pixel, offset=offset, reg=reg, blocksize=B)
+    obj = np.zeros((B, N, N), np.float32)
+    s = sino.copy()
+    lib.getFBPMultiGPU(ptr(GPUS), 1, ptr(obj), ptr(s), ptr(ang), ptr(pf), ptr(pi))
+    return dict(kind="fbp", sino=sino, angles=ang, paramf=pf, parami=pi, out=obj)
+
+
+def index_probe(lib, N, pad, pixel, thetas):
+    """Filter 'none', two angles (theta, theta + 2^-10), bin values = bin index
+    on the first row: the output is exactly idx(theta) * 2^-10 per pixel."""
+    Np = N * (1 + pad)
+    off = (pad * N) // 2
+    out = []
+    for th in thetas:
+        ang = np.array([th, th + 2.0 ** -10], np.float32)
+        sino = np.zeros((1, 2, N), np.float32)
+        # padded bin b holds sino[clamp(b - off)]: make the raw row encode b for b in [off, off+N)
+        sino[0, 0, :] = np.arange(N, dtype=np.float32) + off
+        pf, pi = fbp_params(N, 2, 1, pad=pad, ftype=0, pixel=pixel)
+        obj = np.zeros((1, N, N), np.float32)
+        lib.getFBPMultiGPU(ptr(GPUS), 1, ptr(obj), ptr(sino), ptr(ang), ptr(pf), ptr(pi))
+        out.append(obj[0])
+    return dict(kind="index_probe", N=N, pad=pad, pixel=pixel, thetas=np.asarray(thetas, np.float32),
+                out=np.stack(out), Np=Np)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=HERE)
+    args = ap.parse_args()
+    os.makedirs(args.out, exist_ok=True)
+    lib = load_ref()
+    cases = {}
+    for i, c in enumerate(FBP_CASES):
+        cases[c[0]] = fbp_case(lib, *c, seed=100 + i)
+    # index probes (bit-exact nearest-sample rule)
+    rng = np.random.default_rng(7)
+    th = np.concatenate([[0.0, np.pi / 4, np.pi / 2, 1.0], rng.uniform(0, np.pi, 12)])
+    cases["probe_px1"] = index_probe(lib, 48, 2, 1.0, th)
+    cases["probe_px07"] = index_probe(lib, 40, 1, 0.7, th[:8])
+    # lowpass
+    for name, N, A, pad, ftype in (("lowpass_ramp", 64, 30, 2, 7), ("lowpass_hann_pad1", 72, 24, 1, 5)):
+        sino, ang = sino_case(N, A, 2, seed=300)
+        pf, pi = fbp_params(N, A, 2, pad=pad, ftype=ftype)
+        t = sino.copy()
+        lib.getFilterLowPassMultiGPU(ptr(GPUS), 1, ptr(t), ptr(pf), ptr(pi))
+        cases[name] = dict(kind="lowpass", sino=sino, angles=ang, paramf=pf, parami=pi, out=t)
+    # Radon RT
+    img = phantom_case(64, 2, seed=400)
+    ang = (np.arange(90) * (np.pi / 90)).astype(np.float32)
+    proj = -np.ones((2, 90, 64), np.float32)
+    lib.getRadonRTMultiGPU(ptr(GPUS), 1, ptr(proj), ptr(img), ptr(ang), 64, 64, 64, 90, 2, 1.0, 1.0)
+    cases["radon_n64"] = dict(kind="radon", img=img, angles=ang, out=proj)
+    # tEM: blocksize == nangles == nslices and a constant flat, the setting in which the
+    # reference's angle-indexed flat buffer (em_rt.cu:107,134) is fully initialised
+    N, A, B, it = 48, 32, 32, 4
+    img = phantom_case(N, B, seed=500, scale=0.02)
+    ang = (np.arange(A) * (np.pi / A)).astype(np.float32)
+    import oracle as O  # only to make the transmission data from a forward projection
+    p = O.em_forward(img.astype(np.float64), ang, N)
+    counts = np.exp(-p).astype(np.float32)            # exp(-data) as em_methods.py:109 produces
+    flat = np.ones((B, N), np.float32)
+    obj = np.ones((B, N, N), np.float32)
+    pi = np.array([N, A, B, N, 0, 0, 0, B, it, A], np.int32)
+    pf = np.array([0], np.float32)
+    c = counts.copy()
+    lib.get_tEM_RT_MultiGPU(ptr(GPUS), 1, ptr(obj), ptr(c), ptr(flat), ptr(ang), ptr(pf), ptr(pi))
+    cases["tem_n48"] = dict(kind="tem", counts=counts, flat=flat, angles=ang, iterations=it, out=obj)
+    # eEM
+    N, A, B, it = 48, 40, 2, 5
+    img = phantom_case(N, B, seed=600)
+    ang = (np.arange(A) * (np.pi / A)).astype(np.float32)
+    tomo = O.em_forward(img.astype(np.float64), ang, N).astype(np.float32)
+    obj = np.ones((B, N, N), np.float32)
+    pi = np.array([N, A, B, N, 0, 0, 0, 1, it, 0], np.int32)
+    t = tomo.copy()
+    lib.get_eEM_RT_MultiGPU(ptr(GPUS), 1, ptr(obj), ptr(t), ptr(ang), ptr(pf), ptr(pi))
+    cases["eem_n48"] = dict(kind="eem", tomo=tomo, angles=ang, iterations=it, out=obj)
+    for name, d in cases.items():
+        np.savez_compressed(os.path.join(args.out, f"ref_{name}.npz"), **d)
+    print("wrote", len(cases), "fixtures to", args.out)
+
+
+if __name__ == "__main__":
+    main()
