@@ -105,6 +105,11 @@ int raft_em_device(int kind, int gpu, float *d_obj, const float *d_data, const f
                    const float *angles, int nrays, int nangles, int nslices, int niter,
                    double *d_metrics, int use_graph, void *stream);
 
+/* sin/cos of angles[0..n) computed on `gpu` with the fast intrinsics the reference
+ * uses: kind 0 = __sinf/__cosf (setSinCosTable, cuda/src/common/opt.cu:187-194),
+ * kind 1 = __sincosf (kernel_backprojection, em_RT_kernel.cu:120).  Returns 0 on success. */
+int raft_fast_sincos(int gpu, const float *angles, int n, int kind, float *cos_out, float *sin_out);
+
 /* Instrumentation (no reference counterpart): total kernel launches issued by
  * this library in the process; optional CUDA-event timing of the filter (class 0),
  * backprojector (1) and projector (2) launches, summed since the last read. */

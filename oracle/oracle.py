@@ -47,16 +47,16 @@ def lib():
         _lib.oracle_filter_spectrum.argtypes = [I, I, I, D, D, D, D, P, P]
         _lib.oracle_filter_rows.argtypes = [I, I, I, I, I, D, D, D, D, P, P]
         _lib.oracle_lowpass.argtypes = [I, I, I, I, I, D, D, D, P, P]
-        _lib.oracle_fbp_backproject.argtypes = [I, I, I, I, I, F, F, P, P, P]
-        _lib.oracle_fbp_backproject_f32.argtypes = [I, I, I, I, I, F, F, P, P, P]
-        _lib.oracle_fbp.argtypes = [I, I, I, I, I, I, D, D, D, F, F, P, P, P]
+        _lib.oracle_fbp_backproject.argtypes = [I, I, I, I, I, F, F, P, P, P, P, P]
+        _lib.oracle_fbp_backproject_f32.argtypes = [I, I, I, I, I, F, F, P, P, P, P, P]
+        _lib.oracle_fbp.argtypes = [I, I, I, I, I, I, D, D, D, F, F, P, P, P, P, P]
         _lib.oracle_fbp_f32.argtypes = [I, I, I, I, I, I, D, D, D, F, F, P, P, P]
-        _lib.oracle_radon_rt.argtypes = [I, I, I, I, I, F, F, P, P, P]
-        _lib.oracle_em_forward.argtypes = [I, I, I, I, P, P, P]
-        _lib.oracle_em_backproject.argtypes = [I, I, I, I, P, P, P]
-        _lib.oracle_tem.argtypes = [I, I, I, I, I, P, P, P, P]
-        _lib.oracle_eem.argtypes = [I, I, I, I, I, P, P, P]
-        _lib.oracle_tem_metrics.argtypes = [I, I, I, I, P, P, P, P, P, P]
+        _lib.oracle_radon_rt.argtypes = [I, I, I, I, I, F, F, P, P, P, P, P]
+        _lib.oracle_em_forward.argtypes = [I, I, I, I, P, P, P, P, P]
+        _lib.oracle_em_backproject.argtypes = [I, I, I, I, P, P, P, P, P]
+        _lib.oracle_tem.argtypes = [I, I, I, I, I, P, P, P, P, P, P, P, P]
+        _lib.oracle_eem.argtypes = [I, I, I, I, I, P, P, P, P, P, P, P]
+        _lib.oracle_tem_metrics.argtypes = [I, I, I, I, P, P, P, P, P, P, P, P]
     return _lib
 
 
@@ -75,6 +75,15 @@ def _p(a):
 def _as3(a):
     a = np.asarray(a)
     return a[None] if a.ndim == 2 else a
+
+
+def _trig(tr):
+    """(cos, sin) float32 arrays to use for the nearest-sample index rule, or
+    None for libm's.  Keeps the arrays alive in the returned tuple."""
+    if tr is None:
+        return None, None, None
+    c, s = _f32(tr[0]), _f32(tr[1])
+    return (c, s), _p(c), _p(s)
 
 
 def filter_spectrum(mode, ftype, Np, paganin=0.0, reg=0.0, offset=0.0, pixel=1.0):
@@ -104,11 +113,13 @@ def lowpass(sino, mode, ftype, pad, paganin=0.0, reg=0.0, pixel=1.0):
 
 
 def fbp(sino, angles, mode, ftype, pad, paganin=0.0, reg=0.0, offset=0.0, pixel=1.0,
-        f32=False):
-    """FBP of sino [B, A, N] -> [B, N, N] (float64, or float32 if f32)."""
+        f32=False, trig=None):
+    """FBP of sino [B, A, N] -> [B, N, N] (float64, or float32 if f32).
+    trig = (cos, sin) overrides libm's values in the nearest-sample index rule."""
     s = _f32(_as3(sino))
     B, A, N = s.shape
     ang = _f32(angles)
+    keep, pc, ps = _trig(trig)
     if f32:
         img = np.zeros((B, N, N), dtype=np.float32)
         lib().oracle_fbp_f32(mode, ftype, N, A, B, pad, paganin, reg, offset, pixel, pixel,
@@ -116,77 +127,85 @@ def fbp(sino, angles, mode, ftype, pad, paganin=0.0, reg=0.0, offset=0.0, pixel=
     else:
         img = np.zeros((B, N, N))
         lib().oracle_fbp(mode, ftype, N, A, B, pad, paganin, reg, offset, pixel, pixel,
-                         _p(ang), _p(s), _p(img))
+                         _p(ang), _p(s), _p(img), pc, ps)
     return img
 
 
-def fbp_backproject(q, angles, mode, N, pad, pixel=1.0):
+def fbp_backproject(q, angles, mode, N, pad, pixel=1.0, trig=None):
     q = _f64(_as3(q))
     B, A, Np = q.shape
     img = np.zeros((B, N, N))
-    lib().oracle_fbp_backproject(mode, N, A, B, pad, pixel, pixel, _p(_f32(angles)), _p(q), _p(img))
+    keep, pc, ps = _trig(trig)
+    lib().oracle_fbp_backproject(mode, N, A, B, pad, pixel, pixel, _p(_f32(angles)), _p(q), _p(img), pc, ps)
     return img
 
 
-def radon_rt(img, angles, nrays=None, ax=1.0, ay=1.0):
+def radon_rt(img, angles, nrays=None, ax=1.0, ay=1.0, trig=None):
     """Radon_RT_version_sscRadon (without the Python-side N*pixel/2 scale)."""
     im = _f32(_as3(img))
     B, ny, nx = im.shape
     nrays = nx if nrays is None else nrays
     ang = _f32(angles)
     out = np.zeros((B, len(ang), nrays))
-    lib().oracle_radon_rt(nx, ny, nrays, len(ang), B, ax, ay, _p(ang), _p(im), _p(out))
+    keep, pc, ps = _trig(trig)
+    lib().oracle_radon_rt(nx, ny, nrays, len(ang), B, ax, ay, _p(ang), _p(im), _p(out), pc, ps)
     return out
 
 
-def em_forward(img, angles, nrays):
+def em_forward(img, angles, nrays, trig=None):
     im = _f64(_as3(img))
     B, N, _ = im.shape
     ang = _f32(angles)
     out = np.zeros((B, len(ang), nrays))
-    lib().oracle_em_forward(N, nrays, len(ang), B, _p(ang), _p(im), _p(out))
+    keep, pc, ps = _trig(trig)
+    lib().oracle_em_forward(N, nrays, len(ang), B, _p(ang), _p(im), _p(out), pc, ps)
     return out
 
 
-def em_backproject(sino, angles, N):
-    s = None if sino is None else _f64(_as3(sino))
+def em_backproject(sino, angles, N, trig=None):
+    s = _f64(_as3(sino))
     ang = _f32(angles)
-    if s is None:
-        raise ValueError("use em_backproject_ones")
     B, A, nrays = s.shape
     img = np.zeros((B, N, N))
-    lib().oracle_em_backproject(N, nrays, A, B, _p(ang), _p(s), _p(img))
+    keep, pc, ps = _trig(trig)
+    lib().oracle_em_backproject(N, nrays, A, B, _p(ang), _p(s), _p(img), pc, ps)
     return img
 
 
-def em_backproject_ones(angles, N, nrays, nslices=1):
+def em_backproject_ones(angles, N, nrays, nslices=1, trig=None):
     ang = _f32(angles)
     img = np.zeros((nslices, N, N))
-    lib().oracle_em_backproject(N, nrays, len(ang), nslices, _p(ang), None, _p(img))
+    keep, pc, ps = _trig(trig)
+    lib().oracle_em_backproject(N, nrays, len(ang), nslices, _p(ang), None, _p(img), pc, ps)
     return img
 
 
-def tem(counts_exp, flat, angles, niter, obj=None):
-    """tEM on counts already mapped through exp(-x) (em_methods.py:109)."""
+def tem(counts_exp, flat, angles, niter, obj=None, fwd_trig=None, bp_trig=None):
+    """tEM on counts already mapped through exp(-x) (em_methods.py:109).
+    fwd_trig / bp_trig: (cos, sin) for the projector and the backprojector."""
     c = _f32(_as3(counts_exp))
     B, A, nrays = c.shape
     N = nrays
     fl = _f32(np.asarray(flat).reshape(B, nrays))
     o = np.ones((B, N, N)) if obj is None else _f64(_as3(obj)).copy()
-    lib().oracle_tem(N, nrays, A, B, niter, _p(_f32(angles)), _p(c), _p(fl), _p(o))
+    k1, fc, fs = _trig(fwd_trig)
+    k2, bc, bs = _trig(bp_trig)
+    lib().oracle_tem(N, nrays, A, B, niter, _p(_f32(angles)), _p(c), _p(fl), _p(o), fc, fs, bc, bs)
     return o
 
 
-def eem(tomo, angles, niter, obj=None):
+def eem(tomo, angles, niter, obj=None, fwd_trig=None, bp_trig=None):
     t = _f32(_as3(tomo))
     B, A, nrays = t.shape
     N = nrays
     o = np.ones((B, N, N)) if obj is None else _f64(_as3(obj)).copy()
-    lib().oracle_eem(N, nrays, A, B, niter, _p(_f32(angles)), _p(t), _p(o))
+    k1, fc, fs = _trig(fwd_trig)
+    k2, bc, bs = _trig(bp_trig)
+    lib().oracle_eem(N, nrays, A, B, niter, _p(_f32(angles)), _p(t), _p(o), fc, fs, bc, bs)
     return o
 
 
-def tem_metrics(counts_exp, flat, angles, obj):
+def tem_metrics(counts_exp, flat, angles, obj, fwd_trig=None):
     c = _f32(_as3(counts_exp))
     B, A, nrays = c.shape
     N = nrays
@@ -194,5 +213,7 @@ def tem_metrics(counts_exp, flat, angles, obj):
     o = _f64(_as3(obj))
     res = np.zeros(B)
     nll = np.zeros(B)
-    lib().oracle_tem_metrics(N, nrays, A, B, _p(_f32(angles)), _p(c), _p(fl), _p(o), _p(res), _p(nll))
+    k1, fc, fs = _trig(fwd_trig)
+    lib().oracle_tem_metrics(N, nrays, A, B, _p(_f32(angles)), _p(c), _p(fl), _p(o), _p(res), _p(nll),
+                             fc, fs)
     return res, nll

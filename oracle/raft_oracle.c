@@ -252,7 +252,7 @@ static float angle_scale(const float *angles, int A)
  * same sample grid (u = (t - tmin)/dt, samples at integer u, zero outside). */
 #define DEFINE_BP(NAME, ACC)                                                                   \
 void NAME(int mode, int N, int A, int nslices, int pad, float pixel_x, float pixel_y,           \
-          const float *angles, const double *q, ACC *img)                                       \
+          const float *angles, const double *q, ACC *img, const float *tcos, const float *tsin) \
 {                                                                                               \
     int Np = N * (1 + pad);                                                                     \
     int off = (pad * N) / 2;                                                                    \
@@ -260,7 +260,7 @@ void NAME(int mode, int N, int A, int nslices, int pad, float pixel_x, float pix
     float *dth = (float *)malloc(sizeof(float) * A);                                            \
     double *cd = (double *)malloc(sizeof(double) * A), *sd = (double *)malloc(sizeof(double) * A); \
     for (int a = 0; a < A; a++) {                                                               \
-        cs[a] = cosf(angles[a]); sn[a] = sinf(angles[a]);                                       \
+        cs[a] = tcos ? tcos[a] : cosf(angles[a]); sn[a] = tsin ? tsin[a] : sinf(angles[a]);     \
         cd[a] = cos((double)angles[a]); sd[a] = sin((double)angles[a]);                         \
     }                                                                                           \
     angle_steps(angles, A, dth);                                                                \
@@ -307,14 +307,17 @@ DEFINE_BP(oracle_fbp_backproject, double)
 DEFINE_BP(oracle_fbp_backproject_f32, float)
 
 /* Full FBP: filter (unless type 'none') then backproject.  img is [nslices,N,N]. */
+/* tcos/tsin (may be NULL): sin/cos values to use for the nearest-sample
+ * index rule instead of libm's, e.g. the GPU fast-intrinsic values the
+ * reference computes (opt.cu:187-194), recorded as data in the fixtures. */
 void oracle_fbp(int mode, int type, int N, int A, int nslices, int pad, double paganin,
                 double reg, double offset, float pixel_x, float pixel_y, const float *angles,
-                const float *sino, double *img)
+                const float *sino, double *img, const float *tcos, const float *tsin)
 {
     int Np = N * (1 + pad);
     double *q = (double *)malloc(sizeof(double) * (size_t)nslices * A * Np);
     oracle_filter_rows(mode, type, N, nslices * A, pad, paganin, reg, offset, pixel_x, sino, q);
-    oracle_fbp_backproject(mode, N, A, nslices, pad, pixel_x, pixel_y, angles, q, img);
+    oracle_fbp_backproject(mode, N, A, nslices, pad, pixel_x, pixel_y, angles, q, img, tcos, tsin);
     free(q);
 }
 
@@ -326,7 +329,7 @@ void oracle_fbp_f32(int mode, int type, int N, int A, int nslices, int pad, doub
     int Np = N * (1 + pad);
     double *q = (double *)malloc(sizeof(double) * (size_t)nslices * A * Np);
     oracle_filter_rows(mode, type, N, nslices * A, pad, paganin, reg, offset, pixel_x, sino, q);
-    oracle_fbp_backproject_f32(mode, N, A, nslices, pad, pixel_x, pixel_y, angles, q, img);
+    oracle_fbp_backproject_f32(mode, N, A, nslices, pad, pixel_x, pixel_y, angles, q, img, NULL, NULL);
     free(q);
 }
 
@@ -334,14 +337,15 @@ void oracle_fbp_f32(int mode, int type, int N, int A, int nslices, int pad, doub
 /* Radon RT (radon_rt.cu:131-174).  out[k][a][i]                            */
 /* ------------------------------------------------------------------------ */
 void oracle_radon_rt(int nx, int ny, int nrays, int A, int nslices, float ax, float ay,
-                     const float *angles, const float *img, double *out)
+                     const float *angles, const float *img, double *out, const float *tcos,
+                     const float *tsin)
 {
     float dx = 2.0f * ax / (float)(nx - 1);
     float dy = 2.0f * ay / (float)(ny - 1);
 #pragma omp parallel for collapse(2) schedule(dynamic, 4)
     for (int k = 0; k < nslices; k++)
         for (int a = 0; a < A; a++) {
-            float c = cosf(angles[a]), s = sinf(angles[a]);
+            float c = tcos ? tcos[a] : cosf(angles[a]), s = tsin ? tsin[a] : sinf(angles[a]);
             for (int i = 0; i < nrays; i++) {
                 float t = -ax + (float)i * dx;
                 double sum = 0;
@@ -365,14 +369,14 @@ void oracle_radon_rt(int nx, int ny, int nrays, int A, int nslices, float ax, fl
 
 /* kernel_radon (em_RT_kernel.cu:145-185), a = 1: out[k][a][r] */
 void oracle_em_forward(int N, int nrays, int A, int nslices, const float *angles,
-                       const double *img, double *out)
+                       const double *img, double *out, const float *tcos, const float *tsin)
 {
     float a1 = 1.0f;
     float dt = (float)(2.0 * a1 / (nrays - 1));
 #pragma omp parallel for collapse(2) schedule(dynamic, 4)
     for (int k = 0; k < nslices; k++)
         for (int a = 0; a < A; a++) {
-            float c = cosf(angles[a]), s = sinf(angles[a]);
+            float c = tcos ? tcos[a] : cosf(angles[a]), s = tsin ? tsin[a] : sinf(angles[a]);
             for (int r = 0; r < nrays; r++) {
                 float t = -a1 + (float)r * dt;
                 double sum = 0;
@@ -393,13 +397,16 @@ void oracle_em_forward(int N, int nrays, int A, int nslices, const float *angles
 /* kernel_backprojection (em_RT_kernel.cu:92-142); sino==NULL gives the
  * back-projection of ones (kernel_backprojectionOfOnes, :303-351). */
 void oracle_em_backproject(int N, int nrays, int A, int nslices, const float *angles,
-                           const double *sino, double *img)
+                           const double *sino, double *img, const float *tcos, const float *tsin)
 {
     float dxy = (float)(2.0 / (N - 1));
     float dt = (float)(2.0 / (nrays - 1));
     float *cs = (float *)malloc(sizeof(float) * A), *sn = (float *)malloc(sizeof(float) * A);
     float *dth = (float *)malloc(sizeof(float) * A);
-    for (int a = 0; a < A; a++) { cs[a] = cosf(angles[a]); sn[a] = sinf(angles[a]); }
+    for (int a = 0; a < A; a++) {
+        cs[a] = tcos ? tcos[a] : cosf(angles[a]);
+        sn[a] = tsin ? tsin[a] : sinf(angles[a]);
+    }
     angle_steps(angles, A, dth);
 #pragma omp parallel for collapse(2) schedule(dynamic, 8)
     for (int k = 0; k < nslices; k++)
@@ -423,7 +430,8 @@ void oracle_em_backproject(int N, int nrays, int A, int nslices, const float *an
  * Python wrapper does, em_methods.py:109).  flat is [nslices][nrays]
  * (intended semantics: flat of the slice, not of the angle row). */
 void oracle_tem(int N, int nrays, int A, int nslices, int niter, const float *angles,
-                const float *counts, const float *flat, double *obj)
+                const float *counts, const float *flat, double *obj, const float *fcos,
+                const float *fsin, const float *bcos, const float *bsin)
 {
     size_t ns = (size_t)nslices * A * nrays, ni = (size_t)nslices * N * N;
     double *c = (double *)malloc(sizeof(double) * ns);
@@ -431,16 +439,16 @@ void oracle_tem(int N, int nrays, int A, int nslices, int niter, const float *an
     double *bc = (double *)malloc(sizeof(double) * ni);
     double *b = (double *)malloc(sizeof(double) * ni);
     for (size_t i = 0; i < ns; i++) c[i] = counts[i];
-    oracle_em_backproject(N, nrays, A, nslices, angles, c, bc);
+    oracle_em_backproject(N, nrays, A, nslices, angles, c, bc, bcos, bsin);
     for (int it = 0; it < niter; it++) {
-        oracle_em_forward(N, nrays, A, nslices, angles, obj, p);
+        oracle_em_forward(N, nrays, A, nslices, angles, obj, p, fcos, fsin);
         for (int k = 0; k < nslices; k++)
             for (int a = 0; a < A; a++)
                 for (int r = 0; r < nrays; r++) {
                     size_t ix = ((size_t)k * A + a) * nrays + r;
                     p[ix] = (double)flat[(size_t)k * nrays + r] * exp(-p[ix]);
                 }
-        oracle_em_backproject(N, nrays, A, nslices, angles, p, b);
+        oracle_em_backproject(N, nrays, A, nslices, angles, p, b, bcos, bsin);
         for (size_t i = 0; i < ni; i++) obj[i] = obj[i] * b[i] / bc[i];
     }
     free(c); free(p); free(bc); free(b);
@@ -448,22 +456,23 @@ void oracle_tem(int N, int nrays, int A, int nslices, int niter, const float *an
 
 /* eEM (em_rt.cu:316-355; kernel_radonWithDivision em_RT_kernel.cu:188-246). */
 void oracle_eem(int N, int nrays, int A, int nslices, int niter, const float *angles,
-                const float *tomo, double *obj)
+                const float *tomo, double *obj, const float *fcos, const float *fsin,
+                const float *bcos, const float *bsin)
 {
     size_t ns = (size_t)nslices * A * nrays, ni = (size_t)nslices * N * N;
     double *p = (double *)malloc(sizeof(double) * ns);
     double *bo = (double *)malloc(sizeof(double) * ni);
     double *b = (double *)malloc(sizeof(double) * ni);
-    oracle_em_backproject(N, nrays, A, nslices, angles, NULL, bo);
+    oracle_em_backproject(N, nrays, A, nslices, angles, NULL, bo, bcos, bsin);
     for (int it = 0; it < niter; it++) {
-        oracle_em_forward(N, nrays, A, nslices, angles, obj, p);
+        oracle_em_forward(N, nrays, A, nslices, angles, obj, p, fcos, fsin);
         for (size_t i = 0; i < ns; i++) {
             double v = p[i];
             double sg = (v > 0) ? 1.0 : ((v < 0) ? -1.0 : 0.0);
             double r = (double)tomo[i] * sg / sqrt(1e-8 + v * v);
             p[i] = r < 0 ? 0.0 : r;
         }
-        oracle_em_backproject(N, nrays, A, nslices, angles, p, b);
+        oracle_em_backproject(N, nrays, A, nslices, angles, p, b, bcos, bsin);
         for (size_t i = 0; i < ni; i++) obj[i] = obj[i] * b[i] / bo[i];
     }
     free(p); free(bo); free(b);
@@ -473,11 +482,11 @@ void oracle_eem(int N, int nrays, int A, int nslices, int niter, const float *an
  * negative log-likelihood sum(flat*exp(-Ax) + y*Ax), both per slice. */
 void oracle_tem_metrics(int N, int nrays, int A, int nslices, const float *angles,
                         const float *counts, const float *flat, const double *obj,
-                        double *residual, double *nll)
+                        double *residual, double *nll, const float *fcos, const float *fsin)
 {
     size_t ns = (size_t)nslices * A * nrays;
     double *p = (double *)malloc(sizeof(double) * ns);
-    oracle_em_forward(N, nrays, A, nslices, angles, obj, p);
+    oracle_em_forward(N, nrays, A, nslices, angles, obj, p, fcos, fsin);
     for (int k = 0; k < nslices; k++) {
         double num = 0, den = 0, l = 0;
         for (int a = 0; a < A; a++)

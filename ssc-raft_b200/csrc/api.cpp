@@ -393,6 +393,33 @@ int raft_em_device(int kind, int gpu, float *d_obj, const float *d_data, const f
     return has_error() ? 1 : 0;
 }
 
+// sin/cos of `angles` as the GPU's fast intrinsics produce them: kind 0 =
+// __sinf/__cosf (FBP table, opt.cu:187-194; the projectors' fast-math
+// sinf/cosf), kind 1 = __sincosf (EM backprojector, em_RT_kernel.cu:120).
+int raft_fast_sincos(int gpu, const float *angles, int n, int kind, float *cos_out, float *sin_out)
+{
+    clear_error();
+    if (!check_gpus(&gpu, 1)) return 1;
+    if (n < 1 || !angles || !cos_out || !sin_out) {
+        set_error("raft_fast_sincos: bad arguments");
+        return 1;
+    }
+    try {
+        DeviceState &ds = device_state(gpu);
+        std::lock_guard<std::mutex> lk(ds.mtx);
+        RAFT_CUDA(cudaSetDevice(gpu));
+        ds.ensure();
+        float *d = (float *)ds.angles.get(sizeof(float) * 3 * (size_t)n);
+        RAFT_CUDA(cudaMemcpy(d, angles, sizeof(float) * n, cudaMemcpyHostToDevice));
+        launch_angle_tables(d, n, d + n, d + 2 * n, nullptr, kind, ds.s_comp);
+        RAFT_CUDA(cudaStreamSynchronize(ds.s_comp));
+        RAFT_CUDA(cudaMemcpy(cos_out, d + n, sizeof(float) * n, cudaMemcpyDeviceToHost));
+        RAFT_CUDA(cudaMemcpy(sin_out, d + 2 * n, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    } catch (const CudaFail &) {
+    }
+    return has_error() ? 1 : 0;
+}
+
 // Adjacent reference exports that this library does not implement: they
 // record an error instead of running (rafttypes.py binds them if present).
 void getBSTMultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *angles, float *paramf, int *parami,

@@ -74,7 +74,21 @@ libraft.raft_profile_enable.restype = None
 libraft.raft_profile_read.argtypes = [_P, _P, _I]
 libraft.raft_profile_read.restype = _I
 
+libraft.raft_fast_sincos.argtypes = [_I, _P, _I, _I, _P, _P]
+libraft.raft_fast_sincos.restype = _I
+
 GEOMETRY = {"nearest": 0, "linear": 1}
+
+
+def fast_sincos(angles, kind=0, gpu=0):
+    """(cos, sin) of angles with the GPU fast intrinsics (kind 0: __sinf/__cosf,
+    1: __sincosf) -- the values the reference's index rules use."""
+    a = numpy.ascontiguousarray(angles, dtype=numpy.float32)
+    c = numpy.zeros_like(a)
+    s = numpy.zeros_like(a)
+    libraft.raft_fast_sincos(gpu, _ptr(a), a.size, kind, _ptr(c), _ptr(s))
+    check_error("fast_sincos")
+    return c, s
 STORE = {"float32": 1, "bfloat16": 2}
 
 

@@ -139,6 +139,17 @@ def main():
     t = tomo.copy()
     lib.get_eEM_RT_MultiGPU(ptr(GPUS), 1, ptr(obj), ptr(t), ptr(ang), ptr(pf), ptr(pi))
     cases["eem_n48"] = dict(kind="eem", tomo=tomo, angles=ang, iterations=it, out=obj)
+    # the fast-intrinsic sin/cos values the reference's index rules use, as data
+    # for the oracle: kind 0 = __sinf/__cosf, kind 1 = __sincosf
+    from sscRaft.rafttypes import fast_sincos
+    for name, d in cases.items():
+        if "angles" in d:
+            d["fcos"], d["fsin"] = fast_sincos(d["angles"], 0)
+            d["bcos"], d["bsin"] = fast_sincos(d["angles"], 1)
+        elif d["kind"] == "index_probe":
+            allang = np.concatenate([[t, np.float32(t) + np.float32(2.0 ** -10)] for t in d["thetas"]])
+            allang = allang.astype(np.float32)
+            d["fcos"], d["fsin"] = fast_sincos(allang, 0)
     for name, d in cases.items():
         np.savez_compressed(os.path.join(args.out, f"ref_{name}.npz"), **d)
     print("wrote", len(cases), "fixtures to", args.out)
