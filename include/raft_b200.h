@@ -105,6 +105,11 @@ int raft_em_device(int kind, int gpu, float *d_obj, const float *d_data, const f
                    const float *angles, int nrays, int nangles, int nslices, int niter,
                    double *d_metrics, int use_graph, void *stream);
 
+/* Host-only helper (no GPU needed, no reference counterpart): the detector-window
+ * layout the backprojector stages for a configuration; out = {wlo, Wg, W, align}.
+ * geometry 0/1 with FBP packing, 2 with EM packing.  Returns 0 on success. */
+int raft_plan_window(const float *paramf, const int *parami, int geometry, int store, int *out);
+
 /* sin/cos of angles[0..n) computed on `gpu` with the fast intrinsics the reference
  * uses: kind 0 = __sinf/__cosf (setSinCosTable, cuda/src/common/opt.cu:187-194),
  * kind 1 = __sincosf (kernel_backprojection, em_RT_kernel.cu:120).  Returns 0 on success. */

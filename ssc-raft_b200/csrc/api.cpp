@@ -393,6 +393,44 @@ int raft_em_device(int kind, int gpu, float *d_obj, const float *d_data, const f
     return has_error() ? 1 : 0;
 }
 
+// Host-only: the window layout the backprojector would use (for tests of
+// the bounds logic without a GPU).  geometry/store as raft_fbp_ext; for
+// geometry 2 (EM) paramf/parami follow the EM packing.  out = {wlo, Wg, W, align}.
+int raft_plan_window(const float *paramf, const int *parami, int geometry, int store, int *out)
+{
+    clear_error();
+    try {
+        if (geometry == GEOM_EM_REF) {
+            EmConfig c;
+            if (!parse_em_arrays(paramf, parami, c)) return 1;
+            EmPrepared ep = prepare_em(c);
+            out[0] = ep.win.wlo; out[1] = ep.win.Wg; out[2] = ep.win.W; out[3] = ep.win.align;
+            return 0;
+        }
+        FbpConfig c;
+        if (!parse_fbp_arrays(paramf, parami, c, true)) return 1;
+        c.geometry = geometry;
+        c.store = store;
+        const int N = c.nrays, No = c.objsize, pad = c.pad;
+        BpPlanInput pi;
+        pi.geometry = geometry;
+        pi.store = store;
+        pi.No = No;
+        const int Np = N * (1 + pad), Npo = No * (1 + pad);
+        pi.xmin = -c.pixel_x * (float)Npo / 2.0f;
+        pi.ymin = -c.pixel_y * (float)Npo / 2.0f;
+        pi.dx = c.pixel_x;
+        pi.dy = c.pixel_y;
+        pi.tmin = -c.pixel_x * (float)Np / 2.0f;
+        pi.dt = c.pixel_x;
+        pi.offo = (pad * No) / 2;
+        WindowLayout w = plan_window(pi);
+        out[0] = w.wlo; out[1] = w.Wg; out[2] = w.W; out[3] = w.align;
+    } catch (const CudaFail &) {
+    }
+    return has_error() ? 1 : 0;
+}
+
 // sin/cos of `angles` as the GPU's fast intrinsics produce them: kind 0 =
 // __sinf/__cosf (FBP table, opt.cu:187-194; the projectors' fast-math
 // sinf/cosf), kind 1 = __sincosf (EM backprojector, em_RT_kernel.cu:120).
