@@ -7,11 +7,14 @@
  *
  * Everything accumulates in FP64.  Where the reference computes an integer
  * sample index from FP32 arithmetic (nearest-truncation operators, "ref"
- * mode) the index is computed here with the same FP32 expression order, but
- * with the C library's correctly rounded-ish sinf/cosf instead of the GPU's
- * fast intrinsics, so a handful of borderline samples (fractional part within
- * ~1e-3 of an integer) may pick the neighbouring bin.  Tests therefore compare
- * ref-mode results in relative L2 with a stated tolerance.
+ * mode) the index is computed here with the same FP32 expressions, including
+ * the multiply-add contraction the reference build applies (a*b - c*d is
+ * evaluated as fmaf(a, b, -(c*d)) and i*d + m as fmaf(i, d, m); found by
+ * comparing against the reference library's own outputs).  Two things the
+ * oracle cannot restate: the GPU fast-intrinsic sin/cos (the caller may pass
+ * those values as data, `tcos`/`tsin`; otherwise libm's are used) and the
+ * fast approximate division (here an IEEE division), so a sample whose exact
+ * position lies on a bin boundary may land in the neighbouring bin.
  *
  * Reference files followed (paths inside cnpem/ssc-raft):
  *   edge padding      cuda/src/common/padding.cu:140-178 (paddR2R)
@@ -277,10 +280,10 @@ void NAME(int mode, int N, int A, int nslices, int pad, float pixel_x, float pix
                 int i = ii + off, j = jj + off;                                                 \
                 ACC sum = 0;                                                                    \
                 if (mode == 0) {                                                                \
-                    float x = xmin + (float)i * pixel_x;                                        \
-                    float y = ymin + (float)j * pixel_y;                                        \
+                    float x = fmaf((float)i, pixel_x, xmin);                                    \
+                    float y = fmaf((float)j, pixel_y, ymin);                                    \
                     for (int a = 0; a < A; a++) {                                               \
-                        float t = x * cs[a] - y * sn[a];                                        \
+                        float t = fmaf(x, cs[a], -(y * sn[a]));                                 \
                         int ti = (int)((t - tmin) / dt);                                        \
                         if (ti > -1 && ti < Np) sum += (ACC)qk[(size_t)a * Np + ti] * (ACC)dth[a]; \
                     }                                                                           \
@@ -347,12 +350,12 @@ void oracle_radon_rt(int nx, int ny, int nrays, int A, int nslices, float ax, fl
         for (int a = 0; a < A; a++) {
             float c = tcos ? tcos[a] : cosf(angles[a]), s = tsin ? tsin[a] : sinf(angles[a]);
             for (int i = 0; i < nrays; i++) {
-                float t = -ax + (float)i * dx;
+                float t = fmaf((float)i, dx, -ax);
                 double sum = 0;
                 for (int r = 0; r < ny; r++) {
-                    float sr = -ay + (float)r * dy;
-                    float x = t * c - sr * s;
-                    float y = t * s + sr * c;
+                    float sr = fmaf((float)r, dy, -ay);
+                    float x = fmaf(t, c, -(sr * s));
+                    float y = fmaf(t, s, sr * c);
                     int ix = (int)((x + 1) / dx);
                     int iy = (int)((y + 1) / dy);
                     if (ix >= 0 && ix < nx && iy >= 0 && iy < ny)
@@ -378,12 +381,12 @@ void oracle_em_forward(int N, int nrays, int A, int nslices, const float *angles
         for (int a = 0; a < A; a++) {
             float c = tcos ? tcos[a] : cosf(angles[a]), s = tsin ? tsin[a] : sinf(angles[a]);
             for (int r = 0; r < nrays; r++) {
-                float t = -a1 + (float)r * dt;
+                float t = fmaf((float)r, dt, -a1);
                 double sum = 0;
                 for (int m = 0; m < nrays; m++) {
-                    float sm = -a1 + (float)m * dt;
-                    float x = t * c - sm * s;
-                    float y = t * s + sm * c;
+                    float sm = fmaf((float)m, dt, -a1);
+                    float x = fmaf(t, c, -(sm * s));
+                    float y = fmaf(t, s, sm * c);
                     int X = (int)((x + 1) / dt);
                     int Y = (int)((y + 1) / dt);
                     if (X >= 0 && X < N && Y >= 0 && Y < N)
@@ -412,11 +415,11 @@ void oracle_em_backproject(int N, int nrays, int A, int nslices, const float *an
     for (int k = 0; k < nslices; k++)
         for (int j = 0; j < N; j++)
             for (int i = 0; i < N; i++) {
-                float x = -1.0f + (float)i * dxy;
-                float y = -1.0f + (float)j * dxy;
+                float x = fmaf((float)i, dxy, -1.0f);
+                float y = fmaf((float)j, dxy, -1.0f);
                 double sum = 0;
                 for (int a = 0; a < A; a++) {
-                    float t = x * cs[a] + y * sn[a];
+                    float t = fmaf(x, cs[a], y * sn[a]);
                     int T = (int)((t + 1.0f) / dt);
                     if (T > -1 && T < nrays)
                         sum += (sino ? sino[((size_t)k * A + a) * nrays + T] : 1.0) * (double)dth[a];
