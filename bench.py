@@ -247,6 +247,14 @@ def run_ours(args):
         return ms[0], cnt[0], ms[1], cnt[1]
 
     hbm_peak, sm_max, peak_kind = peaks()
+    if args.quick:
+        # profiling mode: only the device-resident FBP of the chosen operator
+        g, s = {"nearest": (0, 0), "linear": (1, 1), "linear_bf16": (1, 2)}[args.op]
+        ms, launches = time_device(g, s, args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({"quick": True, "op": args.op, "slices": nsl, "ms_per_step": ms,
+                              "slices_per_s": ws * nsl / (ms / 1e3), "gpu_launches": int(launches)}), flush=True)
+        return
     result = {}
     with ClockSampler(local) as clk:
         ms_dev, launches = time_device(0, 0, args.steps, args.warmup)
@@ -406,6 +414,8 @@ def main():
     ap.add_argument("--slices", type=int, default=N_SLICES)
     ap.add_argument("--ref-slices", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="device timing of one operator only (profiling)")
+    ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16"])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
