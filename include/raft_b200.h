@@ -91,6 +91,20 @@ int raft_fbp_ext(int *gpus, int ngpus, float *obj, const float *tomogram, const 
 int raft_fbp_device(int gpu, float *d_obj, const float *d_tomogram, const float *angles,
                     const float *paramf, const int *parami, int geometry, int store, void *stream);
 
+/* raft_fbp_device without any device-memory allocation (no counterpart in the reference).
+ * For callers that cannot allocate GPU memory while reconstructing -- e.g. acquisition
+ * pipelines that reserve the device memory when a scan starts so reconstruction can never
+ * run out of memory mid-scan, or hosts whose own allocator owns the device memory.
+ * Working memory comes from one fixed 64 MiB device array inside the library, held by
+ * every GPU that loads it until exit; the first call on a device looks up that array's
+ * address (make it before any stream capture).  Calls share the array: calls whose work
+ * overlaps on one GPU race.  Limits: N*(1+pad) <= 14080 with prime factors 2,3,5,7,
+ * nangles <= 32768, one slice's filtered rows + tables within 64 MiB; larger requests
+ * return 1 with a message.  Synchronises `stream` before returning. */
+int raft_fbp_device_noalloc(int gpu, float *d_obj, const float *d_tomogram, const float *angles,
+                            const float *paramf, const int *parami, int geometry, int store,
+                            void *stream);
+
 /* EM (kind 0 = tEM as get_tEM_RT_MultiGPU, 1 = eEM as get_eEM_RT_MultiGPU) on one GPU with
  * host buffers, the iteration loop replayed as one CUDA graph when use_graph != 0, and
  * per-iteration FP64 metrics [niter][nslices][3] = {sum (model-data)^2, sum data^2,

@@ -159,6 +159,14 @@ static void split_slabs(const int *gpus, int ngpus, int nslices, F work)
         }
 }
 
+// Non-static access for other translation units (the no-allocation entry point).
+bool parse_fbp_params(const float *paramf, const int *parami, FbpConfig &cfg)
+{
+    return parse_fbp_arrays(paramf, parami, cfg, true);
+}
+
+bool check_gpu_id(int gpu) { return check_gpus(&gpu, 1); }
+
 }  // namespace raft
 
 using namespace raft;

@@ -100,4 +100,9 @@ void em_chunk(DeviceState &ds, const EmPrepared &ep, int kind, const float *d_da
 void em_host_slab(const EmConfig &cfg, int kind, int device, float *obj, const float *data, const float *flat,
                   const float *angles, int nslices, bool flat_by_angle);
 
+// Parameter parsing / device check shared with the no-allocation entry point.
+bool parse_fbp_params(const float *paramf, const int *parami, FbpConfig &cfg);
+bool check_gpu_id(int gpu);
+bool filter_plan_shape(FilterPlan &plan, int ftype, int N, int pad);
+
 }  // namespace raft

@@ -505,3 +505,23 @@ void launch_filter(const FilterPlan &plan, const FilterLaunch &fl, cudaStream_t 
 }
 
 }  // namespace raft
+
+namespace raft {
+
+// Shape of an FFT filter plan (length, radix passes, CTA size) without
+// allocating anything; returns false when the padded length needs the
+// direct-convolution path.  Used by the no-allocation FBP entry point.
+bool filter_plan_shape(FilterPlan &plan, int ftype, int N, int pad)
+{
+    plan.N = N;
+    plan.pad = pad;
+    plan.Np = N * (1 + pad);
+    plan.off = (pad * N) / 2;
+    plan.skip = (ftype == FILTER_NONE);
+    plan.threads = fft_threads(plan.Np);
+    plan.fft = factorize(plan.Np, plan.radix, plan.nradix) &&
+               2 * (size_t)plan.Np * sizeof(float2) <= kFilterSmemMax;
+    return plan.skip || plan.fft;
+}
+
+}  // namespace raft

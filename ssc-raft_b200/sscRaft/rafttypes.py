@@ -62,6 +62,8 @@ libraft.raft_fbp_ext.argtypes = [_P, _I, _P, _P, _P, _P, _P, _I, _I]
 libraft.raft_fbp_ext.restype = _I
 libraft.raft_fbp_device.argtypes = [_I, _P, _P, _P, _P, _P, _I, _I, _P]
 libraft.raft_fbp_device.restype = _I
+libraft.raft_fbp_device_noalloc.argtypes = [_I, _P, _P, _P, _P, _P, _I, _I, _P]
+libraft.raft_fbp_device_noalloc.restype = _I
 libraft.raft_em_ext.argtypes = [_I, _I, _P, _P, _P, _P, _I, _I, _I, _I, _P, _I]
 libraft.raft_em_ext.restype = _I
 libraft.raft_em_device.argtypes = [_I, _I, _P, _P, _P, _P, _I, _I, _I, _I, _P, _I, _P]
