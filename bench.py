@@ -188,7 +188,7 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     import sscRaft
-    from sscRaft.rafttypes import libraft, check_error, _ptr, GEOMETRY, STORE
+    from sscRaft.rafttypes import libraft, check_error, _ptr, GEOMETRY, STORE, autotune_table
 
     nsl = args.slices
     t0 = time.perf_counter()
@@ -253,7 +253,8 @@ def run_ours(args):
         ms, launches = time_device(g, s, args.steps, args.warmup)
         if rank == 0:
             print(json.dumps({"quick": True, "op": args.op, "slices": nsl, "ms_per_step": ms,
-                              "slices_per_s": ws * nsl / (ms / 1e3), "gpu_launches": int(launches)}), flush=True)
+                              "slices_per_s": ws * nsl / (ms / 1e3), "gpu_launches": int(launches),
+                              "autotune": autotune_table()}), flush=True)
         return
     result = {}
     with ClockSampler(local) as clk:
@@ -337,6 +338,7 @@ def run_ours(args):
             "kernel_ms": {"filter_per_launch": f_ms / max(1, f_n), "bp_per_launch": bp_ms / max(1, bp_n),
                           "launches_per_step": {"filter": f_n, "bp": bp_n}},
             "variants": variants,
+            "autotune": autotune_table(),
             "clocks": clocks,
             "gpu_launches": int(launches),
         }

@@ -133,6 +133,9 @@ int raft_fast_sincos(int gpu, const float *angles, int n, int kind, float *cos_o
  * this library in the process; optional CUDA-event timing of the filter (class 0),
  * backprojector (1) and projector (2) launches, summed since the last read. */
 long long raft_launch_count(void);
+/* JSON list of the backprojector launch shapes (slices per CTA, angles per stage) the
+ * autotuner chose so far in this process; returns the string length. */
+int raft_autotune_table(char *buf, int len);
 void raft_profile_enable(int on);
 int raft_profile_read(double *ms, long long *counts, int nclasses);
 

@@ -188,6 +188,18 @@ void raft_clear_error(void) { clear_error(); }
 
 int raft_abi_version(void) { return 1; }
 
+// JSON list of the backprojector launch shapes chosen so far by the autotuner.
+int raft_autotune_table(char *buf, int len)
+{
+    const std::string t = bp_tune_table();
+    if (buf && len > 0) {
+        const int n = (int)std::min<size_t>(t.size(), (size_t)len - 1);
+        std::memcpy(buf, t.data(), n);
+        buf[n] = 0;
+    }
+    return (int)t.size();
+}
+
 // --- FBP ------------------------------------------------------------------
 static void fbp_common(int *gpus, int ngpus, float *obj, const float *tomogram, const float *angles,
                        const float *paramf, const int *parami, int geometry, int store)

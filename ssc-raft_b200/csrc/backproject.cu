@@ -28,8 +28,14 @@
 #include "ptx.hpp"
 #include "profile.hpp"
 
-#include <cmath>
 #include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
 
 namespace raft {
 
@@ -58,7 +64,7 @@ struct BpArgs {
 };
 
 constexpr uint32_t kWaitLimit = 1u << 24;
-constexpr int kParamBytes = 2 * BP_AB * (int)sizeof(AngleParam);
+constexpr int kParamBytes = 2 * 32 * (int)sizeof(AngleParam);   // two stages of at most 32 angles
 constexpr int kWinOffset = 128 + kParamBytes;   // bytes before the windows
 
 static_assert(kWinOffset % 128 == 0, "window area alignment");
@@ -136,23 +142,33 @@ __device__ __forceinline__ float lerp_fetch(const unsigned char *w, int k, float
 
 // ------------------------------------------------------------------------
 // kernel
+//
+// S slices share one CTA: the per-pixel position, rounding and window index
+// are computed once per (pixel, angle) and reused for every slice, whose
+// windows sit side by side in shared memory ([angle][slice][W]), so the
+// per-slice address is the shared one plus an immediate offset.  AB (angles
+// per pipeline stage) is a launch parameter; S and AB are chosen by the
+// autotuner below.
 // ------------------------------------------------------------------------
-template <int GEOM, int STORE>
+template <int GEOM, int STORE, int S>
 __global__ void __launch_bounds__(BP_THREADS)
-bp_kernel(const BpArgs p)
+bp_kernel(const BpArgs p, const int AB)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     AngleParam *prm = reinterpret_cast<AngleParam *>(smem + 128);
     unsigned char *win = smem + kWinOffset;
-    const int esize = (STORE == STORE_PAIR_F32) ? 8 : 4;
+    constexpr int esize = (STORE == STORE_PAIR_F32) ? 8 : 4;
     const int W = p.W;
-    const int stage_bytes = BP_AB * W * esize;
+    const int wbytes = W * esize;                // one window
+    const int stage_bytes = AB * S * wbytes;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int x0 = blockIdx.x * BP_TX, y0 = blockIdx.y * BP_TY, slice = blockIdx.z;
+    const int x0 = blockIdx.x * BP_TX, y0 = blockIdx.y * BP_TY;
+    const int slice0 = blockIdx.z * S;
+    const int nsl = min(S, p.nslices - slice0);  // valid slices of this CTA
     const int A = p.nangles;
-    const int nst = (A + BP_AB - 1) / BP_AB;
+    const int nst = (A + AB - 1) / AB;
 
     // thread -> pixels: warp covers an 8 x 4 block per (i, j)
     const int lx = lane & 7, ly = lane >> 3;
@@ -170,36 +186,44 @@ bp_kernel(const BpArgs p)
     }
     __syncthreads();
 
-    const unsigned char *rows = p.filt + (size_t)slice * A * p.Wg * esize;
+    const unsigned char *rows = p.filt + (size_t)slice0 * A * p.Wg * esize;
+    const size_t slice_stride = (size_t)A * p.Wg * esize;
 
     auto issue = [&](int s, int b) {
-        // warp 0 only
-        const int a = s * BP_AB + lane;
-        const int na = min(BP_AB, A - s * BP_AB);
-        int base = 0;
+        // warp 0 only: one window base per angle, then one bulk copy per (angle, slice)
+        const int a0 = s * AB;
+        const int na = min(AB, A - a0);
         if (lane < na) {
             AngleParam ap;
-            angle_param<GEOM>(p, a, x0, y0, ap, base);
-            prm[b * BP_AB + lane] = ap;
+            int base;
+            angle_param<GEOM>(p, a0 + lane, x0, y0, ap, base);
+            prm[b * 32 + lane] = ap;
         }
         if (lane == 0) {
             fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&bars[b], (uint32_t)(na * W * esize));
+            mbar_arrive_expect_tx(&bars[b], (uint32_t)(na * nsl * wbytes));
         }
         __syncwarp();
-        if (lane < na)
-            bulk_g2s(win + (size_t)b * stage_bytes + (size_t)lane * W * esize,
-                     rows + ((size_t)a * p.Wg + base) * esize, (uint32_t)(W * esize), &bars[b]);
+        unsigned char *dst = win + (size_t)b * stage_bytes;
+        for (int c = lane; c < na * nsl; c += 32) {
+            const int al = c / nsl, sl = c - al * nsl;
+            const int base = prm[b * 32 + al].d - (GEOM == GEOM_FBP_LIN ? 0 : p.wlo);
+            bulk_g2s(dst + (size_t)(al * S + sl) * wbytes,
+                     rows + sl * slice_stride + ((size_t)(a0 + al) * p.Wg + base) * esize, (uint32_t)wbytes,
+                     &bars[b]);
+        }
     };
 
     if (warp == 0) issue(0, 0);
     __syncthreads();
 
-    float acc[2][4];
+    float acc[S][2][4];
 #pragma unroll
-    for (int j = 0; j < 2; j++)
+    for (int q = 0; q < S; q++)
 #pragma unroll
-        for (int i = 0; i < 4; i++) acc[j][i] = 0.f;
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+            for (int i = 0; i < 4; i++) acc[q][j][i] = 0.f;
 
     // per-thread coordinates in the reference's float arithmetic
     float xr[4], yr[2];
@@ -229,12 +253,12 @@ bp_kernel(const BpArgs p)
             if (p.err) atomicExch(p.err, 1);
             break;
         }
-        const int na = min(BP_AB, A - s * BP_AB);
+        const int na = min(AB, A - s * AB);
         const unsigned char *wb = win + (size_t)b * stage_bytes;
-        const AngleParam *pb = prm + b * BP_AB;
+        const AngleParam *pb = prm + b * 32;
         for (int al = 0; al < na; al++) {
             const AngleParam ap = pb[al];
-            const unsigned char *w = wb + (size_t)al * W * esize;
+            const unsigned char *w = wb + (size_t)al * S * wbytes;
             if constexpr (GEOM == GEOM_FBP_LIN) {
                 const float MAGIC = 12582912.0f;   // 1.5 * 2^23: fadd rounds to an integer
 #pragma unroll
@@ -244,34 +268,29 @@ bp_kernel(const BpArgs p)
                     for (int i = 0; i < 4; i++) {
                         const float v = fmaf(xr[i], ap.b, vrow);
                         const float m = __fadd_rn(v, MAGIC);
-                        const int k = __float_as_int(m) - 0x4B400000;
+                        const unsigned k = min((unsigned)(__float_as_int(m) - 0x4B400000), (unsigned)(W - 1));
                         const float f = __fsub_rn(v, __fsub_rn(m, MAGIC));
-                        acc[j][i] += lerp_fetch<STORE>(w, min((unsigned)k, (unsigned)(W - 1)), f);
+                        const unsigned char *wk = w + (size_t)k * esize;
+#pragma unroll
+                        for (int q = 0; q < S; q++)
+                            acc[q][j][i] += lerp_fetch<STORE>(wk + q * wbytes, 0, f);
                     }
                 }
-            } else if constexpr (GEOM == GEOM_FBP_REF) {
-                const float c = ap.a, sn = ap.b;
-                const int wbase = ap.d;
-                const float *wf = reinterpret_cast<const float *>(w);
-#pragma unroll
-                for (int j = 0; j < 2; j++)
-#pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        float t = xr[i] * c - yr[j] * sn;
-                        int ti = (int)((t - p.tmin) / p.dt);
-                        acc[j][i] += wf[min((unsigned)(ti - wbase), (unsigned)(W - 1))];
-                    }
             } else {
                 const float c = ap.a, sn = ap.b;
                 const int wbase = ap.d;
-                const float *wf = reinterpret_cast<const float *>(w);
 #pragma unroll
                 for (int j = 0; j < 2; j++)
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
-                        float t = xr[i] * c + yr[j] * sn;
+                        float t;
+                        if constexpr (GEOM == GEOM_FBP_REF) t = xr[i] * c - yr[j] * sn;
+                        else t = xr[i] * c + yr[j] * sn;
                         int ti = (int)((t - p.tmin) / p.dt);
-                        acc[j][i] += wf[min((unsigned)(ti - wbase), (unsigned)(W - 1))];
+                        const unsigned k = min((unsigned)(ti - wbase), (unsigned)(W - 1));
+                        const float *wk = reinterpret_cast<const float *>(w) + k;
+#pragma unroll
+                        for (int q = 0; q < S; q++) acc[q][j][i] += wk[q * W];
                     }
             }
         }
@@ -279,19 +298,23 @@ bp_kernel(const BpArgs p)
     }
     if (!ok) return;
 
-    float *out = p.img + (size_t)slice * p.No * p.No;
-    const float *den = p.den ? p.den + (size_t)slice * p.No * p.No : nullptr;
 #pragma unroll
-    for (int j = 0; j < 2; j++)
+    for (int q = 0; q < S; q++) {
+        if (q >= nsl) break;
+        float *out = p.img + (size_t)(slice0 + q) * p.No * p.No;
+        const float *den = p.den ? p.den + (size_t)(slice0 + q) * p.No * p.No : nullptr;
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const int X = x0 + li[i], Y = y0 + lj[j];
-            if (X < p.No && Y < p.No) {
-                const size_t o = (size_t)Y * p.No + X;
-                if (p.update) out[o] = out[o] * acc[j][i] / den[o];
-                else out[o] = acc[j][i];
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int X = x0 + li[i], Y = y0 + lj[j];
+                if (X < p.No && Y < p.No) {
+                    const size_t o = (size_t)Y * p.No + X;
+                    if (p.update) out[o] = out[o] * acc[q][j][i] / den[o];
+                    else out[o] = acc[q][j][i];
+                }
             }
-        }
+    }
 }
 
 // ------------------------------------------------------------------------
@@ -377,24 +400,134 @@ WindowLayout plan_window(const BpPlanInput &in)
     return L;
 }
 
-template <int GEOM, int STORE>
-static void launch_bp_t(const BpArgs &a, int nslices, cudaStream_t st)
+// ------------------------------------------------------------------------
+// launch + autotuner
+// ------------------------------------------------------------------------
+constexpr size_t kBpSmemMax = 100 * 1024;
+
+static size_t bp_smem(int S, int AB, int W, int esize)
+{
+    return kWinOffset + 2 * (size_t)AB * S * W * esize;
+}
+
+template <int GEOM, int STORE, int S>
+static void launch_bp_s(const BpArgs &a, int AB, cudaStream_t st)
 {
     const int esize = (STORE == STORE_PAIR_F32) ? 8 : 4;
-    const size_t smem = kWinOffset + 2 * (size_t)BP_AB * a.W * esize;
+    const size_t smem = bp_smem(S, AB, a.W, esize);
+    RAFT_CHECK(smem <= kBpSmemMax && AB >= 1 && AB <= 32, "backprojector: staged window too large");
     static thread_local int configured = -1;
     int dev = 0;
     cudaGetDevice(&dev);
     if (configured != dev) {
-        RAFT_CUDA(cudaFuncSetAttribute(bp_kernel<GEOM, STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       200 * 1024));
+        RAFT_CUDA(cudaFuncSetAttribute(bp_kernel<GEOM, STORE, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kBpSmemMax));
         configured = dev;
     }
-    RAFT_CHECK(smem <= 200 * 1024, "backprojector: staged window too large");
-    dim3 grid((a.No + BP_TX - 1) / BP_TX, (a.No + BP_TY - 1) / BP_TY, nslices);
+    dim3 grid((a.No + BP_TX - 1) / BP_TX, (a.No + BP_TY - 1) / BP_TY, (a.nslices + S - 1) / S);
     ProfScope ps(PROF_BACKPROJECT, st);
-    bp_kernel<GEOM, STORE><<<grid, BP_THREADS, smem, st>>>(a);
+    bp_kernel<GEOM, STORE, S><<<grid, BP_THREADS, smem, st>>>(a, AB);
     RAFT_CUDA(cudaGetLastError());
+}
+
+template <int GEOM, int STORE>
+static void launch_bp_cfg(const BpArgs &a, BpTune t, cudaStream_t st)
+{
+    switch (t.S) {
+    case 1: launch_bp_s<GEOM, STORE, 1>(a, t.AB, st); break;
+    case 2: launch_bp_s<GEOM, STORE, 2>(a, t.AB, st); break;
+    default: launch_bp_s<GEOM, STORE, 4>(a, t.AB, st); break;
+    }
+}
+
+static void launch_bp_any(const BpArgs &a, int geometry, int store, BpTune t, cudaStream_t st)
+{
+    switch (geometry) {
+    case GEOM_FBP_REF: launch_bp_cfg<GEOM_FBP_REF, STORE_F32>(a, t, st); break;
+    case GEOM_EM_REF: launch_bp_cfg<GEOM_EM_REF, STORE_F32>(a, t, st); break;
+    default:
+        if (store == STORE_PAIR_BF16) launch_bp_cfg<GEOM_FBP_LIN, STORE_PAIR_BF16>(a, t, st);
+        else launch_bp_cfg<GEOM_FBP_LIN, STORE_PAIR_F32>(a, t, st);
+        break;
+    }
+}
+
+// Tuning table: (device, geometry, store, No, W, nangles) -> (S, AB).
+using TuneKey = std::tuple<int, int, int, int, int, int>;
+static std::mutex g_tune_mtx;
+static std::map<TuneKey, BpTune> g_tune;
+
+static const BpTune kTuneCandidates[] = {{1, 32}, {1, 16}, {2, 32}, {2, 16}, {2, 8}, {4, 16}, {4, 8}};
+
+static bool tuning_enabled()
+{
+    const char *e = std::getenv("RAFT_BP_TUNE");
+    return !(e && e[0] == '0');
+}
+
+// Pick (S, AB) for this configuration: the cached choice, else time every
+// candidate that fits shared memory on up to 8 slices of the real data
+// (store launches only -- they are idempotent), else a default.
+static BpTune choose_tune(const BpArgs &a, int geometry, int store, cudaStream_t st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const TuneKey key(dev, geometry, store, a.No, a.W, a.nangles);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mtx);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) return it->second;
+    }
+    const int esize = store_bytes(store);
+    BpTune best{2, 16};
+    if (bp_smem(best.S, best.AB, a.W, esize) > kBpSmemMax) best = {1, 8};
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cap);
+    const bool can_tune = tuning_enabled() && a.update == 0 && cap == cudaStreamCaptureStatusNone;
+    if (can_tune) {
+        BpArgs t = a;
+        t.nslices = std::min(a.nslices, 8);
+        cudaEvent_t e0, e1;
+        RAFT_CUDA(cudaEventCreate(&e0));
+        RAFT_CUDA(cudaEventCreate(&e1));
+        float best_ms = 1e30f;
+        for (const BpTune &c : kTuneCandidates) {
+            if (bp_smem(c.S, c.AB, a.W, esize) > kBpSmemMax) continue;
+            launch_bp_any(t, geometry, store, c, st);   // warm
+            RAFT_CUDA(cudaEventRecord(e0, st));
+            launch_bp_any(t, geometry, store, c, st);
+            launch_bp_any(t, geometry, store, c, st);
+            RAFT_CUDA(cudaEventRecord(e1, st));
+            RAFT_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            RAFT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    if (can_tune || !tuning_enabled()) {
+        std::lock_guard<std::mutex> lk(g_tune_mtx);
+        g_tune[key] = best;
+    }
+    return best;
+}
+
+std::string bp_tune_table()
+{
+    std::lock_guard<std::mutex> lk(g_tune_mtx);
+    std::string out = "[";
+    for (auto &kv : g_tune) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "%s{\"geometry\":%d,\"store\":%d,\"N\":%d,\"W\":%d,\"nangles\":%d,\"S\":%d,\"AB\":%d}",
+                 out.size() > 1 ? "," : "", std::get<1>(kv.first), std::get<2>(kv.first), std::get<3>(kv.first),
+                 std::get<4>(kv.first), std::get<5>(kv.first), kv.second.S, kv.second.AB);
+        out += buf;
+    }
+    return out + "]";
 }
 
 void launch_backproject(const BpLaunch &bl, cudaStream_t st)
@@ -429,18 +562,9 @@ void launch_backproject(const BpLaunch &bl, cudaStream_t st)
     a.snd = bl.snd;
     a.err = bl.err;
     a.update = bl.den ? 1 : 0;
-    switch (bl.geometry) {
-    case GEOM_FBP_REF:
-        launch_bp_t<GEOM_FBP_REF, STORE_F32>(a, bl.nslices, st);
-        break;
-    case GEOM_EM_REF:
-        launch_bp_t<GEOM_EM_REF, STORE_F32>(a, bl.nslices, st);
-        break;
-    default:
-        if (bl.store == STORE_PAIR_BF16) launch_bp_t<GEOM_FBP_LIN, STORE_PAIR_BF16>(a, bl.nslices, st);
-        else launch_bp_t<GEOM_FBP_LIN, STORE_PAIR_F32>(a, bl.nslices, st);
-        break;
-    }
+    const int store = bl.geometry == GEOM_FBP_LIN ? bl.store : STORE_F32;
+    const BpTune t = choose_tune(a, bl.geometry, store, st);
+    launch_bp_any(a, bl.geometry, store, t, st);
 }
 
 }  // namespace raft

@@ -116,7 +116,7 @@ struct WindowLayout {
 constexpr int BP_THREADS = 256;
 constexpr int BP_TX = 64;     // tile width  (pixels)
 constexpr int BP_TY = 32;     // tile height (pixels)
-constexpr int BP_AB = 32;     // angles per pipeline stage
+constexpr int BP_AB = 32;     // maximum angles per pipeline stage
 
 // Geometry constants of one backprojection, in the reference's FP32
 // arithmetic (FBP: fbp.cu:38-44; EM: em_RT_kernel.cu:97-102).
@@ -152,6 +152,13 @@ struct BpLaunch {
 };
 
 void launch_backproject(const BpLaunch &bl, cudaStream_t st);
+
+// Backprojector launch shape chosen by the autotuner: S slices per CTA
+// (sharing each pixel's position arithmetic) and AB angles per pipeline stage.
+struct BpTune {
+    int S, AB;
+};
+std::string bp_tune_table();   // JSON list of the tuned configurations
 
 // sin/cos with the reference's fast intrinsics (__sinf/__cosf for FBP,
 // opt.cu:187-194; __sincosf for EM, em_RT_kernel.cu:120) and the per-angle

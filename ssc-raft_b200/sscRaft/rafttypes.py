@@ -71,6 +71,8 @@ libraft.raft_em_device.restype = _I
 
 libraft.raft_launch_count.argtypes = []
 libraft.raft_launch_count.restype = ctypes.c_longlong
+libraft.raft_autotune_table.argtypes = [ctypes.c_char_p, _I]
+libraft.raft_autotune_table.restype = _I
 libraft.raft_profile_enable.argtypes = [_I]
 libraft.raft_profile_enable.restype = None
 libraft.raft_profile_read.argtypes = [_P, _P, _I]
@@ -82,6 +84,14 @@ libraft.raft_fast_sincos.argtypes = [_I, _P, _I, _I, _P, _P]
 libraft.raft_fast_sincos.restype = _I
 
 GEOMETRY = {"nearest": 0, "linear": 1}
+
+
+def autotune_table():
+    """Backprojector launch shapes chosen by the autotuner in this process."""
+    import json
+    buf = ctypes.create_string_buffer(1 << 16)
+    libraft.raft_autotune_table(buf, 1 << 16)
+    return json.loads(buf.value.decode() or "[]")
 
 
 def fast_sincos(angles, kind=0, gpu=0):
