@@ -32,129 +32,199 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
-template <int EM, int EPI>
+// S slices per thread share every sample's position and pixel index (the
+// geometry is the same for all slices).  Warps whose angle is steeper than
+// 45 degrees read a transposed copy of the images (imgT[x][y]) so that the
+// 32 rays of the warp touch consecutive addresses; the index arithmetic and
+// therefore the chosen pixels are unchanged.
+template <int EM, int EPI, int S>
 __global__ void __launch_bounds__(PJ_RAYS * PJ_ANGLES)
 project_kernel(const ProjLaunch p)
 {
     const int i = blockIdx.x * PJ_RAYS + threadIdx.x;     // ray
     const int j = blockIdx.y * PJ_ANGLES + threadIdx.y;   // angle
-    const int k = blockIdx.z;                             // slice
+    const int k0 = blockIdx.z * S;                        // first slice
+    const int nsl = min(S, p.nslices - k0);
     const bool valid = (i < p.nrays) && (j < p.nangles);
     const int nx = p.nx, ny = p.ny;
-    const float *img = p.img + (size_t)k * nx * ny;
-    float value = 0.f;
+    const size_t plane = (size_t)nx * ny;
+    float value[S];
+#pragma unroll
+    for (int q = 0; q < S; q++) value[q] = 0.f;
     if (valid) {
+        const float ang = p.angles[j];
+        const float ctheta = __cosf(ang);
+        const float stheta = __sinf(ang);
+        const bool steep = p.imgT && fabsf(stheta) > fabsf(ctheta);
+        const float *img = (steep ? p.imgT : p.img) + (size_t)k0 * plane;
+        // address = Y*nx + X (row-major) or X*ny + Y (transposed)
+        const int sy = steep ? 1 : nx, sx = steep ? ny : 1;
+        float linesum[S];
+#pragma unroll
+        for (int q = 0; q < S; q++) linesum[q] = 0.f;
         if constexpr (EM) {
             // kernel_radon: dt = 2.0*a/(nrays-1) in double, a = 1
             const float a = p.ax;
             const float dt = (float)(2.0 * a / (p.nrays - 1));
-            const float ctheta = __cosf(p.angles[j]);
-            const float stheta = __sinf(p.angles[j]);
             const float t = -a + i * dt;
-            float linesum = 0.f;
             for (int m = 0; m < p.nrays; m++) {
                 const float s = -a + m * dt;
                 const float x = t * ctheta - s * stheta;
                 const float y = t * stheta + s * ctheta;
                 const int X = (int)((x + 1) / dt);
                 const int Y = (int)((y + 1) / dt);
-                if ((X >= 0) & (X < nx) & (Y >= 0) & (Y < nx))
-                    linesum += __ldg(&img[Y * nx + X]);
+                if ((X >= 0) & (X < nx) & (Y >= 0) & (Y < nx)) {
+                    const float *pix = img + (size_t)Y * sy + (size_t)X * sx;
+#pragma unroll
+                    for (int q = 0; q < S; q++)
+                        if (q < nsl) linesum[q] += __ldg(pix + q * plane);
+                }
             }
-            value = linesum * dt;
+#pragma unroll
+            for (int q = 0; q < S; q++) value[q] = linesum[q] * dt;
         } else {
             const float dx = 2.0f * p.ax / (float)(unsigned)(nx - 1);
             const float dy = 2.0f * p.ay / (float)(unsigned)(ny - 1);
-            const float ctheta = __cosf(p.angles[j]);
-            const float stheta = __sinf(p.angles[j]);
             const float t = -p.ax + i * dx;
-            float linesum = 0.f;
             for (int r = 0; r < ny; r++) {
                 const float s = -p.ay + r * dy;
                 const float x = t * ctheta - s * stheta;
                 const float y = t * stheta + s * ctheta;
                 const int ix = (int)((x + 1) / dx);
                 const int iy = (int)((y + 1) / dy);
-                if ((ix >= 0) & (ix < nx) & (iy >= 0) & (iy < ny))
-                    linesum += __ldg(&img[(size_t)iy * nx + ix]);
+                if ((ix >= 0) & (ix < nx) & (iy >= 0) & (iy < ny)) {
+                    const float *pix = img + (size_t)iy * sy + (size_t)ix * sx;
+#pragma unroll
+                    for (int q = 0; q < S; q++)
+                        if (q < nsl) linesum[q] += __ldg(pix + q * plane);
+                }
             }
-            value = linesum * dy;
+#pragma unroll
+            for (int q = 0; q < S; q++) value[q] = linesum[q] * dy;
         }
     }
 
-    const size_t vox = ((size_t)k * p.nangles + j) * p.nrays + i;
-    float q = value;
-    double r2 = 0.0, y2 = 0.0, nll = 0.0;
-    if (valid) {
+    double r2[S], y2[S], nll[S];
+#pragma unroll
+    for (int q = 0; q < S; q++) r2[q] = y2[q] = nll[q] = 0.0;
+#pragma unroll
+    for (int q = 0; q < S; q++) {
+        const int k = k0 + q;
+        if (!valid || q >= nsl) continue;
+        const size_t vox = ((size_t)k * p.nangles + j) * p.nrays + i;
+        float out = value[q];
         if constexpr (EPI == 1) {
-            // tEM: model = flat * exp(-p); data = counts
+            // tEM: model = flat * exp(-p); data = counts (kernel_flatTimesExp, em_RT_kernel.cu:20-32)
             const float fl = p.flat[(size_t)k * p.nrays + i];
-            q = fl * __expf(-value);
+            out = fl * __expf(-value[q]);
             if (p.metrics) {
                 const double y = p.data[vox];
-                const double m = fl * exp(-(double)value);
-                r2 = (m - y) * (m - y);
-                y2 = y * y;
-                nll = m + y * (double)value;
+                const double m = fl * exp(-(double)value[q]);
+                r2[q] = (m - y) * (m - y);
+                y2[q] = y * y;
+                nll[q] = m + y * (double)value[q];
             }
         } else if constexpr (EPI == 2) {
             // eEM ratio, APPROXINVX(value, 1e-4) = SIGN/sqrtf(SQR(e)+SQR(x)) (configs.hpp:30-32)
             const float TOLZERO = 0.0001f;
             const float y = p.data[vox];
-            const int sgn = (value > 0) ? 1 : ((value < 0) ? -1 : 0);
-            q = y * (sgn / sqrtf(TOLZERO * TOLZERO + value * value));
-            if (q < 0) q = 0.0f;
+            const int sgn = (value[q] > 0) ? 1 : ((value[q] < 0) ? -1 : 0);
+            out = y * (sgn / sqrtf(TOLZERO * TOLZERO + value[q] * value[q]));
+            if (out < 0) out = 0.0f;
             if (p.metrics) {
-                const double yd = y, m = value;
-                r2 = (m - yd) * (m - yd);
-                y2 = yd * yd;
-                nll = (m > 0) ? m - yd * log(m) : 0.0;
+                const double yd = y, m = value[q];
+                r2[q] = (m - yd) * (m - yd);
+                y2[q] = yd * yd;
+                nll[q] = (m > 0) ? m - yd * log(m) : 0.0;
             }
         }
         if (p.windowed) {
             const float w = p.wt ? p.wt[j] : 1.f;
-            p.out[((size_t)k * p.nangles + j) * p.Wg + (i - p.wlo)] = q * w;
+            p.out[((size_t)k * p.nangles + j) * p.Wg + (i - p.wlo)] = out * w;
         } else {
-            p.out[vox] = q;
+            p.out[vox] = out;
         }
     }
     if constexpr (EPI != 0) {
         if (p.metrics) {
-            __shared__ double red[3][PJ_ANGLES];
-            r2 = warp_sum(r2);
-            y2 = warp_sum(y2);
-            nll = warp_sum(nll);
-            if (threadIdx.x == 0) {
-                red[0][threadIdx.y] = r2;
-                red[1][threadIdx.y] = y2;
-                red[2][threadIdx.y] = nll;
+            // FP64 per-slice sums: warp shuffle, then across the block's warps
+            __shared__ double red[3][S][PJ_ANGLES];
+#pragma unroll
+            for (int q = 0; q < S; q++) {
+                const double a0 = warp_sum(r2[q]), a1 = warp_sum(y2[q]), a2 = warp_sum(nll[q]);
+                if (threadIdx.x == 0) {
+                    red[0][q][threadIdx.y] = a0;
+                    red[1][q][threadIdx.y] = a1;
+                    red[2][q][threadIdx.y] = a2;
+                }
             }
             __syncthreads();
-            if (threadIdx.y == 0 && threadIdx.x < 3) {
-                double s = 0.0;
-                for (int w = 0; w < PJ_ANGLES; w++) s += red[threadIdx.x][w];
-                atomicAdd(&p.metrics[(size_t)k * 3 + threadIdx.x], s);
+            if (threadIdx.y == 0 && threadIdx.x < 3 * S) {
+                const int q = threadIdx.x / 3, c = threadIdx.x - 3 * q;
+                if (q < nsl) {
+                    double sum = 0.0;
+                    for (int w = 0; w < PJ_ANGLES; w++) sum += red[c][q][w];
+                    atomicAdd(&p.metrics[(size_t)(k0 + q) * 3 + c], sum);
+                }
             }
         }
     }
 }
 
+// Tiled transpose of each slice: out[k][x][y] = in[k][y][x].
+__global__ void transpose_kernel(const float *__restrict__ in, float *__restrict__ out, int nx, int ny)
+{
+    __shared__ float tile[32][33];
+    const size_t plane = (size_t)nx * ny;
+    const float *src = in + blockIdx.z * plane;
+    float *dst = out + blockIdx.z * plane;
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int y = by + r, x = bx + threadIdx.x;
+        if (x < nx && y < ny) tile[r][threadIdx.x] = src[(size_t)y * nx + x];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int x = bx + r, y = by + threadIdx.x;
+        if (x < nx && y < ny) dst[(size_t)x * ny + y] = tile[threadIdx.x][r];
+    }
+}
+
+void launch_transpose(const float *in, float *out, int nx, int ny, int nslices, cudaStream_t st)
+{
+    if (nslices <= 0) return;
+    count_launch();
+    dim3 grid((nx + 31) / 32, (ny + 31) / 32, nslices);
+    transpose_kernel<<<grid, dim3(32, 8), 0, st>>>(in, out, nx, ny);
+    RAFT_CUDA(cudaGetLastError());
+}
+
+template <int EM, int EPI>
+static void launch_project_s(const ProjLaunch &pl, int S, cudaStream_t st)
+{
+    dim3 block(PJ_RAYS, PJ_ANGLES);
+    dim3 grid((pl.nrays + PJ_RAYS - 1) / PJ_RAYS, (pl.nangles + PJ_ANGLES - 1) / PJ_ANGLES,
+              (pl.nslices + S - 1) / S);
+    ProfScope ps(PROF_PROJECT, st);
+    if (S == 4) project_kernel<EM, EPI, 4><<<grid, block, 0, st>>>(pl);
+    else if (S == 2) project_kernel<EM, EPI, 2><<<grid, block, 0, st>>>(pl);
+    else project_kernel<EM, EPI, 1><<<grid, block, 0, st>>>(pl);
+    RAFT_CUDA(cudaGetLastError());
+}
+
 void launch_project(const ProjLaunch &pl, cudaStream_t st)
 {
     if (pl.nslices <= 0 || pl.nangles <= 0 || pl.nrays <= 0) return;
-    ProfScope ps(PROF_PROJECT, st);
-    dim3 block(PJ_RAYS, PJ_ANGLES);
-    dim3 grid((pl.nrays + PJ_RAYS - 1) / PJ_RAYS, (pl.nangles + PJ_ANGLES - 1) / PJ_ANGLES, pl.nslices);
+    const int S = pl.nslices >= 4 ? 4 : (pl.nslices >= 2 ? 2 : 1);
     if (!pl.em) {
-        project_kernel<0, 0><<<grid, block, 0, st>>>(pl);
+        launch_project_s<0, 0>(pl, S, st);
     } else {
         switch (pl.epilogue) {
-        case 1: project_kernel<1, 1><<<grid, block, 0, st>>>(pl); break;
-        case 2: project_kernel<1, 2><<<grid, block, 0, st>>>(pl); break;
-        default: project_kernel<1, 0><<<grid, block, 0, st>>>(pl); break;
+        case 1: launch_project_s<1, 1>(pl, S, st); break;
+        case 2: launch_project_s<1, 2>(pl, S, st); break;
+        default: launch_project_s<1, 0>(pl, S, st); break;
         }
     }
-    RAFT_CUDA(cudaGetLastError());
 }
 
 // Plain sinogram -> weighted window rows (the rest of each row stays zero).

@@ -169,6 +169,7 @@ void launch_angle_tables(const float *d_angles, int nangles, float *d_cos, float
 // ------------------------------------------------------------ projector --
 struct ProjLaunch {
     const float *img = nullptr;     // [nslices][ny][nx]
+    const float *imgT = nullptr;    // optional transposed copy [nslices][nx][ny] for steep angles
     float *out = nullptr;           // plain [nslices][nangles][nrays] or window rows
     const float *angles = nullptr;
     int nx = 0, ny = 0, nrays = 0, nangles = 0, nslices = 0;
@@ -183,6 +184,9 @@ struct ProjLaunch {
 };
 
 void launch_project(const ProjLaunch &pl, cudaStream_t st);
+
+// out[k][x][y] = in[k][y][x] for each of nslices planes.
+void launch_transpose(const float *in, float *out, int nx, int ny, int nslices, cudaStream_t st);
 
 // Copy a plain sinogram into weighted window rows (EM: BP of the counts).
 void launch_to_window(const float *sino, float *rows, const float *wt, int nrows, int nangles,
