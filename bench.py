@@ -322,6 +322,12 @@ def run_ours(args):
         return ms[0], cnt[0], ms[1], cnt[1]
 
     hbm_peak, sm_max, peak_kind = peaks()
+    if args.quick and args.op == "tem":
+        # profiling mode: a short tEM run (args.slices x 1024^2, 900 angles)
+        r = run_tem(local, dev, nslices=args.slices, iters=args.steps, warm_iters=args.warmup)
+        if rank == 0:
+            print(json.dumps({"quick": True, "op": "tem", **r}), flush=True)
+        return
     if args.quick:
         # profiling mode: only the device-resident FBP of the chosen operator
         g, s = {"nearest": (0, 0), "linear": (1, 1), "linear_bf16": (1, 2)}[args.op]
@@ -496,7 +502,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-em", action="store_true")
     ap.add_argument("--quick", action="store_true", help="device timing of one operator only (profiling)")
-    ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16"])
+    ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "tem"])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
