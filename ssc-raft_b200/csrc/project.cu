@@ -62,43 +62,59 @@ project_kernel(const ProjLaunch p)
         float linesum[S];
 #pragma unroll
         for (int q = 0; q < S; q++) linesum[q] = 0.f;
-        if constexpr (EM) {
-            // kernel_radon: dt = 2.0*a/(nrays-1) in double, a = 1
-            const float a = p.ax;
-            const float dt = (float)(2.0 * a / (p.nrays - 1));
-            const float t = -a + i * dt;
-            for (int m = 0; m < p.nrays; m++) {
-                const float s = -a + m * dt;
+        // Samples are processed four at a time: the four positions and pixel
+        // loads are issued together (independent, so their latency overlaps),
+        // then added in sample order, exactly as the reference's sequential sum.
+        auto sample_loop = [&](const float t, const float d0, const float ay0, const float ddx,
+                               const float ddy, const int nsamp, const int limx, const int limy) {
+            int m = 0;
+            for (; m + 4 <= nsamp; m += 4) {
+                float v[4][S];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const float s = -ay0 + (m + u) * d0;
+                    const float x = t * ctheta - s * stheta;
+                    const float y = t * stheta + s * ctheta;
+                    const int X = (int)((x + 1) / ddx);
+                    const int Y = (int)((y + 1) / ddy);
+                    const bool in = (X >= 0) & (X < limx) & (Y >= 0) & (Y < limy);
+                    const float *pix = img + (size_t)(in ? Y : 0) * sy + (size_t)(in ? X : 0) * sx;
+#pragma unroll
+                    for (int q = 0; q < S; q++) v[u][q] = (in && q < nsl) ? __ldg(pix + q * plane) : 0.f;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+#pragma unroll
+                    for (int q = 0; q < S; q++) linesum[q] += v[u][q];
+            }
+            for (; m < nsamp; m++) {
+                const float s = -ay0 + m * d0;
                 const float x = t * ctheta - s * stheta;
                 const float y = t * stheta + s * ctheta;
-                const int X = (int)((x + 1) / dt);
-                const int Y = (int)((y + 1) / dt);
-                if ((X >= 0) & (X < nx) & (Y >= 0) & (Y < nx)) {
+                const int X = (int)((x + 1) / ddx);
+                const int Y = (int)((y + 1) / ddy);
+                if ((X >= 0) & (X < limx) & (Y >= 0) & (Y < limy)) {
                     const float *pix = img + (size_t)Y * sy + (size_t)X * sx;
 #pragma unroll
                     for (int q = 0; q < S; q++)
                         if (q < nsl) linesum[q] += __ldg(pix + q * plane);
                 }
             }
+        };
+        if constexpr (EM) {
+            // kernel_radon: dt = 2.0*a/(nrays-1) in double, a = 1; one step for
+            // rays, samples and pixels; the image is N x N with N = nx
+            const float a = p.ax;
+            const float dt = (float)(2.0 * a / (p.nrays - 1));
+            const float t = -a + i * dt;
+            sample_loop(t, dt, a, dt, dt, p.nrays, nx, nx);
 #pragma unroll
             for (int q = 0; q < S; q++) value[q] = linesum[q] * dt;
         } else {
             const float dx = 2.0f * p.ax / (float)(unsigned)(nx - 1);
             const float dy = 2.0f * p.ay / (float)(unsigned)(ny - 1);
             const float t = -p.ax + i * dx;
-            for (int r = 0; r < ny; r++) {
-                const float s = -p.ay + r * dy;
-                const float x = t * ctheta - s * stheta;
-                const float y = t * stheta + s * ctheta;
-                const int ix = (int)((x + 1) / dx);
-                const int iy = (int)((y + 1) / dy);
-                if ((ix >= 0) & (ix < nx) & (iy >= 0) & (iy < ny)) {
-                    const float *pix = img + (size_t)iy * sy + (size_t)ix * sx;
-#pragma unroll
-                    for (int q = 0; q < S; q++)
-                        if (q < nsl) linesum[q] += __ldg(pix + q * plane);
-                }
-            }
+            sample_loop(t, dy, p.ay, dx, dy, ny, nx, ny);
 #pragma unroll
             for (int q = 0; q < S; q++) value[q] = linesum[q] * dy;
         }
