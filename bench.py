@@ -51,6 +51,23 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(x, device=None):
+    """Max of a per-rank float over all ranks (the timing reduction); identity
+    without an initialised process group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def slice_seed_base(rank, nslices):
+    """Per-rank seed base: every rank reconstructs its own distinct slices."""
+    return 2_000_000 + rank * nslices
+
+
 # ------------------------------------------------------------------ data --
 def make_sinograms_gpu(nslices, seed_base, device):
     """Exact ellipse projections (50 ellipses/slice) + Poisson noise, on the GPU."""
@@ -267,7 +284,7 @@ def run_ours(args):
 
     nsl = args.slices
     t0 = time.perf_counter()
-    sino, ang = make_sinograms_gpu(nsl, 2_000_000 + rank * nsl, dev)
+    sino, ang = make_sinograms_gpu(nsl, slice_seed_base(rank, nsl), dev)
     torch.cuda.synchronize()
     log(f"[rank {rank}] generated {nsl} sinograms in {time.perf_counter() - t0:.1f} s")
     img = torch.empty((nsl, N_RAYS, N_RAYS), dtype=torch.float32, device=dev)
@@ -279,13 +296,8 @@ def run_ours(args):
             import torch.distributed as dist
             dist.barrier()
 
-    def max_over_ranks(x):
-        if ws == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def ranks_max(x):
+        return max_over_ranks(x, dev)
 
     def device_step(geometry, store):
         st = torch.cuda.current_stream(dev).cuda_stream
@@ -309,7 +321,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier()
         launches = libraft.raft_launch_count() - n0
-        return max_over_ranks(e0.elapsed_time(e1) / K), launches
+        return ranks_max(e0.elapsed_time(e1) / K), launches
 
     def profile_bp(geometry, store):
         libraft.raft_profile_enable(1)
@@ -356,7 +368,7 @@ def run_ours(args):
             sscRaft.fbp(hs, dic=dict(dic), obj=hi)
             t_e2e.append(time.perf_counter() - t1)
         barrier()
-        ms_e2e = max_over_ranks(1e3 * sum(t_e2e) / len(t_e2e))
+        ms_e2e = ranks_max(1e3 * sum(t_e2e) / len(t_e2e))
         # parity spot check of the e2e output against the device-path output
         spot = float((torch.from_numpy(hi[nsl // 2]).to(dev) - img[nsl // 2]).abs().max())
         variants = {}

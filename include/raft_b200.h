@@ -119,6 +119,11 @@ int raft_em_device(int kind, int gpu, float *d_obj, const float *d_data, const f
                    const float *angles, int nrays, int nangles, int nslices, int niter,
                    double *d_metrics, int use_graph, void *stream);
 
+/* Host-only: slab of slices each of ngpus devices gets in the *MultiGPU calls --
+ * contiguous blocks of ceil(nslices/ngpus), as the reference's split
+ * (fbp.cu:267-301, em_rt.cu:43-81).  Returns 0 on success. */
+int raft_slab_partition(int nslices, int ngpus, int *start, int *count);
+
 /* Host-only helper (no GPU needed, no reference counterpart): the detector-window
  * layout the backprojector stages for a configuration; out = {wlo, Wg, W, align}.
  * geometry 0/1 with FBP packing, 2 with EM packing.  Returns 0 on success. */

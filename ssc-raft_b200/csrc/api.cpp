@@ -119,12 +119,25 @@ static bool check_gpus(const int *gpus, int ngpus)
     return true;
 }
 
-// Contiguous z-slabs, one host thread per device (fbp.cu:267-301); errors
-// from worker threads are carried back into the caller's status.
+// Contiguous z-slabs of ceil(nslices/ngpus) slices, the last ones shorter or
+// empty (fbp.cu:267-301).
+static void slab_partition(int nslices, int ngpus, int *start, int *count)
+{
+    const int sub = (nslices + ngpus - 1) / ngpus;
+    int ptr = 0;
+    for (int i = 0; i < ngpus; i++) {
+        const int n = std::max(0, std::min(nslices - ptr, sub));
+        start[i] = ptr;
+        count[i] = n;
+        ptr += n;
+    }
+}
+
+// One host thread per device over its slab; errors from worker threads are
+// carried back into the caller's status.
 template <class F>
 static void split_slabs(const int *gpus, int ngpus, int nslices, F work)
 {
-    const int sub = (nslices + ngpus - 1) / ngpus;
     if (ngpus == 1) {
         try {
             work(gpus[0], 0, nslices);
@@ -136,10 +149,11 @@ static void split_slabs(const int *gpus, int ngpus, int nslices, F work)
     }
     std::vector<std::thread> th;
     std::vector<std::string> errs(ngpus);
-    int ptr = 0;
+    std::vector<int> starts(ngpus), counts(ngpus);
+    slab_partition(nslices, ngpus, starts.data(), counts.data());
     for (int i = 0; i < ngpus; i++) {
-        const int n = std::max(0, std::min(nslices - ptr, sub));
-        const int start = ptr;
+        const int n = counts[i];
+        const int start = starts[i];
         th.emplace_back([&, i, start, n] {
             try {
                 work(gpus[i], start, n);
@@ -149,7 +163,6 @@ static void split_slabs(const int *gpus, int ngpus, int nslices, F work)
             }
             errs[i] = get_error();
         });
-        ptr += n;
     }
     for (auto &t : th) t.join();
     for (auto &e : errs)
@@ -187,6 +200,18 @@ int raft_last_error(char *buf, int len)
 void raft_clear_error(void) { clear_error(); }
 
 int raft_abi_version(void) { return 1; }
+
+// Host-only: the slab each of `ngpus` devices receives for `nslices` slices.
+int raft_slab_partition(int nslices, int ngpus, int *start, int *count)
+{
+    clear_error();
+    if (nslices < 0 || ngpus < 1 || !start || !count) {
+        set_error("raft_slab_partition: bad arguments");
+        return 1;
+    }
+    slab_partition(nslices, ngpus, start, count);
+    return 0;
+}
 
 // JSON list of the backprojector launch shapes chosen so far by the autotuner.
 int raft_autotune_table(char *buf, int len)

@@ -78,6 +78,8 @@ libraft.raft_profile_enable.restype = None
 libraft.raft_profile_read.argtypes = [_P, _P, _I]
 libraft.raft_profile_read.restype = _I
 
+libraft.raft_slab_partition.argtypes = [_I, _I, _P, _P]
+libraft.raft_slab_partition.restype = _I
 libraft.raft_plan_window.argtypes = [_P, _P, _I, _I, _P]
 libraft.raft_plan_window.restype = _I
 libraft.raft_fast_sincos.argtypes = [_I, _P, _I, _I, _P, _P]
