@@ -177,6 +177,56 @@ def run_tem(local, dev, nslices=EM_SLICES, iters=EM_ITERS, warm_iters=3):
             "metrics": "FP64 data residual ||flat*exp(-Ax)-y||/||y|| and Poisson NLL per iteration"}
 
 
+# ----------------------------------------------------------- ragged batch --
+def run_ragged(dev, nreq=96, seed=5_000_000, em_iters=30):
+    """96 requests, side log-uniform in [256, 2048], angles U[180, 1800], bins =
+    side; alternate FBP (Hann, padding 2) and 30-iteration eEM; device-resident,
+    one batch call.  Returns p50/p99 request latency and aggregate GUPS."""
+    import torch
+    from sscRaft import synthetic as S
+    from sscRaft.geometries.parallel.batch_methods import reconstruct_ragged
+    from sscRaft.rafttypes import libraft, check_error, _ptr
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sides = np.exp(rng.uniform(np.log(256), np.log(2048), nreq)).astype(int)
+    nangs = rng.integers(180, 1801, nreq)
+    reqs, updates = [], 0.0
+    for i in range(nreq):
+        N, A = int(sides[i]), int(nangs[i])
+        ang = S.uniform_angles(A)
+        prm = S.ellipse_params(seed + i, 20)
+        if i % 2 == 0:
+            sino = S.ellipse_sinogram(prm, ang, N, xp=torch, device=dev).float().contiguous()
+            reqs.append({"kind": "fbp", "data": sino, "out": torch.empty((N, N), dtype=torch.float32, device=dev),
+                         "angles": ang, "filter": "hann", "padding": 2})
+            updates += float(N) * N * A
+        else:
+            img = S.phantom_image(prm, N, xp=torch, device=dev).cpu().numpy()[None]
+            proj = -np.ones((1, A, N), np.float32)
+            g = np.array([dev.index or 0], np.intc)
+            libraft.getRadonRTMultiGPU(_ptr(g), 1, _ptr(proj), _ptr(np.ascontiguousarray(img)), _ptr(ang),
+                                       N, N, N, A, 1, 1.0, 1.0)
+            check_error("radon")
+            reqs.append({"kind": "eem", "data": torch.from_numpy(proj[0]).to(dev),
+                         "out": torch.ones((N, N), dtype=torch.float32, device=dev), "angles": ang,
+                         "iterations": em_iters})
+            updates += 2.0 * N * N * A * em_iters
+    reconstruct_ragged(reqs)            # warm-up (plans, tuning, graph capture paths)
+    for r in reqs:
+        if r["kind"] == "eem":
+            r["out"].fill_(1.0)
+    torch.cuda.synchronize()
+    lat, total = reconstruct_ragged(reqs)
+    fbp_lat = lat[0::2]
+    em_lat = lat[1::2]
+    return {"workload": f"{nreq} requests, side log-uniform [256,2048], angles U[180,1800], bins = side, "
+                        f"alternating FBP (Hann) and {em_iters}-iteration eEM, one ragged batch",
+            "total_ms": total, "gups": updates / (total / 1e3) / 1e9,
+            "latency_ms_p50": float(np.percentile(lat, 50)), "latency_ms_p99": float(np.percentile(lat, 99)),
+            "fbp_latency_ms_p50": float(np.percentile(fbp_lat, 50)),
+            "eem_latency_ms_p50": float(np.percentile(em_lat, 50)),
+            "updates": updates}
+
+
 # ---------------------------------------------------------------- clocks --
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -334,6 +384,11 @@ def run_ours(args):
         return ms[0], cnt[0], ms[1], cnt[1]
 
     hbm_peak, sm_max, peak_kind = peaks()
+    if args.quick and args.op == "ragged":
+        r = run_ragged(dev)
+        if rank == 0:
+            print(json.dumps({"quick": True, "op": "ragged", **r}), flush=True)
+        return
     if args.quick and args.op == "tem":
         # profiling mode: a short tEM run (args.slices x 1024^2, 900 angles)
         r = run_tem(local, dev, nslices=args.slices, iters=args.steps, warm_iters=args.warmup)
@@ -397,6 +452,7 @@ def run_ours(args):
                                                                    "frac": vg / pk}})
 
     em_result = None if args.no_em else run_tem(local, dev)
+    ragged_result = None if args.no_ragged else run_ragged(dev)
 
     if rank == 0:
         value = ws * nsl / (ms_dev / 1e3)
@@ -435,6 +491,7 @@ def run_ours(args):
             "variants": variants,
             "autotune": autotune_table(),
             "em": em_result,
+            "ragged": ragged_result,
             "clocks": clocks,
             "gpu_launches": int(launches),
         }
@@ -513,8 +570,9 @@ def main():
     ap.add_argument("--ref-slices", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-em", action="store_true")
+    ap.add_argument("--no-ragged", action="store_true")
     ap.add_argument("--quick", action="store_true", help="device timing of one operator only (profiling)")
-    ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "tem"])
+    ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "tem", "ragged"])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -105,6 +105,32 @@ int raft_fbp_device_noalloc(int gpu, float *d_obj, const float *d_tomogram, cons
                             const float *paramf, const int *parami, int geometry, int store,
                             void *stream);
 
+/* One request of a ragged batch (no reference counterpart; the reference handles one
+ * size per call).  All sizes may differ between requests. */
+typedef struct raft_request {
+    int kind;            /* 0 = FBP (getFBPMultiGPU operator), 1 = emission EM (get_eEM_RT_MultiGPU) */
+    int nrays;           /* detector bins = image side N */
+    int nangles;
+    int pad;             /* FBP: padding factor (reference dic 'padding') */
+    int filter;          /* FBP: filter id */
+    int niter;           /* eEM: iterations (equal for all eEM requests of a batch) */
+    float pixel;         /* FBP: detector pixel size */
+    float offset;        /* FBP: rotation-axis offset */
+    const float *angles; /* host, nangles radians */
+    const float *d_data; /* device: sinogram [nangles][nrays] (FBP) or emission tomogram (eEM) */
+    float *d_out;        /* device: FBP image [nrays][nrays]; eEM object, initial guess in / result out */
+} raft_request;
+
+/* Ragged batch on one GPU: FBP requests' backprojection runs as one persistent launch over
+ * all requests' tiles (shortest request first), eEM requests' iterations as one ragged
+ * projector + one persistent backprojector launch per iteration, replayed from a CUDA
+ * graph; FBP and EM proceed on two streams.  geometry/store select the FBP operator as in
+ * raft_fbp_ext.  latency_ms[i] (may be NULL) receives request i's completion time and
+ * *total_ms the whole batch's, both measured on the device from the batch start.
+ * Returns 0 on success. */
+int raft_ragged_device(int gpu, const raft_request *reqs, int nreq, int geometry, int store,
+                       double *latency_ms, double *total_ms, void *stream);
+
 /* EM (kind 0 = tEM as get_tEM_RT_MultiGPU, 1 = eEM as get_eEM_RT_MultiGPU) on one GPU with
  * host buffers, the iteration loop replayed as one CUDA graph when use_graph != 0, and
  * per-iteration FP64 metrics [niter][nslices][3] = {sum (model-data)^2, sum data^2,

@@ -36,6 +36,7 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <vector>
 
 namespace raft {
 
@@ -150,11 +151,13 @@ __device__ __forceinline__ float lerp_fetch(const unsigned char *w, int k, float
 // per pipeline stage) is a launch parameter; S and AB are chosen by the
 // autotuner below.
 // ------------------------------------------------------------------------
+// One 64 x 32 tile of S slices.  `gstage` counts the pipeline stages this
+// CTA has consumed so far (a persistent CTA runs many tiles through the same
+// two buffers and mbarriers); returns false if a staging wait timed out.
 template <int GEOM, int STORE, int S>
-__global__ void __launch_bounds__(BP_THREADS)
-bp_kernel(const BpArgs p, const int AB)
+__device__ __forceinline__ bool bp_tile(const BpArgs &p, const int AB, const int x0, const int y0,
+                                        const int slice0, unsigned char *smem, uint32_t &gstage)
 {
-    extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     AngleParam *prm = reinterpret_cast<AngleParam *>(smem + 128);
     unsigned char *win = smem + kWinOffset;
@@ -164,8 +167,6 @@ bp_kernel(const BpArgs p, const int AB)
     const int stage_bytes = AB * S * wbytes;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int x0 = blockIdx.x * BP_TX, y0 = blockIdx.y * BP_TY;
-    const int slice0 = blockIdx.z * S;
     const int nsl = min(S, p.nslices - slice0);  // valid slices of this CTA
     const int A = p.nangles;
     const int nst = (A + AB - 1) / AB;
@@ -178,13 +179,6 @@ bp_kernel(const BpArgs p, const int AB)
     for (int i = 0; i < 4; i++) li[i] = wx * 32 + lx + 8 * i;
 #pragma unroll
     for (int j = 0; j < 2; j++) lj[j] = wy * 8 + ly + 4 * j;
-
-    if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
 
     const unsigned char *rows = p.filt + (size_t)slice0 * A * p.Wg * esize;
     const size_t slice_stride = (size_t)A * p.Wg * esize;
@@ -214,7 +208,7 @@ bp_kernel(const BpArgs p, const int AB)
         }
     };
 
-    if (warp == 0) issue(0, 0);
+    if (warp == 0) issue(0, gstage & 1);
     __syncthreads();
 
     float acc[S][2][4];
@@ -246,13 +240,11 @@ bp_kernel(const BpArgs p, const int AB)
 
     bool ok = true;
     for (int s = 0; s < nst && ok; s++) {
-        const int b = s & 1;
+        const uint32_t g = gstage + s;
+        const int b = g & 1;
         if (s + 1 < nst && warp == 0) issue(s + 1, b ^ 1);
-        if (!mbar_wait_bounded(&bars[b], (uint32_t)((s >> 1) & 1), kWaitLimit)) {
-            ok = false;
-            if (p.err) atomicExch(p.err, 1);
-            break;
-        }
+        // bounded wait; the CTA agrees on the outcome at the end of the stage
+        const bool got = mbar_wait_bounded(&bars[b], (g >> 1) & 1, kWaitLimit);
         const int na = min(AB, A - s * AB);
         const unsigned char *wb = win + (size_t)b * stage_bytes;
         const AngleParam *pb = prm + b * 32;
@@ -294,9 +286,15 @@ bp_kernel(const BpArgs p, const int AB)
                     }
             }
         }
-        __syncthreads();
+        if (!__syncthreads_and(got)) {
+            ok = false;
+            if (tid == 0 && p.err) atomicExch(p.err, 1);
+            // give copies still in flight a last bounded chance to land
+            mbar_wait_bounded(&bars[b], (g >> 1) & 1, kWaitLimit);
+        }
     }
-    if (!ok) return;
+    gstage += nst;
+    if (!ok) return false;
 
 #pragma unroll
     for (int q = 0; q < S; q++) {
@@ -314,6 +312,79 @@ bp_kernel(const BpArgs p, const int AB)
                     else out[o] = acc[q][j][i];
                 }
             }
+    }
+    return true;
+}
+
+
+template <int GEOM, int STORE, int S>
+__global__ void __launch_bounds__(BP_THREADS)
+bp_kernel(const BpArgs p, const int AB)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t gstage = 0;
+    bp_tile<GEOM, STORE, S>(p, AB, blockIdx.x * BP_TX, blockIdx.y * BP_TY, blockIdx.z * S, smem, gstage);
+}
+
+// ------------------------------------------------------------------------
+// Ragged persistent backprojector: many requests (different image sizes,
+// angle counts, windows) in one launch.  Work items (request, tile, slice
+// group) are numbered request by request; each CTA takes the next item from
+// an atomic counter until none are left.  When a request's last item
+// finishes, its completion time (%globaltimer, ns) is recorded.
+// ------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+template <int GEOM, int STORE, int S>
+__global__ void __launch_bounds__(BP_THREADS)
+bp_ragged_kernel(const BpArgs *__restrict__ reqs, const int *__restrict__ item_start, int nreq, int total,
+                 const int AB, int *queue, int *remaining, unsigned long long *t_done)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    __shared__ int s_item, s_req;
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t gstage = 0;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int it = atomicAdd(queue, 1);
+            int r = 0;
+            if (it < total)
+                while (r + 1 < nreq && item_start[r + 1] <= it) r++;
+            s_item = it;
+            s_req = r;
+        }
+        __syncthreads();
+        const int it = s_item, r = s_req;
+        if (it >= total) break;
+        const BpArgs &p = reqs[r];
+        const int local = it - item_start[r];
+        const int tx = (p.No + BP_TX - 1) / BP_TX, ty = (p.No + BP_TY - 1) / BP_TY;
+        const int bx = local % tx, by = (local / tx) % ty, bz = local / (tx * ty);
+        const bool ok = bp_tile<GEOM, STORE, S>(p, AB, bx * BP_TX, by * BP_TY, bz * S, smem, gstage);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (atomicSub(&remaining[r], 1) == 1 && t_done) t_done[r] = global_ns();
+        }
+        if (!ok) break;   // uniform: bp_tile's outcome is agreed by the whole CTA
     }
 }
 
@@ -530,9 +601,8 @@ std::string bp_tune_table()
     return out + "]";
 }
 
-void launch_backproject(const BpLaunch &bl, cudaStream_t st)
+static BpArgs to_args(const BpLaunch &bl)
 {
-    if (bl.nslices <= 0 || bl.nangles <= 0) return;
     BpArgs a;
     a.filt = reinterpret_cast<const unsigned char *>(bl.filt);
     a.img = bl.img;
@@ -543,7 +613,7 @@ void launch_backproject(const BpLaunch &bl, cudaStream_t st)
     a.wlo = bl.win.wlo;
     a.Wg = bl.win.Wg;
     a.W = bl.win.W;
-    a.esize = store_bytes(bl.store);
+    a.esize = store_bytes(bl.geometry == GEOM_FBP_LIN ? bl.store : STORE_F32);
     a.xmin = bl.geo.xmin;
     a.ymin = bl.geo.ymin;
     a.dx = bl.geo.dx;
@@ -562,9 +632,122 @@ void launch_backproject(const BpLaunch &bl, cudaStream_t st)
     a.snd = bl.snd;
     a.err = bl.err;
     a.update = bl.den ? 1 : 0;
+    return a;
+}
+
+void launch_backproject(const BpLaunch &bl, cudaStream_t st)
+{
+    if (bl.nslices <= 0 || bl.nangles <= 0) return;
+    const BpArgs a = to_args(bl);
     const int store = bl.geometry == GEOM_FBP_LIN ? bl.store : STORE_F32;
     const BpTune t = choose_tune(a, bl.geometry, store, st);
     launch_bp_any(a, bl.geometry, store, t, st);
+}
+
+// ------------------------------------------------------------------------
+// ragged batches
+// ------------------------------------------------------------------------
+constexpr int kRaggedAB = 16;
+
+size_t ragged_bp_bytes(int nreq)
+{
+    return sizeof(BpArgs) * nreq + 256 + sizeof(int) * (3 * nreq + 8) + 256 + sizeof(unsigned long long) * nreq +
+           256;
+}
+
+static size_t al256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+void ragged_bp_prepare(RaggedBp &rb, const BpLaunch *reqs, int nreq, int geometry, int store, void *d_ws)
+{
+    rb.nreq = nreq;
+    rb.geometry = geometry;
+    rb.store = geometry == GEOM_FBP_LIN ? store : STORE_F32;
+    std::vector<BpArgs> args(nreq);
+    std::vector<int> start(nreq + 1), counts(nreq);
+    int total = 0, wmax = 0;
+    for (int r = 0; r < nreq; r++) {
+        args[r] = to_args(reqs[r]);
+        const int tx = (reqs[r].No + BP_TX - 1) / BP_TX, ty = (reqs[r].No + BP_TY - 1) / BP_TY;
+        counts[r] = tx * ty * reqs[r].nslices;    // one slice per CTA (S = 1)
+        start[r] = total;
+        total += counts[r];
+        wmax = std::max(wmax, reqs[r].win.W);
+    }
+    start[nreq] = total;
+    rb.total = total;
+    rb.wmax = wmax;
+    char *base = static_cast<char *>(d_ws);
+    size_t off = 0;
+    rb.d_args = base + off;              off = al256(off + sizeof(BpArgs) * nreq);
+    rb.d_item_start = (int *)(base + off); off = al256(off + sizeof(int) * (nreq + 1));
+    rb.d_counts = (int *)(base + off);   off = al256(off + sizeof(int) * nreq);
+    rb.d_remaining = (int *)(base + off); off = al256(off + sizeof(int) * nreq);
+    rb.d_queue = (int *)(base + off);    off = al256(off + sizeof(int) * 4);
+    rb.d_tdone = (unsigned long long *)(base + off);
+    RAFT_CUDA(cudaMemcpy(rb.d_args, args.data(), sizeof(BpArgs) * nreq, cudaMemcpyHostToDevice));
+    RAFT_CUDA(cudaMemcpy(rb.d_item_start, start.data(), sizeof(int) * (nreq + 1), cudaMemcpyHostToDevice));
+    RAFT_CUDA(cudaMemcpy(rb.d_counts, counts.data(), sizeof(int) * nreq, cudaMemcpyHostToDevice));
+    RAFT_CUDA(cudaMemset(rb.d_tdone, 0, sizeof(unsigned long long) * nreq));
+}
+
+__global__ void ragged_reset_kernel(int *queue, int *remaining, const int *counts, int nreq)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) *queue = 0;
+    for (int r = t; r < nreq; r += gridDim.x * blockDim.x) remaining[r] = counts[r];
+}
+
+template <int GEOM, int STORE>
+static void launch_ragged_t(const RaggedBp &rb, cudaStream_t st)
+{
+    const int esize = (STORE == STORE_PAIR_F32) ? 8 : 4;
+    const size_t smem = bp_smem(1, kRaggedAB, rb.wmax, esize);
+    RAFT_CHECK(smem <= kBpSmemMax, "ragged backprojector: window too large");
+    static thread_local int configured = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured != dev) {
+        RAFT_CUDA(cudaFuncSetAttribute(bp_ragged_kernel<GEOM, STORE, 1>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBpSmemMax));
+        configured = dev;
+    }
+    int per_sm = 0, nsm = 0;
+    RAFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_ragged_kernel<GEOM, STORE, 1>, BP_THREADS,
+                                                            smem));
+    RAFT_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int grid = std::max(1, std::min(rb.total, std::max(1, per_sm) * nsm));
+    count_launch();
+    ragged_reset_kernel<<<1, 256, 0, st>>>(rb.d_queue, rb.d_remaining, rb.d_counts, rb.nreq);
+    ProfScope ps(PROF_BACKPROJECT, st);
+    bp_ragged_kernel<GEOM, STORE, 1><<<grid, BP_THREADS, smem, st>>>(
+        reinterpret_cast<const BpArgs *>(rb.d_args), rb.d_item_start, rb.nreq, rb.total, kRaggedAB, rb.d_queue,
+        rb.d_remaining, rb.d_tdone);
+    RAFT_CUDA(cudaGetLastError());
+}
+
+void ragged_bp_launch(const RaggedBp &rb, cudaStream_t st)
+{
+    if (rb.nreq <= 0 || rb.total <= 0) return;
+    switch (rb.geometry) {
+    case GEOM_FBP_REF: launch_ragged_t<GEOM_FBP_REF, STORE_F32>(rb, st); break;
+    case GEOM_EM_REF: launch_ragged_t<GEOM_EM_REF, STORE_F32>(rb, st); break;
+    default:
+        if (rb.store == STORE_PAIR_BF16) launch_ragged_t<GEOM_FBP_LIN, STORE_PAIR_BF16>(rb, st);
+        else launch_ragged_t<GEOM_FBP_LIN, STORE_PAIR_F32>(rb, st);
+        break;
+    }
+}
+
+__global__ void stamp_kernel(unsigned long long *t)
+{
+    if (threadIdx.x == 0) *t = global_ns();
+}
+
+void launch_stamp(unsigned long long *d_t, cudaStream_t st)
+{
+    count_launch();
+    stamp_kernel<<<1, 32, 0, st>>>(d_t);
+    RAFT_CUDA(cudaGetLastError());
 }
 
 }  // namespace raft

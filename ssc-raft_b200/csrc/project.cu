@@ -38,12 +38,11 @@ __device__ __forceinline__ double warp_sum(double v)
 // 32 rays of the warp touch consecutive addresses; the index arithmetic and
 // therefore the chosen pixels are unchanged.
 template <int EM, int EPI, int S>
-__global__ void __launch_bounds__(PJ_RAYS * PJ_ANGLES)
-project_kernel(const ProjLaunch p)
+__device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx, const int by, const int bz)
 {
-    const int i = blockIdx.x * PJ_RAYS + threadIdx.x;     // ray
-    const int j = blockIdx.y * PJ_ANGLES + threadIdx.y;   // angle
-    const int k0 = blockIdx.z * S;                        // first slice
+    const int i = bx * PJ_RAYS + threadIdx.x;     // ray
+    const int j = by * PJ_ANGLES + threadIdx.y;   // angle
+    const int k0 = bz * S;                        // first slice
     const int nsl = min(S, p.nslices - k0);
     const bool valid = (i < p.nrays) && (j < p.nangles);
     const int nx = p.nx, ny = p.ny;
@@ -185,6 +184,50 @@ project_kernel(const ProjLaunch p)
             }
         }
     }
+}
+
+template <int EM, int EPI, int S>
+__global__ void __launch_bounds__(PJ_RAYS * PJ_ANGLES)
+project_kernel(const ProjLaunch p)
+{
+    project_block<EM, EPI, S>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Ragged projector: one launch over many single-slice requests of different
+// sizes; block b belongs to the request r with blk_start[r] <= b < blk_start[r+1].
+template <int EM, int EPI>
+__global__ void __launch_bounds__(PJ_RAYS * PJ_ANGLES)
+project_ragged_kernel(const ProjLaunch *__restrict__ reqs, const int *__restrict__ blk_start, int nreq)
+{
+    __shared__ int s_r;
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        int lo = 0, hi = nreq - 1;
+        while (lo < hi) {                       // last r with blk_start[r] <= blockIdx.x
+            const int mid = (lo + hi + 1) / 2;
+            if (blk_start[mid] <= (int)blockIdx.x) lo = mid;
+            else hi = mid - 1;
+        }
+        s_r = lo;
+    }
+    __syncthreads();
+    const int r = s_r;
+    const ProjLaunch &p = reqs[r];
+    const int local = blockIdx.x - blk_start[r];
+    const int nbx = (p.nrays + PJ_RAYS - 1) / PJ_RAYS;
+    project_block<EM, EPI, 1>(p, local % nbx, local / nbx, 0);
+}
+
+void launch_project_ragged(const ProjLaunch *d_reqs, const int *d_blk_start, int nreq, int total_blocks, int em,
+                           int epilogue, cudaStream_t st)
+{
+    if (nreq <= 0 || total_blocks <= 0) return;
+    ProfScope ps(PROF_PROJECT, st);
+    dim3 block(PJ_RAYS, PJ_ANGLES);
+    if (!em) project_ragged_kernel<0, 0><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
+    else if (epilogue == 1) project_ragged_kernel<1, 1><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
+    else if (epilogue == 2) project_ragged_kernel<1, 2><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
+    else project_ragged_kernel<1, 0><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
+    RAFT_CUDA(cudaGetLastError());
 }
 
 // Tiled transpose of each slice: out[k][x][y] = in[k][y][x].

@@ -160,6 +160,20 @@ struct BpTune {
 };
 std::string bp_tune_table();   // JSON list of the tuned configurations
 
+// Ragged batch of backprojections (different sizes, angle counts, windows) in
+// one persistent launch; descriptors live on the device so the launch can be
+// replayed inside a CUDA graph.
+struct RaggedBp {
+    int nreq = 0, total = 0, wmax = 0, geometry = 0, store = 0;
+    void *d_args = nullptr;
+    int *d_item_start = nullptr, *d_counts = nullptr, *d_remaining = nullptr, *d_queue = nullptr;
+    unsigned long long *d_tdone = nullptr;   // per-request completion time (ns, %globaltimer)
+};
+size_t ragged_bp_bytes(int nreq);
+void ragged_bp_prepare(RaggedBp &rb, const BpLaunch *reqs, int nreq, int geometry, int store, void *d_ws);
+void ragged_bp_launch(const RaggedBp &rb, cudaStream_t st);
+void launch_stamp(unsigned long long *d_t, cudaStream_t st);   // write %globaltimer
+
 // sin/cos with the reference's fast intrinsics (__sinf/__cosf for FBP,
 // opt.cu:187-194; __sincosf for EM, em_RT_kernel.cu:120) and the per-angle
 // weight dtheta_a (times pi/theta_last beyond pi for FBP).
@@ -184,6 +198,11 @@ struct ProjLaunch {
 };
 
 void launch_project(const ProjLaunch &pl, cudaStream_t st);
+
+// Ragged projector over single-slice requests: block b runs request r with
+// blk_start[r] <= b < blk_start[r+1] (device arrays).
+void launch_project_ragged(const ProjLaunch *d_reqs, const int *d_blk_start, int nreq, int total_blocks, int em,
+                           int epilogue, cudaStream_t st);
 
 // out[k][x][y] = in[k][y][x] for each of nslices planes.
 void launch_transpose(const float *in, float *out, int nx, int ny, int nslices, cudaStream_t st);

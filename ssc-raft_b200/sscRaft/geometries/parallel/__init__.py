@@ -1,3 +1,4 @@
 from .fbp_methods import *
 from .radon_methods import *
 from .em_methods import *
+from .batch_methods import *
