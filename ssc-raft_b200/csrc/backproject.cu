@@ -649,13 +649,29 @@ void launch_backproject(const BpLaunch &bl, cudaStream_t st)
 // ------------------------------------------------------------------------
 constexpr int kRaggedAB = 16;
 
-size_t ragged_bp_bytes(int nreq)
+static size_t al256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// Byte offsets of the regions of a ragged descriptor workspace; the same
+// function sizes the workspace and lays it out.
+struct RaggedLayout {
+    size_t args, item_start, counts, remaining, queue, tdone, total;
+};
+
+static RaggedLayout ragged_layout(int nreq)
 {
-    return sizeof(BpArgs) * nreq + 256 + sizeof(int) * (3 * nreq + 8) + 256 + sizeof(unsigned long long) * nreq +
-           256;
+    RaggedLayout L;
+    size_t off = 0;
+    L.args = off;       off = al256(off + sizeof(BpArgs) * nreq);
+    L.item_start = off; off = al256(off + sizeof(int) * (nreq + 1));
+    L.counts = off;     off = al256(off + sizeof(int) * nreq);
+    L.remaining = off;  off = al256(off + sizeof(int) * nreq);
+    L.queue = off;      off = al256(off + sizeof(int) * 4);
+    L.tdone = off;      off = al256(off + sizeof(unsigned long long) * nreq);
+    L.total = off;
+    return L;
 }
 
-static size_t al256(size_t v) { return (v + 255) & ~(size_t)255; }
+size_t ragged_bp_bytes(int nreq) { return ragged_layout(nreq).total; }
 
 void ragged_bp_prepare(RaggedBp &rb, const BpLaunch *reqs, int nreq, int geometry, int store, void *d_ws)
 {
@@ -677,13 +693,13 @@ void ragged_bp_prepare(RaggedBp &rb, const BpLaunch *reqs, int nreq, int geometr
     rb.total = total;
     rb.wmax = wmax;
     char *base = static_cast<char *>(d_ws);
-    size_t off = 0;
-    rb.d_args = base + off;              off = al256(off + sizeof(BpArgs) * nreq);
-    rb.d_item_start = (int *)(base + off); off = al256(off + sizeof(int) * (nreq + 1));
-    rb.d_counts = (int *)(base + off);   off = al256(off + sizeof(int) * nreq);
-    rb.d_remaining = (int *)(base + off); off = al256(off + sizeof(int) * nreq);
-    rb.d_queue = (int *)(base + off);    off = al256(off + sizeof(int) * 4);
-    rb.d_tdone = (unsigned long long *)(base + off);
+    const RaggedLayout L = ragged_layout(nreq);
+    rb.d_args = base + L.args;
+    rb.d_item_start = (int *)(base + L.item_start);
+    rb.d_counts = (int *)(base + L.counts);
+    rb.d_remaining = (int *)(base + L.remaining);
+    rb.d_queue = (int *)(base + L.queue);
+    rb.d_tdone = (unsigned long long *)(base + L.tdone);
     RAFT_CUDA(cudaMemcpy(rb.d_args, args.data(), sizeof(BpArgs) * nreq, cudaMemcpyHostToDevice));
     RAFT_CUDA(cudaMemcpy(rb.d_item_start, start.data(), sizeof(int) * (nreq + 1), cudaMemcpyHostToDevice));
     RAFT_CUDA(cudaMemcpy(rb.d_counts, counts.data(), sizeof(int) * nreq, cudaMemcpyHostToDevice));
