@@ -72,6 +72,10 @@ void DeviceState::ensure()
     RAFT_CUDA(cudaStreamCreateWithFlags(&s_comp, cudaStreamNonBlocking));
     RAFT_CUDA(cudaStreamCreateWithFlags(&s_h2d, cudaStreamNonBlocking));
     RAFT_CUDA(cudaStreamCreateWithFlags(&s_d2h, cudaStreamNonBlocking));
+    int lo = 0, hi = 0;
+    RAFT_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    RAFT_CUDA(cudaStreamCreateWithPriority(&s_hi, cudaStreamNonBlocking, hi));
+    RAFT_CUDA(cudaStreamCreateWithPriority(&s_lo, cudaStreamNonBlocking, lo));
     for (int b = 0; b < 2; b++) {
         RAFT_CUDA(cudaEventCreateWithFlags(&ev_h2d[b], cudaEventDisableTiming));
         RAFT_CUDA(cudaEventCreateWithFlags(&ev_comp[b], cudaEventDisableTiming));

@@ -30,6 +30,7 @@ struct DeviceState {
     int device = 0;
     std::mutex mtx;
     cudaStream_t s_comp = nullptr, s_h2d = nullptr, s_d2h = nullptr;
+    cudaStream_t s_hi = nullptr, s_lo = nullptr;   // ragged batches: FBP (high) and EM (low) priority
     DevBuf sino[2], img[2], rows, den, flat, data, angles, tabs, metrics, err, imgT;
     PinBuf pin_in[2], pin_out[2];
     cudaEvent_t ev_h2d[2] = {}, ev_comp[2] = {}, ev_d2h[2] = {};

@@ -11,7 +11,8 @@
 //     whole iteration loop -- one ragged projector launch and one persistent
 //     backprojector-with-update launch per iteration over all EM requests --
 //     captured once as a CUDA graph and replayed;
-//   * the FBP and EM halves run concurrently on two streams;
+//   * the FBP and EM halves run concurrently on two streams, FBP at high
+//     priority so short FBP requests are not queued behind EM iterations;
 //   * each request's completion time is stamped on the device (%globaltimer)
 //     by the CTA that finishes its last work item, giving per-request latency.
 #include "engine.hpp"
@@ -36,7 +37,7 @@ struct FbpReq {
 struct EmReq {
     int idx;
     EmPrepared ep;
-    size_t tab, rows, den;
+    size_t tab, rows, den, imgT;
     double cost;
 };
 
@@ -86,8 +87,9 @@ extern "C" int raft_ragged_device(int gpu, const raft_request *reqs, int nreq, i
         std::lock_guard<std::mutex> lk(ds.mtx);
         RAFT_CUDA(cudaSetDevice(gpu));
         ds.ensure();
-        cudaStream_t s0 = stream ? (cudaStream_t)stream : ds.s_comp;
-        cudaStream_t s1 = ds.s_d2h;
+        // s0: caller's stream (or the high-priority one) for FBP; s1: low-priority EM
+        cudaStream_t s0 = stream ? (cudaStream_t)stream : ds.s_hi;
+        cudaStream_t s1 = ds.s_lo;
 
         // ---- plan every request and lay out one workspace ----------------
         std::vector<FbpReq> F;
@@ -227,6 +229,7 @@ extern "C" int raft_ragged_device(int gpu, const raft_request *reqs, int nreq, i
             bU[k].den = (const float *)(ws + E[k].den);
             ProjLaunch &p = P[k];
             p.img = q.d_out;
+            p.imgT = (const float *)(ws + E[k].imgT);   // transposed copy for steep angles
             p.out = rows;
             p.angles = d_ang;
             p.nx = p.ny = p.nrays = N;
@@ -256,6 +259,8 @@ extern "C" int raft_ragged_device(int gpu, const raft_request *reqs, int nreq, i
             RAFT_CUDA(cudaStreamBeginCapture(s1, cudaStreamCaptureModeThreadLocal));
             try {
                 for (int it = 0; it < em_iters; it++) {
+                    for (size_t k = 0; k < E.size(); k++)
+                        launch_transpose(reqs[E[k].idx].d_out, (float *)P[k].imgT, P[k].nx, P[k].nx, 1, s1);
                     launch_project_ragged((const ProjLaunch *)(ws + o_proj), (const int *)(ws + o_blk),
                                           (int)E.size(), blk.back(), 1, 2, s1);
                     ragged_bp_launch(rbU, s1);
