@@ -140,6 +140,11 @@ int raft_em_ext(int kind, int gpu, float *obj, const float *data, const float *f
                 const float *angles, int nrays, int nangles, int nslices, int niter,
                 double *metrics, int use_graph);
 
+/* getRadonRTMultiGPU's operator on device-resident buffers of one GPU (angles host),
+ * issued on `stream` (NULL: library stream, synchronised).  Returns 0 on success. */
+int raft_radon_device(int gpu, float *d_out, const float *d_phantom, const float *angles, int nx, int ny,
+                      int nrays, int nangles, int nslices, float ax, float ay, void *stream);
+
 /* As raft_em_ext on device-resident buffers (metrics device pointer or NULL). */
 int raft_em_device(int kind, int gpu, float *d_obj, const float *d_data, const float *d_flat,
                    const float *angles, int nrays, int nangles, int nslices, int niter,
@@ -169,6 +174,28 @@ long long raft_launch_count(void);
 int raft_autotune_table(char *buf, int len);
 void raft_profile_enable(int on);
 int raft_profile_read(double *ms, long long *counts, int nclasses);
+
+/* Learned warm start: tensor-core kernels of the U-Net (no reference counterpart).
+ * Device pointers; BF16 NHWC activations (channel counts multiples of 32), BF16 weights
+ * [Cout][3][3][Cin], FP32 biases / gradients / master weights.  Return 0 on success. */
+int raft_unet_conv_fwd(const void *x0, int C0, const void *x1, int C1, const void *w, const float *bias,
+                       void *y, void *y1, int Cy0, int N, int H, int W, int Cout, int relu, void *stream);
+int raft_unet_conv_wgrad(const void *dy, const void *x0, int C0, const void *x1, int C1, float *dw,
+                         float *dbias, int N, int H, int W, int Cout, void *stream);
+int raft_unet_flip_weights(const void *w, void *wt, int Cout, int Cin, void *stream);
+int raft_unet_relu_bwd(const void *y, const void *dy, void *dpre, size_t n, void *stream);
+int raft_unet_pool(int backward, const void *src, void *dst, int N, int H, int W, int C, void *stream);
+int raft_unet_upsample(int backward, const void *src, void *dst, int N, int H, int W, int C, void *stream);
+int raft_unet_input(const float *img, const float *scale, void *x, int N, int H, int W, int C, void *stream);
+int raft_unet_head(int backward, const void *h, const float *w, const float *b, const float *img,
+                   const float *scale, float *out_or_grad, void *dh, float *dw, float *db, int N, int HW,
+                   int C, void *stream);
+int raft_unet_mse(const float *out, const float *target, const float *scale, float *grad, double *loss,
+                  int N, int HW, void *stream);
+int raft_unet_adam(float *w, float *m, float *v, const float *g, void *wb, size_t n, float lr, float b1,
+                   float b2, float eps, int step, void *stream);
+int raft_unet_add(void *y, const void *x, size_t n, void *stream);
+int raft_unet_to_bf16(const float *a, void *b, size_t n, void *stream);
 
 #ifdef __cplusplus
 }

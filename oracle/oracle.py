@@ -57,6 +57,9 @@ def lib():
         _lib.oracle_tem.argtypes = [I, I, I, I, I, P, P, P, P, P, P, P, P]
         _lib.oracle_eem.argtypes = [I, I, I, I, I, P, P, P, P, P, P, P]
         _lib.oracle_tem_metrics.argtypes = [I, I, I, I, P, P, P, P, P, P, P, P]
+        _lib.oracle_conv3x3_fwd.argtypes = [P, P, P, P, I, I, I, I, I, I]
+        _lib.oracle_conv3x3_wgrad.argtypes = [P, P, P, I, I, I, I, I]
+        _lib.oracle_conv3x3_dgrad.argtypes = [P, P, P, I, I, I, I, I]
     return _lib
 
 
@@ -217,3 +220,33 @@ def tem_metrics(counts_exp, flat, angles, obj, fwd_trig=None):
     lib().oracle_tem_metrics(N, nrays, A, B, _p(_f32(angles)), _p(c), _p(fl), _p(o), _p(res), _p(nll),
                              fc, fs)
     return res, nll
+
+
+# ----------------------------------------------------------- U-Net convs --
+def conv3x3(x, w, b=None, relu=False):
+    """x [N,H,W,Cin], w [Cout,3,3,Cin] -> y [N,H,W,Cout], FP64."""
+    x, w = _f64(x), _f64(w)
+    N, H, W, Cin = x.shape
+    Cout = w.shape[0]
+    y = np.zeros((N, H, W, Cout))
+    bb = None if b is None else _f64(b)
+    lib().oracle_conv3x3_fwd(_p(x), _p(w), None if bb is None else _p(bb), _p(y), N, H, W, Cin, Cout, int(relu))
+    return y
+
+
+def conv3x3_wgrad(dy, x):
+    dy, x = _f64(dy), _f64(x)
+    N, H, W, Cout = dy.shape
+    Cin = x.shape[-1]
+    dw = np.zeros((Cout, 3, 3, Cin))
+    lib().oracle_conv3x3_wgrad(_p(dy), _p(x), _p(dw), N, H, W, Cin, Cout)
+    return dw
+
+
+def conv3x3_dgrad(dy, w):
+    dy, w = _f64(dy), _f64(w)
+    N, H, W, Cout = dy.shape
+    Cin = w.shape[-1]
+    dx = np.zeros((N, H, W, Cin))
+    lib().oracle_conv3x3_dgrad(_p(dy), _p(w), _p(dx), N, H, W, Cin, Cout)
+    return dx

@@ -506,3 +506,72 @@ void oracle_tem_metrics(int N, int nrays, int A, int nslices, const float *angle
     }
     free(p);
 }
+
+/* ------------------------------------------------------------------------ */
+/* 3x3 convolution, stride 1, zero padding 1, NHWC (the warm-start U-Net's   */
+/* layer; no reference counterpart).  FP64.                                  */
+/* x [N][H][W][Cin], w [Cout][3][3][Cin], y [N][H][W][Cout]                  */
+/* ------------------------------------------------------------------------ */
+void oracle_conv3x3_fwd(const double *x, const double *w, const double *b, double *y, int N, int H, int W,
+                        int Cin, int Cout, int relu)
+{
+#pragma omp parallel for collapse(2)
+    for (int n = 0; n < N; n++)
+        for (int yy = 0; yy < H; yy++)
+            for (int xx = 0; xx < W; xx++)
+                for (int co = 0; co < Cout; co++) {
+                    double s = b ? b[co] : 0.0;
+                    for (int ky = -1; ky <= 1; ky++)
+                        for (int kx = -1; kx <= 1; kx++) {
+                            int sy = yy + ky, sx = xx + kx;
+                            if (sy < 0 || sy >= H || sx < 0 || sx >= W) continue;
+                            const double *xp = x + (((size_t)n * H + sy) * W + sx) * Cin;
+                            const double *wp = w + ((size_t)co * 9 + (ky + 1) * 3 + (kx + 1)) * Cin;
+                            for (int ci = 0; ci < Cin; ci++) s += xp[ci] * wp[ci];
+                        }
+                    if (relu && s < 0) s = 0;
+                    y[(((size_t)n * H + yy) * W + xx) * Cout + co] = s;
+                }
+}
+
+/* dw[co][tap][ci] = sum_p dy[p][co] x[p+tap][ci] */
+void oracle_conv3x3_wgrad(const double *dy, const double *x, double *dw, int N, int H, int W, int Cin, int Cout)
+{
+#pragma omp parallel for collapse(2)
+    for (int co = 0; co < Cout; co++)
+        for (int tap = 0; tap < 9; tap++) {
+            int ky = tap / 3 - 1, kx = tap % 3 - 1;
+            for (int ci = 0; ci < Cin; ci++) {
+                double s = 0;
+                for (int n = 0; n < N; n++)
+                    for (int yy = 0; yy < H; yy++)
+                        for (int xx = 0; xx < W; xx++) {
+                            int sy = yy + ky, sx = xx + kx;
+                            if (sy < 0 || sy >= H || sx < 0 || sx >= W) continue;
+                            s += dy[(((size_t)n * H + yy) * W + xx) * Cout + co] *
+                                 x[(((size_t)n * H + sy) * W + sx) * Cin + ci];
+                        }
+                dw[((size_t)co * 9 + tap) * Cin + ci] = s;
+            }
+        }
+}
+
+/* dx[p][ci] = sum_{co,tap} dy[p - tap][co] w[co][tap][ci] */
+void oracle_conv3x3_dgrad(const double *dy, const double *w, double *dx, int N, int H, int W, int Cin, int Cout)
+{
+#pragma omp parallel for collapse(2)
+    for (int n = 0; n < N; n++)
+        for (int yy = 0; yy < H; yy++)
+            for (int xx = 0; xx < W; xx++)
+                for (int ci = 0; ci < Cin; ci++) {
+                    double s = 0;
+                    for (int tap = 0; tap < 9; tap++) {
+                        int ky = tap / 3 - 1, kx = tap % 3 - 1;
+                        int oy = yy - ky, ox = xx - kx;
+                        if (oy < 0 || oy >= H || ox < 0 || ox >= W) continue;
+                        const double *dp = dy + (((size_t)n * H + oy) * W + ox) * Cout;
+                        for (int co = 0; co < Cout; co++) s += dp[co] * w[((size_t)co * 9 + tap) * Cin + ci];
+                    }
+                    dx[(((size_t)n * H + yy) * W + xx) * Cin + ci] = s;
+                }
+}

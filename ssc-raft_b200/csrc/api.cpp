@@ -503,6 +503,46 @@ int raft_fast_sincos(int gpu, const float *angles, int n, int kind, float *cos_o
     return has_error() ? 1 : 0;
 }
 
+// Radon RT on device-resident buffers of one GPU (d_phantom [nslices][ny][nx],
+// d_out [nslices][nangles][nrays], angles host); no Python-side scaling.
+int raft_radon_device(int gpu, float *d_out, const float *d_phantom, const float *angles, int nx, int ny, int nrays,
+                      int nangles, int nslices, float ax, float ay, void *stream)
+{
+    clear_error();
+    if (nx < 2 || ny < 2 || nrays < 1 || nangles < 1 || nslices < 0) {
+        set_error("invalid Radon sizes");
+        return 1;
+    }
+    if (!check_gpus(&gpu, 1)) return 1;
+    try {
+        DeviceState &ds = device_state(gpu);
+        std::lock_guard<std::mutex> lk(ds.mtx);
+        RAFT_CUDA(cudaSetDevice(gpu));
+        ds.ensure();
+        cudaStream_t st = stream ? (cudaStream_t)stream : ds.s_comp;
+        float *d_ang = (float *)ds.angles.get(sizeof(float) * nangles);
+        RAFT_CUDA(cudaMemcpyAsync(d_ang, angles, sizeof(float) * nangles, cudaMemcpyHostToDevice, st));
+        float *imgT = (float *)ds.imgT.get(sizeof(float) * (size_t)nx * ny * std::max(1, nslices));
+        launch_transpose(d_phantom, imgT, nx, ny, nslices, st);
+        ProjLaunch pl;
+        pl.img = d_phantom;
+        pl.imgT = imgT;
+        pl.out = d_out;
+        pl.angles = d_ang;
+        pl.nx = nx;
+        pl.ny = ny;
+        pl.nrays = nrays;
+        pl.nangles = nangles;
+        pl.nslices = nslices;
+        pl.ax = ax;
+        pl.ay = ay;
+        launch_project(pl, st);
+        if (!stream) RAFT_CUDA(cudaStreamSynchronize(st));
+    } catch (const CudaFail &) {
+    }
+    return has_error() ? 1 : 0;
+}
+
 // Adjacent reference exports that this library does not implement: they
 // record an error instead of running (rafttypes.py binds them if present).
 void getBSTMultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *angles, float *paramf, int *parami,

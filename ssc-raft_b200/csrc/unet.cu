@@ -1,0 +1,585 @@
+// unet.cu -- tensor-core kernels of the learned warm start for EM.
+//
+// A small U-Net maps an FBP image to an estimate that tEM starts from
+// (no reference counterpart: the reference only exposes the initial guess,
+// em_methods.py:117-122 / em_rt.cu:135).  Activations are BF16 NHWC with
+// channel counts that are multiples of 32; weights are BF16 [Cout][3][3][Cin]
+// with FP32 master copies; every accumulation is FP32.
+//
+// Kernels (all implicit GEMM on mma.sync.m16n8k16 BF16 -> FP32):
+//   conv3x3_fwd    y = act(conv(x) + b); x may be the channel concatenation
+//                  of two tensors (the decoder's skip connection), read
+//                  in place -- no concatenated copy is materialised
+//   conv3x3_dgrad  the data gradient is conv3x3_fwd of dY with the weights
+//                  flipped in space and transposed in channels
+//   conv3x3_wgrad  dW[co][tap][ci] = sum over pixels of dY[p][co] * x[p+tap][ci],
+//                  pixels split across CTAs, FP32 atomic accumulation
+// plus the memory-bound pieces: ReLU mask, 2x2 average pooling, nearest 2x
+// upsampling, the 1x1 output head with the residual connection, MSE loss
+// gradient and Adam.
+#include "raft.hpp"
+#include "profile.hpp"
+
+#include <cuda_bf16.h>
+
+namespace raft {
+
+typedef __nv_bfloat16 bf16;
+
+// ------------------------------------------------------------ mma helpers
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void ldmatrix_x4(uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3, const void *p)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(smem_addr(p)));
+}
+
+__device__ __forceinline__ void ldmatrix_x4_trans(uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3,
+                                                  const void *p)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(smem_addr(p)));
+}
+
+// D = A(16x16, row) * B(16x8, col) + D, BF16 inputs, FP32 accumulate
+__device__ __forceinline__ void mma_bf16(float *d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// ------------------------------------------------------------ conv forward
+// CTA: 128 threads = 4 warps; tile = 64 consecutive pixels of one image row
+// (n, y, x0..x0+63) x 32 output channels.  Warp w owns pixels 16w..16w+15
+// and all 32 channels (4 n8 tiles).  K = 9 taps x Cin in chunks of 32
+// channels, staged through shared memory (rows padded to 40 halves so the
+// ldmatrix row addresses fall in distinct banks).
+constexpr int CV_PIX = 64, CV_CO = 32, CV_KC = 32, CV_LD = 40;
+
+struct ConvArgs {
+    const bf16 *x0, *x1;   // inputs [N][H][W][C0] and [N][H][W][C1] (x1 may be null, C1 = 0)
+    int C0, C1;
+    const bf16 *w;         // [Cout][3][3][C0+C1]
+    const float *bias;     // [Cout] or null
+    bf16 *y;               // [N][H][W][Cout], or channels [0, Cy0) when y1 is set
+    bf16 *y1;              // optional second output: channels [Cy0, Cout) as [N][H][W][Cout-Cy0]
+    int Cy0;
+    int N, H, W, Cout;
+    int relu;
+};
+
+__global__ void __launch_bounds__(128) conv3x3_fwd_kernel(const ConvArgs a)
+{
+    __shared__ __align__(128) bf16 As[CV_PIX * CV_LD];
+    __shared__ __align__(128) bf16 Bs[CV_CO * CV_LD];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tiles_x = (a.W + CV_PIX - 1) / CV_PIX;
+    const int row = blockIdx.x / tiles_x;                // n*H + y
+    const int x0 = (blockIdx.x % tiles_x) * CV_PIX;
+    const int n = row / a.H, y = row % a.H;
+    const int co0 = blockIdx.y * CV_CO;
+    const int Cin = a.C0 + a.C1;
+    float acc[4][4];
+#pragma unroll
+    for (int t = 0; t < 4; t++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) acc[t][e] = 0.f;
+
+    for (int tap = 0; tap < 9; tap++) {
+        const int ky = tap / 3 - 1, kx = tap % 3 - 1;
+        const int yy = y + ky;
+        for (int c0 = 0; c0 < Cin; c0 += CV_KC) {
+            // A: 64 pixels x 32 channels (4 x 16-byte chunks per pixel)
+            const bf16 *src;
+            int cs, C;
+            if (c0 < a.C0) { src = a.x0; cs = c0; C = a.C0; }
+            else { src = a.x1; cs = c0 - a.C0; C = a.C1; }
+            for (int e = tid; e < CV_PIX * 4; e += 128) {
+                const int p = e >> 2, q = e & 3;
+                const int xx = x0 + p + kx;
+                uint4 v = make_uint4(0, 0, 0, 0);
+                if (yy >= 0 && yy < a.H && xx >= 0 && xx < a.W && x0 + p < a.W)
+                    v = *reinterpret_cast<const uint4 *>(src + (((size_t)n * a.H + yy) * a.W + xx) * C + cs + q * 8);
+                *reinterpret_cast<uint4 *>(&As[p * CV_LD + q * 8]) = v;
+            }
+            // B: 32 output channels x 32 input channels of this tap
+            for (int e = tid; e < CV_CO * 4; e += 128) {
+                const int o = e >> 2, q = e & 3;
+                uint4 v = make_uint4(0, 0, 0, 0);
+                if (co0 + o < a.Cout)
+                    v = *reinterpret_cast<const uint4 *>(a.w + ((size_t)(co0 + o) * 9 + tap) * Cin + c0 + q * 8);
+                *reinterpret_cast<uint4 *>(&Bs[o * CV_LD + q * 8]) = v;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < CV_KC; kk += 16) {
+                uint32_t a0, a1, a2, a3;
+                {
+                    const int mi = lane >> 3, r = lane & 7;
+                    const bf16 *pa = &As[(warp * 16 + (mi & 1) * 8 + r) * CV_LD + kk + (mi >> 1) * 8];
+                    ldmatrix_x4(a0, a1, a2, a3, pa);
+                }
+#pragma unroll
+                for (int nt = 0; nt < 4; nt += 2) {
+                    uint32_t b0, b1, b2, b3;
+                    const int mi = lane >> 3, r = lane & 7;
+                    // matrices: (n 0-7,k lo) (n 0-7,k hi) (n 8-15,k lo) (n 8-15,k hi)
+                    const bf16 *pb = &Bs[(nt * 8 + (mi >> 1) * 8 + r) * CV_LD + kk + (mi & 1) * 8];
+                    ldmatrix_x4(b0, b1, b2, b3, pb);
+                    mma_bf16(acc[nt], a0, a1, a2, a3, b0, b1);
+                    mma_bf16(acc[nt + 1], a0, a1, a2, a3, b2, b3);
+                }
+            }
+            __syncthreads();
+        }
+    }
+    // epilogue: bias, ReLU, BF16 store
+    const int g = lane >> 2, tg = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int p = warp * 16 + g + h * 8;
+            const int co = co0 + nt * 8 + tg * 2;
+            if (x0 + p >= a.W || co >= a.Cout) continue;
+            float v0 = acc[nt][h * 2], v1 = acc[nt][h * 2 + 1];
+            if (a.bias) {
+                v0 += a.bias[co];
+                v1 += a.bias[co + 1];
+            }
+            if (a.relu) {
+                v0 = fmaxf(v0, 0.f);
+                v1 = fmaxf(v1, 0.f);
+            }
+            const size_t pix = ((size_t)n * a.H + y) * a.W + x0 + p;
+            bf16 *dst;
+            if (a.y1 && co >= a.Cy0) dst = a.y1 + pix * (a.Cout - a.Cy0) + (co - a.Cy0);
+            else if (a.y1) dst = a.y + pix * a.Cy0 + co;
+            else dst = a.y + pix * a.Cout + co;
+            *reinterpret_cast<__nv_bfloat162 *>(dst) = __floats2bfloat162_rn(v0, v1);
+        }
+    }
+}
+
+// ------------------------------------------------------------ weight grad
+// CTA tile: 32 output channels x 32 input channels of one tap; K = a slice of
+// NP pixels; the partial sums are added atomically into dW (FP32).
+// A = dY^T (co x pixels) and B = x_tap (pixels x ci) are both stored
+// pixel-major in shared memory and read with transposing ldmatrix.
+constexpr int WG_CO = 32, WG_CI = 32, WG_KP = 32, WG_LD = 40;
+
+struct WgradArgs {
+    const bf16 *dy;        // [N][H][W][Cout]
+    const bf16 *x0, *x1;   // inputs as in ConvArgs
+    int C0, C1;
+    float *dw;             // [Cout][3][3][C0+C1], accumulated
+    float *dbias;          // [Cout], accumulated (taps 0 CTAs only) or null
+    int N, H, W, Cout;
+    int pix_per_cta;
+};
+
+__global__ void __launch_bounds__(128) conv3x3_wgrad_kernel(const WgradArgs a)
+{
+    __shared__ __align__(128) bf16 Ds[WG_KP * WG_LD];   // [pixel][co]
+    __shared__ __align__(128) bf16 Xs[WG_KP * WG_LD];   // [pixel][ci]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Cin = a.C0 + a.C1;
+    const int nci = Cin / WG_CI, nco = (a.Cout + WG_CO - 1) / WG_CO;
+    int b = blockIdx.x;
+    const int cib = b % nci; b /= nci;
+    const int cob = b % nco; b /= nco;
+    const int tap = b % 9;
+    const int pchunk = blockIdx.y;
+    const int ky = tap / 3 - 1, kx = tap % 3 - 1;
+    const int co0 = cob * WG_CO, ci0 = cib * WG_CI;
+    const bf16 *src;
+    int cs, C;
+    if (ci0 < a.C0) { src = a.x0; cs = ci0; C = a.C0; }
+    else { src = a.x1; cs = ci0 - a.C0; C = a.C1; }
+    const long total = (long)a.N * a.H * a.W;
+    const long p_begin = (long)pchunk * a.pix_per_cta;
+    const long p_end = min(total, p_begin + a.pix_per_cta);
+    // warp w: co rows 16*(w&1).., ci cols 16*(w>>1).. (2 n8 tiles)
+    const int wm = (warp & 1) * 16, wn = (warp >> 1) * 16;
+    float acc[2][4];
+#pragma unroll
+    for (int t = 0; t < 2; t++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) acc[t][e] = 0.f;
+    float bsum = 0.f;
+    for (long p0 = p_begin; p0 < p_end; p0 += WG_KP) {
+        for (int e = tid; e < WG_KP * 4; e += 128) {
+            const int pp = e >> 2, q = e & 3;
+            const long p = p0 + pp;
+            uint4 vd = make_uint4(0, 0, 0, 0), vx = make_uint4(0, 0, 0, 0);
+            if (p < p_end) {
+                const int xx = (int)(p % a.W);
+                const long r = p / a.W;
+                const int yy = (int)(r % a.H), n = (int)(r / a.H);
+                if (co0 + q * 8 < a.Cout)
+                    vd = *reinterpret_cast<const uint4 *>(a.dy + p * a.Cout + co0 + q * 8);
+                const int sy = yy + ky, sx = xx + kx;
+                if (sy >= 0 && sy < a.H && sx >= 0 && sx < a.W)
+                    vx = *reinterpret_cast<const uint4 *>(src + (((size_t)n * a.H + sy) * a.W + sx) * C + cs + q * 8);
+            }
+            *reinterpret_cast<uint4 *>(&Ds[pp * WG_LD + q * 8]) = vd;
+            *reinterpret_cast<uint4 *>(&Xs[pp * WG_LD + q * 8]) = vx;
+        }
+        __syncthreads();
+        if (a.dbias && tap == 4 && cib == 0 && tid < WG_CO) {
+            for (int pp = 0; pp < WG_KP; pp++) bsum += __bfloat162float(Ds[pp * WG_LD + tid]);
+        }
+#pragma unroll
+        for (int kk = 0; kk < WG_KP; kk += 16) {
+            // A (16 co x 16 pixels) from Ds[pixel][co]: transposed loads
+            uint32_t a0, a1, a2, a3;
+            {
+                const int mi = lane >> 3, r = lane & 7;
+                // matrices: (co lo, k lo) (co hi, k lo) (co lo, k hi) (co hi, k hi)
+                const bf16 *pa = &Ds[(kk + (mi >> 1) * 8 + r) * WG_LD + wm + (mi & 1) * 8];
+                ldmatrix_x4_trans(a0, a1, a2, a3, pa);
+            }
+            // B (16 pixels x 16 ci) from Xs[pixel][ci]: transposed loads give [ci][k] fragments
+            uint32_t b0, b1, b2, b3;
+            {
+                const int mi = lane >> 3, r = lane & 7;
+                // matrices: (ci 0-7, k lo) (ci 0-7, k hi) (ci 8-15, k lo) (ci 8-15, k hi)
+                const bf16 *pb = &Xs[(kk + (mi & 1) * 8 + r) * WG_LD + wn + (mi >> 1) * 8];
+                ldmatrix_x4_trans(b0, b1, b2, b3, pb);
+            }
+            mma_bf16(acc[0], a0, a1, a2, a3, b0, b1);
+            mma_bf16(acc[1], a0, a1, a2, a3, b2, b3);
+        }
+        __syncthreads();
+    }
+    const int g = lane >> 2, tg = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int co = co0 + wm + g + h * 8;
+            const int ci = ci0 + wn + nt * 8 + tg * 2;
+            if (co >= a.Cout) continue;
+            float *d = a.dw + ((size_t)co * 9 + tap) * Cin + ci;
+            atomicAdd(d, acc[nt][h * 2]);
+            atomicAdd(d + 1, acc[nt][h * 2 + 1]);
+        }
+    if (a.dbias && tap == 4 && cib == 0 && tid < WG_CO && co0 + tid < a.Cout) atomicAdd(&a.dbias[co0 + tid], bsum);
+}
+
+// --------------------------------------------------------- small kernels
+// w'[ci][tap'][co] = w[co][8 - tap'][ci]  (data-gradient weights)
+__global__ void flip_weights_kernel(const bf16 *w, bf16 *wt, int Cout, int Cin)
+{
+    const size_t n = (size_t)Cout * 9 * Cin;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int ci = (int)(e % Cin);
+        const int tap = (int)((e / Cin) % 9);
+        const int co = (int)(e / ((size_t)Cin * 9));
+        wt[((size_t)ci * 9 + (8 - tap)) * Cout + co] = w[e];
+    }
+}
+
+__global__ void relu_bwd_kernel(const bf16 *y, const bf16 *dy, bf16 *dpre, size_t n)
+{
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        dpre[e] = __bfloat162float(y[e]) > 0.f ? dy[e] : __float2bfloat16(0.f);
+}
+
+// 2x2 average pooling, NHWC
+__global__ void pool_fwd_kernel(const bf16 *x, bf16 *y, int N, int H, int W, int C)
+{
+    const int Ho = H / 2, Wo = W / 2;
+    const size_t n = (size_t)N * Ho * Wo * C;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const size_t pix = e / C;
+        const int xo = (int)(pix % Wo), yo = (int)((pix / Wo) % Ho), b = (int)(pix / ((size_t)Wo * Ho));
+        const size_t base = (((size_t)b * H + 2 * yo) * W + 2 * xo) * C + c;
+        const float s = __bfloat162float(x[base]) + __bfloat162float(x[base + C]) +
+                        __bfloat162float(x[base + (size_t)W * C]) + __bfloat162float(x[base + (size_t)W * C + C]);
+        y[e] = __float2bfloat16(0.25f * s);
+    }
+}
+
+__global__ void pool_bwd_kernel(const bf16 *dy, bf16 *dx, int N, int H, int W, int C)
+{
+    // dx[b][y][x][c] = 0.25 * dy[b][y/2][x/2][c]
+    const size_t n = (size_t)N * H * W * C;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const size_t pix = e / C;
+        const int x = (int)(pix % W), y = (int)((pix / W) % H), b = (int)(pix / ((size_t)W * H));
+        dx[e] = __float2bfloat16(0.25f * __bfloat162float(dy[(((size_t)b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c]));
+    }
+}
+
+// nearest 2x upsampling (H, W = input size)
+__global__ void up_fwd_kernel(const bf16 *x, bf16 *y, int N, int H, int W, int C)
+{
+    const size_t n = (size_t)N * 4 * H * W * C;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const size_t pix = e / C;
+        const int X = (int)(pix % (2 * W)), Y = (int)((pix / (2 * W)) % (2 * H)), b = (int)(pix / ((size_t)4 * W * H));
+        y[e] = x[(((size_t)b * H + Y / 2) * W + X / 2) * C + c];
+    }
+}
+
+__global__ void up_bwd_kernel(const bf16 *dy, bf16 *dx, int N, int H, int W, int C)
+{
+    const size_t n = (size_t)N * H * W * C;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const size_t pix = e / C;
+        const int x = (int)(pix % W), y = (int)((pix / W) % H), b = (int)(pix / ((size_t)W * H));
+        const size_t base = (((size_t)b * 2 * H + 2 * y) * 2 * W + 2 * x) * C + c;
+        const size_t rs = (size_t)2 * W * C;
+        dx[e] = __float2bfloat16(__bfloat162float(dy[base]) + __bfloat162float(dy[base + C]) +
+                                 __bfloat162float(dy[base + rs]) + __bfloat162float(dy[base + rs + C]));
+    }
+}
+
+// input image (FP32 [N][H][W], scaled) -> BF16 NHWC with C channels, channel 0 = image
+__global__ void input_pack_kernel(const float *img, const float *scale, bf16 *x, int N, int H, int W, int C)
+{
+    const size_t n = (size_t)N * H * W * C;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const size_t pix = e / C;
+        const int b = (int)(pix / ((size_t)H * W));
+        x[e] = __float2bfloat16(c == 0 ? img[pix] * scale[b] : 0.f);
+    }
+}
+
+// head: out[p] = inp[p] + sum_c h[p][c] * w[c] + b   (FP32 out; residual on the scaled input)
+__global__ void head_fwd_kernel(const bf16 *h, const float *w, const float *b, const float *img, const float *scale,
+                                float *out, int N, int HW, int C)
+{
+    const size_t n = (size_t)N * HW;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        float s = b[0];
+        for (int c = 0; c < C; c++) s += __bfloat162float(h[p * C + c]) * w[c];
+        out[p] = img[p] * scale[p / HW] + s;
+    }
+}
+
+// MSE loss gradient on the head output: g = 2 (out - target*scale) / count; loss partial sums in FP64
+__global__ void mse_grad_kernel(const float *out, const float *target, const float *scale, float *g, double *loss,
+                                int N, int HW)
+{
+    const size_t n = (size_t)N * HW;
+    double part = 0.0;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const float d = out[p] - target[p] * scale[p / HW];
+        g[p] = 2.f * d / (float)n;
+        part += (double)d * d;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    if ((threadIdx.x & 31) == 0 && loss) atomicAdd(loss, part / (double)n);
+}
+
+// head backward: dh[p][c] = g[p] * w[c]; dw[c] += sum_p g[p] h[p][c]; db += sum g
+__global__ void head_bwd_kernel(const bf16 *h, const float *w, const float *g, bf16 *dh, float *dw, float *db, int N,
+                                int HW, int C)
+{
+    const size_t n = (size_t)N * HW;
+    float lw[64];
+    for (int c = 0; c < C; c++) lw[c] = 0.f;
+    float lb = 0.f;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const float gp = g[p];
+        lb += gp;
+        for (int c = 0; c < C; c++) {
+            dh[p * C + c] = __float2bfloat16(gp * w[c]);
+            lw[c] += gp * __bfloat162float(h[p * C + c]);
+        }
+    }
+    for (int c = 0; c < C; c++) {
+        float v = lw[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&dw[c], v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lb += __shfl_xor_sync(0xffffffffu, lb, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(db, lb);
+}
+
+// Adam on FP32 master weights; writes the BF16 compute copy (wb may be null)
+__global__ void adam_kernel(float *w, float *m, float *v, const float *g, bf16 *wb, size_t n, float lr, float b1,
+                            float b2, float eps, float c1, float c2)
+{
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const float gi = g[e];
+        const float mi = b1 * m[e] + (1.f - b1) * gi;
+        const float vi = b2 * v[e] + (1.f - b2) * gi * gi;
+        m[e] = mi;
+        v[e] = vi;
+        const float wi = w[e] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        w[e] = wi;
+        if (wb) wb[e] = __float2bfloat16(wi);
+    }
+}
+
+__global__ void add_bf16_kernel(bf16 *y, const bf16 *x, size_t n)
+{
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        y[e] = __float2bfloat16(__bfloat162float(y[e]) + __bfloat162float(x[e]));
+}
+
+__global__ void f32_to_bf16_kernel(const float *a, bf16 *b, size_t n)
+{
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        b[e] = __float2bfloat16(a[e]);
+}
+
+static int grid_for(size_t n)
+{
+    size_t g = (n + 255) / 256;
+    return (int)(g > 148 * 32 ? 148 * 32 : (g == 0 ? 1 : g));
+}
+
+}  // namespace raft
+
+using namespace raft;
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+// y = act(conv3x3(concat(x0, x1)) + bias); C0, C1, Cout multiples of 32 (C1 may be 0).
+// With y1 != NULL the output channels are split: [0, Cy0) -> y, [Cy0, Cout) -> y1
+// (the data gradient of a concatenated input, back into its two parts).
+int raft_unet_conv_fwd(const void *x0, int C0, const void *x1, int C1, const void *w, const float *bias, void *y,
+                       void *y1, int Cy0, int N, int H, int W, int Cout, int relu, void *stream)
+{
+    if (C0 % 32 || C1 % 32 || Cout % 32 || N < 1 || H < 1 || W < 1) return 1;
+    if (y1 && (Cy0 % 32 || Cy0 <= 0 || Cy0 >= Cout)) return 1;
+    ConvArgs a{(const bf16 *)x0, (const bf16 *)x1, C0, C1, (const bf16 *)w, bias, (bf16 *)y, (bf16 *)y1, Cy0,
+               N, H, W, Cout, relu};
+    dim3 grid((unsigned)((size_t)N * H * ((W + CV_PIX - 1) / CV_PIX)), Cout / CV_CO);
+    count_launch();
+    conv3x3_fwd_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(a);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// dW += sum_p dY[p] x[p+tap] (FP32), dbias += sum_p dY[p] (if non-null).
+int raft_unet_conv_wgrad(const void *dy, const void *x0, int C0, const void *x1, int C1, float *dw, float *dbias,
+                         int N, int H, int W, int Cout, void *stream)
+{
+    if (C0 % 32 || C1 % 32 || Cout % 32) return 1;
+    const int Cin = C0 + C1;
+    const long total = (long)N * H * W;
+    const int ppc = 2048;
+    WgradArgs a{(const bf16 *)dy, (const bf16 *)x0, (const bf16 *)x1, C0, C1, dw, dbias, N, H, W, Cout, ppc};
+    dim3 grid((unsigned)(9 * (Cin / WG_CI) * (Cout / WG_CO)), (unsigned)((total + ppc - 1) / ppc));
+    count_launch();
+    conv3x3_wgrad_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(a);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+int raft_unet_flip_weights(const void *w, void *wt, int Cout, int Cin, void *stream)
+{
+    const size_t n = (size_t)Cout * 9 * Cin;
+    count_launch();
+    flip_weights_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const bf16 *)w, (bf16 *)wt, Cout, Cin);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+int raft_unet_relu_bwd(const void *y, const void *dy, void *dpre, size_t n, void *stream)
+{
+    count_launch();
+    relu_bwd_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const bf16 *)y, (const bf16 *)dy, (bf16 *)dpre, n);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+int raft_unet_pool(int backward, const void *src, void *dst, int N, int H, int W, int C, void *stream)
+{
+    count_launch();
+    if (!backward)
+        pool_fwd_kernel<<<grid_for((size_t)N * H * W * C / 4), 256, 0, (cudaStream_t)stream>>>((const bf16 *)src,
+                                                                                                (bf16 *)dst, N, H, W, C);
+    else
+        pool_bwd_kernel<<<grid_for((size_t)N * H * W * C), 256, 0, (cudaStream_t)stream>>>((const bf16 *)src,
+                                                                                            (bf16 *)dst, N, H, W, C);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// H, W: the low-resolution size
+int raft_unet_upsample(int backward, const void *src, void *dst, int N, int H, int W, int C, void *stream)
+{
+    count_launch();
+    if (!backward)
+        up_fwd_kernel<<<grid_for((size_t)N * 4 * H * W * C), 256, 0, (cudaStream_t)stream>>>(
+            (const bf16 *)src, (bf16 *)dst, N, H, W, C);
+    else
+        up_bwd_kernel<<<grid_for((size_t)N * H * W * C), 256, 0, (cudaStream_t)stream>>>((const bf16 *)src,
+                                                                                          (bf16 *)dst, N, H, W, C);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+int raft_unet_input(const float *img, const float *scale, void *x, int N, int H, int W, int C, void *stream)
+{
+    count_launch();
+    input_pack_kernel<<<grid_for((size_t)N * H * W * C), 256, 0, (cudaStream_t)stream>>>(img, scale, (bf16 *)x, N, H,
+                                                                                        W, C);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+int raft_unet_head(int backward, const void *h, const float *w, const float *b, const float *img,
+                   const float *scale, float *out_or_grad, void *dh, float *dw, float *db, int N, int HW, int C,
+                   void *stream)
+{
+    if (C > 64) return 1;
+    count_launch();
+    if (!backward)
+        head_fwd_kernel<<<grid_for((size_t)N * HW), 256, 0, (cudaStream_t)stream>>>((const bf16 *)h, w, b, img, scale,
+                                                                                    out_or_grad, N, HW, C);
+    else
+        head_bwd_kernel<<<grid_for((size_t)N * HW), 256, 0, (cudaStream_t)stream>>>((const bf16 *)h, w, out_or_grad,
+                                                                                    (bf16 *)dh, dw, db, N, HW, C);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+int raft_unet_mse(const float *out, const float *target, const float *scale, float *grad, double *loss, int N, int HW,
+                  void *stream)
+{
+    count_launch();
+    mse_grad_kernel<<<grid_for((size_t)N * HW), 256, 0, (cudaStream_t)stream>>>(out, target, scale, grad, loss, N, HW);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+int raft_unet_adam(float *w, float *m, float *v, const float *g, void *wb, size_t n, float lr, float b1, float b2,
+                   float eps, int step, void *stream)
+{
+    const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+    count_launch();
+    adam_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(w, m, v, g, (bf16 *)wb, n, lr, b1, b2, eps, c1, c2);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+int raft_unet_add(void *y, const void *x, size_t n, void *stream)
+{
+    count_launch();
+    add_bf16_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((bf16 *)y, (const bf16 *)x, n);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+int raft_unet_to_bf16(const float *a, void *b, size_t n, void *stream)
+{
+    count_launch();
+    f32_to_bf16_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(a, (bf16 *)b, n);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+}  // extern "C"
