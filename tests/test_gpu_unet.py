@@ -5,8 +5,10 @@
   rel-L2 <= 1e-2 for BF16 outputs, <= 1e-4 for the FP32 weight gradient;
 * the whole network's parameter gradients vs PyTorch FP32 autograd on the
   same weights and inputs: rel-L2 <= 5e-2 per tensor (BF16 activations);
-* training lowers the loss, and a briefly trained network's warm start
-  reaches the plain 100-iteration EM residual in fewer iterations."""
+* training lowers the loss by a quarter or more, the trained network's output
+  on held-out pairs is closer to the EM label than its FBP input (MSE below
+  0.8x), and its warm start reaches the plain-EM target residual in fewer
+  iterations than plain EM."""
 import ctypes
 
 import numpy as np
@@ -124,8 +126,15 @@ def test_training_reduces_loss_and_warm_start_helps():
     dev = torch.device("cuda", 0)
     inputs, labels, trans, ang = ws.make_pairs(96, 70_000, dev, N=128, A=96, em_iters=60, chunk=48)
     net = ws.UNet(dev, seed=0)
-    losses = ws.train(net, inputs[:80], labels[:80], epochs=10, batch=8, lr=2e-3)
-    assert np.mean(losses[-8:]) < 0.5 * np.mean(losses[:8])
+    losses = ws.train(net, inputs[:80], labels[:80], epochs=24, batch=8, lr=2e-3)
+    assert np.mean(losses[-8:]) < 0.75 * np.mean(losses[:8]), (np.mean(losses[:8]), np.mean(losses[-8:]))
+    # held-out: the network's output is closer to the EM label than its own FBP input
+    x, y = inputs[80:].contiguous(), labels[80:].contiguous()
+    sc = ws.input_scale(x)
+    out = net.forward(x, sc)
+    mse_net = float(((out - y * sc[:, None, None]) ** 2).mean())
+    mse_fbp = float((((x - y) * sc[:, None, None]) ** 2).mean())
+    assert mse_net < 0.8 * mse_fbp, (mse_net, mse_fbp)
     r = ws.evaluate(net, inputs[80:], trans[80:], ang, plain_iters=40, max_warm_iters=40)
     # the trained network's start is closer to the data than the uniform start,
     # and reaches the plain-EM target residual in fewer iterations
