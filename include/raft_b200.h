@@ -85,8 +85,13 @@ int raft_abi_version(void);
 int raft_fbp_ext(int *gpus, int ngpus, float *obj, const float *tomogram, const float *angles,
                  const float *paramf, const int *parami, int geometry, int store);
 
-/* FBP on device-resident buffers of one GPU (d_obj, d_tomogram on `gpu`;
- * angles host), issued on `stream` (NULL: library stream, synchronised).
+/* Streams of the device-pointer entry points below: work is issued on `stream`; NULL
+ * means "ordered after everything already queued on the legacy default stream" (the
+ * stream PyTorch uses by default): the library then runs on its own stream, made to
+ * wait for that work, and synchronises it before returning.
+ *
+ * FBP on device-resident buffers of one GPU (d_obj, d_tomogram on `gpu`;
+ * angles host), issued on `stream` (NULL: see above).
  * Same operator as raft_fbp_ext; getFBPGPU-level entry (fbp.cu:127-236). */
 int raft_fbp_device(int gpu, float *d_obj, const float *d_tomogram, const float *angles,
                     const float *paramf, const int *parami, int geometry, int store, void *stream);
@@ -127,7 +132,7 @@ typedef struct raft_request {
  * graph; FBP and EM proceed on two streams.  geometry/store select the FBP operator as in
  * raft_fbp_ext.  latency_ms[i] (may be NULL) receives request i's completion time and
  * *total_ms the whole batch's, both measured on the device from the batch start.
- * Returns 0 on success. */
+ * NULL stream as raft_fbp_device.  Returns 0 on success. */
 int raft_ragged_device(int gpu, const raft_request *reqs, int nreq, int geometry, int store,
                        double *latency_ms, double *total_ms, void *stream);
 
@@ -141,11 +146,12 @@ int raft_em_ext(int kind, int gpu, float *obj, const float *data, const float *f
                 double *metrics, int use_graph);
 
 /* getRadonRTMultiGPU's operator on device-resident buffers of one GPU (angles host),
- * issued on `stream` (NULL: library stream, synchronised).  Returns 0 on success. */
+ * issued on `stream` (NULL: after the legacy default stream's queued work, synchronised).  Returns 0 on success. */
 int raft_radon_device(int gpu, float *d_out, const float *d_phantom, const float *angles, int nx, int ny,
                       int nrays, int nangles, int nslices, float ax, float ay, void *stream);
 
-/* As raft_em_ext on device-resident buffers (metrics device pointer or NULL). */
+/* As raft_em_ext on device-resident buffers (metrics device pointer or NULL); NULL
+ * stream as raft_fbp_device.  Synchronises before returning. */
 int raft_em_device(int kind, int gpu, float *d_obj, const float *d_data, const float *d_flat,
                    const float *angles, int nrays, int nangles, int nslices, int niter,
                    double *d_metrics, int use_graph, void *stream);

@@ -270,8 +270,9 @@ int raft_fbp_ext(int *gpus, int ngpus, float *obj, const float *tomogram, const 
 }
 
 // Device-resident FBP on one GPU: d_obj / d_tomogram are device pointers on
-// `gpu`, angles is host.  Runs on `stream` (0 = the library's own stream,
-// synchronised before returning).
+// `gpu`, angles is host.  Runs on `stream`; 0 = after the work already queued
+// on the legacy default stream, on the library's own stream, synchronised
+// before returning.
 int raft_fbp_device(int gpu, float *d_obj, const float *d_tomogram, const float *angles, const float *paramf,
                     const int *parami, int geometry, int store, void *stream)
 {
@@ -286,7 +287,7 @@ int raft_fbp_device(int gpu, float *d_obj, const float *d_tomogram, const float 
         std::lock_guard<std::mutex> lk(ds.mtx);
         RAFT_CUDA(cudaSetDevice(gpu));
         ds.ensure();
-        cudaStream_t st = stream ? (cudaStream_t)stream : ds.s_comp;
+        cudaStream_t st = resolve_stream(ds, stream, ds.s_comp);
         FbpPrepared fp = prepare_fbp(cfg, gpu);
         FbpTables tb = fbp_tables(ds, fp, angles, st);
         const size_t tomo_ps = (size_t)cfg.nangles * cfg.nrays;
@@ -431,7 +432,7 @@ int raft_em_device(int kind, int gpu, float *d_obj, const float *d_data, const f
         RAFT_CUDA(cudaSetDevice(gpu));
         ds.ensure();
         EmPrepared ep = prepare_em(cfg);
-        cudaStream_t st = stream ? (cudaStream_t)stream : ds.s_comp;
+        cudaStream_t st = resolve_stream(ds, stream, ds.s_comp);
         em_chunk(ds, ep, kind, d_data, d_flat, angles, d_obj, nslices, d_metrics, use_graph != 0, st);
     } catch (const CudaFail &) {
     }
@@ -519,7 +520,7 @@ int raft_radon_device(int gpu, float *d_out, const float *d_phantom, const float
         std::lock_guard<std::mutex> lk(ds.mtx);
         RAFT_CUDA(cudaSetDevice(gpu));
         ds.ensure();
-        cudaStream_t st = stream ? (cudaStream_t)stream : ds.s_comp;
+        cudaStream_t st = resolve_stream(ds, stream, ds.s_comp);
         float *d_ang = (float *)ds.angles.get(sizeof(float) * nangles);
         RAFT_CUDA(cudaMemcpyAsync(d_ang, angles, sizeof(float) * nangles, cudaMemcpyHostToDevice, st));
         float *imgT = (float *)ds.imgT.get(sizeof(float) * (size_t)nx * ny * std::max(1, nslices));

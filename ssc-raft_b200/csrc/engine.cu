@@ -81,7 +81,16 @@ void DeviceState::ensure()
         RAFT_CUDA(cudaEventCreateWithFlags(&ev_comp[b], cudaEventDisableTiming));
         RAFT_CUDA(cudaEventCreateWithFlags(&ev_d2h[b], cudaEventDisableTiming));
     }
+    RAFT_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     init = true;
+}
+
+cudaStream_t resolve_stream(DeviceState &ds, void *stream, cudaStream_t own)
+{
+    if (stream) return (cudaStream_t)stream;
+    RAFT_CUDA(cudaEventRecord(ds.ev_join, cudaStreamLegacy));
+    RAFT_CUDA(cudaStreamWaitEvent(own, ds.ev_join, 0));
+    return own;
 }
 
 static std::mutex g_state_mtx;

@@ -34,11 +34,21 @@ struct DeviceState {
     DevBuf sino[2], img[2], rows, den, flat, data, angles, tabs, metrics, err, imgT;
     PinBuf pin_in[2], pin_out[2];
     cudaEvent_t ev_h2d[2] = {}, ev_comp[2] = {}, ev_d2h[2] = {};
+    cudaEvent_t ev_join = nullptr;
     bool init = false;
     void ensure();
 };
 
 DeviceState &device_state(int device);
+
+// The stream a device-pointer entry point runs on.  A caller stream is used
+// as given.  NULL means the legacy default stream (PyTorch's default stream
+// is that stream); the library does not run on it (a CUDA graph cannot be
+// captured there) but on its own non-blocking stream `own`, which does not
+// order itself after the legacy stream by itself -- so `own` is first made to
+// wait for everything already queued there (the caller's copy that produced
+// an input, say).  Entry points synchronise `own` before returning.
+cudaStream_t resolve_stream(DeviceState &ds, void *stream, cudaStream_t own);
 
 // Filter plan cache (per device, keyed by every spectrum input).
 const FilterPlan &cached_filter_plan(int device, int geometry, int ftype, int N, int pad, double paganin,

@@ -27,18 +27,20 @@ namespace raft {
 
 namespace {
 
+// Byte offsets into the batch workspace (every region is assigned by the
+// layout loop below; they start at zero only so that none is ever undefined).
 struct FbpReq {
-    int idx;
+    int idx = 0;
     FbpPrepared fp;
-    size_t tab, rows;
-    double cost;
+    size_t tab = 0, rows = 0;
+    double cost = 0.0;
 };
 
 struct EmReq {
-    int idx;
+    int idx = 0;
     EmPrepared ep;
-    size_t tab, rows, den, imgT;
-    double cost;
+    size_t tab = 0, rows = 0, den = 0, imgT = 0;
+    double cost = 0.0;
 };
 
 size_t a256(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -88,7 +90,7 @@ extern "C" int raft_ragged_device(int gpu, const raft_request *reqs, int nreq, i
         RAFT_CUDA(cudaSetDevice(gpu));
         ds.ensure();
         // s0: caller's stream (or the high-priority one) for FBP; s1: low-priority EM
-        cudaStream_t s0 = stream ? (cudaStream_t)stream : ds.s_hi;
+        cudaStream_t s0 = resolve_stream(ds, stream, ds.s_hi);
         cudaStream_t s1 = ds.s_lo;
 
         // ---- plan every request and lay out one workspace ----------------
@@ -134,6 +136,8 @@ extern "C" int raft_ragged_device(int gpu, const raft_request *reqs, int nreq, i
                 r.rows = off;
                 off = a256(off + sizeof(float) * (size_t)A * r.ep.win.Wg);
                 r.den = off;
+                off = a256(off + sizeof(float) * (size_t)N * N);
+                r.imgT = off;                      // transposed iterate for the projector's steep angles
                 off = a256(off + sizeof(float) * (size_t)N * N);
                 r.cost = 2.0 * N * N * A * q.niter;
                 E.push_back(r);

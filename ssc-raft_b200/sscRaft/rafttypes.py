@@ -67,6 +67,8 @@ libraft.raft_fbp_device_noalloc.restype = _I
 libraft.raft_em_ext.argtypes = [_I, _I, _P, _P, _P, _P, _I, _I, _I, _I, _P, _I]
 libraft.raft_em_ext.restype = _I
 libraft.raft_em_device.argtypes = [_I, _I, _P, _P, _P, _P, _I, _I, _I, _I, _P, _I, _P]
+libraft.raft_radon_device.argtypes = [_I, _P, _P, _P, _I, _I, _I, _I, _I, _F, _F, _P]
+libraft.raft_radon_device.restype = _I
 libraft.raft_em_device.restype = _I
 
 libraft.raft_launch_count.argtypes = []
