@@ -536,6 +536,21 @@ static bool tuning_enabled()
     return !(e && e[0] == '0');
 }
 
+// RAFT_BP_TUNE="S,AB" forces one candidate (for tests that compare every
+// launch shape); returns false when unset, malformed or not a candidate.
+static bool forced_tune(BpTune &t)
+{
+    const char *e = std::getenv("RAFT_BP_TUNE");
+    int s = 0, ab = 0;
+    if (!e || std::sscanf(e, "%d,%d", &s, &ab) != 2) return false;
+    for (const BpTune &c : kTuneCandidates)
+        if (c.S == s && c.AB == ab) {
+            t = c;
+            return true;
+        }
+    return false;
+}
+
 // Pick (S, AB) for this configuration: the cached choice, else time every
 // candidate that fits shared memory on up to 8 slices of the real data
 // (store launches only -- they are idempotent), else a default.
@@ -544,12 +559,14 @@ static BpTune choose_tune(const BpArgs &a, int geometry, int store, cudaStream_t
     int dev = 0;
     cudaGetDevice(&dev);
     const TuneKey key(dev, geometry, store, a.No, a.W, a.nangles);
+    const int esize = store_bytes(store);
+    BpTune forced;
+    if (forced_tune(forced) && bp_smem(forced.S, forced.AB, a.W, esize) <= kBpSmemMax) return forced;
     {
         std::lock_guard<std::mutex> lk(g_tune_mtx);
         auto it = g_tune.find(key);
         if (it != g_tune.end()) return it->second;
     }
-    const int esize = store_bytes(store);
     BpTune best{2, 16};
     if (bp_smem(best.S, best.AB, a.W, esize) > kBpSmemMax) best = {1, 8};
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
