@@ -34,8 +34,6 @@ libraft.raft_unet_mse.argtypes = [_P, _P, _P, _P, _P, _I, _I, _P]
 libraft.raft_unet_adam.argtypes = [_P, _P, _P, _P, _P, _Z, _F, _F, _F, _F, _I, _P]
 libraft.raft_unet_add.argtypes = [_P, _P, _Z, _P]
 libraft.raft_unet_to_bf16.argtypes = [_P, _P, _Z, _P]
-libraft.raft_radon_device.argtypes = [_I, _P, _P, _P, _I, _I, _I, _I, _I, _F, _F, _P]
-libraft.raft_radon_device.restype = _I
 for _f in ("raft_unet_conv_fwd", "raft_unet_conv_wgrad", "raft_unet_flip_weights", "raft_unet_relu_bwd",
            "raft_unet_pool", "raft_unet_upsample", "raft_unet_input", "raft_unet_head", "raft_unet_mse",
            "raft_unet_adam", "raft_unet_add", "raft_unet_to_bf16"):
@@ -265,6 +263,39 @@ class UNet:
             self.b[k] = torch.as_tensor(state[k + ".bias"], device=self.dev).contiguous()
         self._sync_bf16()
 
+    def save(self, path, **meta):
+        """Weights file: 3x3 convolution weights as BF16 bit patterns (the
+        precision inference runs in), biases and the head in FP32, plus
+        free-form metadata (training recipe)."""
+        torch = self.torch
+        arr = {}
+        for k, v in self.w.items():
+            if k == "head":
+                arr[k] = v.detach().cpu().numpy().astype(np.float32)
+            else:
+                arr[k + ".bf16"] = v.detach().to(torch.bfloat16).view(torch.int16).cpu().numpy()
+        for k, v in self.b.items():
+            arr[k + ".bias"] = v.detach().cpu().numpy().astype(np.float32)
+        arr["meta"] = np.array(repr(meta))
+        np.savez_compressed(path, **arr)
+
+    @classmethod
+    def from_file(cls, path, device):
+        """A network with the weights `save` wrote (FP32 masters = the BF16 values)."""
+        import torch
+        net = cls(device, seed=0)
+        z = np.load(path)
+        st = {}
+        for k in net.w:
+            if k == "head":
+                st[k] = z[k]
+            else:
+                st[k] = torch.from_numpy(z[k + ".bf16"]).view(torch.bfloat16).float().numpy()
+            st[k + ".bias"] = z[k + ".bias"]
+        net.load(st)
+        net.meta = str(z["meta"])
+        return net
+
 
 def input_scale(img):
     """Per-image normalisation: 1 / mean |input|."""
@@ -296,19 +327,38 @@ def perlin(N, seed, cells=8, device=None):
     return (n0 * (1 - v) + n1 * v) * 1.4
 
 
-def make_pairs(n, seed0, device, N=512, A=720, em_iters=200, chunk=64, i0_range=(1e3, 1e5), gpu=0):
-    """(input, label, transmission) triples made by the method itself:
-    ellipse + Perlin-texture phantoms on the EM grid, scaled so the largest
-    line integral is 3; Radon projections; Poisson counts at I0 ~ U[i0_range];
-    FBP (linear operator, Hann) of -log(transmission) mapped to the EM grid as
-    the network input; `em_iters`-iteration tEM from a uniform start as the
-    label.  Everything stays on the device."""
+def fbp_input(trans, ang, gpu=0, out=None):
+    """Network input from normalised transmissions t [n, A, N] (device):
+    FBP (linear-interpolation backprojector, Hann filter, pad 2) of -log t,
+    flipped in y and scaled by (N-1)/2 onto the EM grid."""
     import torch
-    ang = S.uniform_angles(A)
-    angp = np.ascontiguousarray(ang)
-    inputs = torch.empty((n, N, N), dtype=torch.float32, device=device)
-    labels = torch.empty((n, N, N), dtype=torch.float32, device=device)
-    trans = torch.empty((n, A, N), dtype=torch.float32, device=device)
+    n, A, N = trans.shape
+    dev = trans.device
+    st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    sino = (-torch.log(trans)).contiguous()
+    fbp = torch.empty((n, N, N), dtype=torch.float32, device=dev)
+    pf = np.array([0, 0, 1, 0, 1, 1, 0], np.float32)
+    pi = np.array([N, A, n, N, 2, 0, 0, 5, 0, 0], np.int32)
+    rc = libraft.raft_fbp_device(gpu, _p(fbp), _p(sino), _ptr(np.ascontiguousarray(ang)), _ptr(pf), _ptr(pi),
+                                 1, 1, st)
+    if rc:
+        check_error("fbp")
+    res = torch.flip(fbp, dims=(1,))
+    res *= (N - 1) / 2.0
+    if out is None:
+        return res
+    out.copy_(res)
+    return out
+
+
+def make_transmissions(n, seed0, device, N=512, A=720, chunk=64, i0_range=(1e3, 1e5), gpu=0, out=None):
+    """Normalised transmissions t = counts/I0 [n, A, N] of seeded phantoms:
+    random ellipses (seed s = seed0 + i) with seeded Perlin texture on the EM
+    grid, Radon projections scaled so the largest line integral is 3, Poisson
+    counts at I0 ~ U[i0_range] per slice."""
+    import torch
+    angp = np.ascontiguousarray(S.uniform_angles(A))
+    trans = out if out is not None else torch.empty((n, A, N), dtype=torch.float32, device=device)
     st = ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
     rng = np.random.Generator(np.random.PCG64(seed0))
     for c0 in range(0, n, chunk):
@@ -326,22 +376,45 @@ def make_pairs(n, seed0, device, N=512, A=720, em_iters=200, chunk=64, i0_range=
         i0 = torch.as_tensor(rng.uniform(i0_range[0], i0_range[1], m), dtype=torch.float64, device=device)
         gen = torch.Generator(device=device).manual_seed(seed0 + c0)
         counts = torch.poisson(i0[:, None, None] * torch.exp(-proj.double()), generator=gen)
-        t = (counts.clamp(min=1.0) / i0[:, None, None]).float().contiguous()
-        trans[c0:c0 + m] = t
-        sino = (-torch.log(t)).contiguous()
-        fbp = torch.empty((m, N, N), dtype=torch.float32, device=device)
-        pf = np.array([0, 0, 1, 0, 1, 1, 0], np.float32)
-        pi = np.array([N, A, m, N, 2, 0, 0, 5, 0, 0], np.int32)
-        rc = libraft.raft_fbp_device(gpu, _p(fbp), _p(sino), _ptr(angp), _ptr(pf), _ptr(pi), 1, 1, st)
-        if rc:
-            check_error("fbp")
-        inputs[c0:c0 + m] = torch.flip(fbp, dims=(1,)) * ((N - 1) / 2.0)
-        obj = torch.ones((m, N, N), dtype=torch.float32, device=device)
-        flat = torch.ones((m, N), dtype=torch.float32, device=device)
-        rc = libraft.raft_em_device(0, gpu, _p(obj), _p(t), _p(flat), _ptr(angp), N, A, m, em_iters, None, 1, st)
-        if rc:
-            check_error("tem")
-        labels[c0:c0 + m] = obj
+        trans[c0:c0 + m] = (counts.clamp(min=1.0) / i0[:, None, None]).float()
+    return trans
+
+
+def em_label(trans, iters, gpu=0):
+    """`iters` tEM iterations from the uniform start (the reference's default
+    initial guess), [n, N, N] on the EM grid."""
+    import torch
+    n, A, N = trans.shape
+    dev = trans.device
+    st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    ang = np.ascontiguousarray(S.uniform_angles(A))
+    obj = torch.ones((n, N, N), dtype=torch.float32, device=dev)
+    flat = torch.ones((n, N), dtype=torch.float32, device=dev)
+    rc = libraft.raft_em_device(0, gpu, _p(obj), _p(trans), _p(flat), _ptr(ang), N, A, n, iters, None, 1, st)
+    if rc:
+        check_error("tem")
+    return obj
+
+
+def make_pairs(n, seed0, device, N=512, A=720, em_iters=200, chunk=64, i0_range=(1e3, 1e5), gpu=0,
+               keep_trans=True):
+    """(input, label, transmission) triples made by the method itself:
+    make_transmissions' seeded data, the FBP input of fbp_input, and
+    `em_iters`-iteration tEM from a uniform start as the label.  Everything
+    stays on the device; with keep_trans=False only one chunk of
+    transmissions is held at a time and None is returned in its place."""
+    import torch
+    ang = S.uniform_angles(A)
+    inputs = torch.empty((n, N, N), dtype=torch.float32, device=device)
+    labels = torch.empty((n, N, N), dtype=torch.float32, device=device)
+    trans = torch.empty((n, A, N), dtype=torch.float32, device=device) if keep_trans else None
+    for c0 in range(0, n, chunk):
+        m = min(chunk, n - c0)
+        t = make_transmissions(m, seed0 + c0, device, N, A, chunk=m, i0_range=i0_range, gpu=gpu)
+        if keep_trans:
+            trans[c0:c0 + m] = t
+        fbp_input(t, ang, gpu, out=inputs[c0:c0 + m])
+        labels[c0:c0 + m] = em_label(t, em_iters, gpu)
     torch.cuda.synchronize(device)
     return inputs, labels, trans, ang
 
@@ -426,3 +499,178 @@ def evaluate(net, inputs, trans, ang, plain_iters=100, max_warm_iters=100, tol=0
             "residual_plain100_median": float(np.median(res_plain[plain_iters])),
             "residual_start_warm_median": float(np.median(res_warm[0])),
             "residual_start_plain_median": float(np.median(res_plain[0]))}
+
+
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _em_timed(obj, trans, ang, iters, gpu=0):
+    """`iters` tEM iterations in place (no metrics, graph-captured loop), device ms."""
+    import torch
+    n, A, N = trans.shape
+    flat = torch.ones((n, N), dtype=torch.float32, device=trans.device)
+    st = ctypes.c_void_p(torch.cuda.current_stream(trans.device).cuda_stream)
+    e0, e1 = _events()
+    e0.record()
+    rc = 0
+    if iters > 0:
+        rc = libraft.raft_em_device(0, gpu, _p(obj), _p(trans), _p(flat), _ptr(np.ascontiguousarray(ang)), N, A, n,
+                                    iters, None, 1, st)
+    e1.record()
+    if rc:
+        check_error("tem")
+    torch.cuda.synchronize(trans.device)
+    return e0.elapsed_time(e1)
+
+
+def _first_within(res, target, cap):
+    """Per slice: first iterate index whose residual is <= target (cap + 1 if none)."""
+    ok = res <= target[None, :]
+    return np.where(ok.any(0), ok.argmax(0), cap + 1)
+
+
+def fbp_start(x):
+    """The FBP image itself as an EM start (ablation without the network):
+    clamped to the same positive floor predict() uses."""
+    import torch
+    floor = 1e-3 * torch.clamp(x.abs().mean(dim=(1, 2)), min=1e-12)
+    return torch.maximum(x, floor[:, None, None])
+
+
+def evaluate_wall(net, trans, ang, plain_iters=100, tol=0.01, max_iters=100, gpu=0, batch=16):
+    """Wall time to the plain-EM data residual, learned start vs plain EM.
+
+    For every held-out slice the target is r* = (1 + tol) x the data residual
+    ||exp(-A x_k) - y|| / ||y|| of plain tEM after `plain_iters` iterations
+    from the uniform start.  Iteration counts come from FP64-metric runs;
+    the times are separate device-timed runs of the same work without
+    metrics, all slices batched as EM runs them:
+      plain   = `plain_iters` EM iterations from the uniform start;
+      learned = FBP of the data + U-Net inference + k EM iterations, k = the
+                largest per-slice count the warm start needs to reach r*;
+      fbp     = FBP + k' EM iterations from the clamped FBP image (the
+                method without the network, reported beside it)."""
+    import torch
+    n, A, N = trans.shape
+    dev = trans.device
+    # iteration counts (metric runs)
+    res_plain, _ = em_residuals(torch.ones((n, N, N), device=dev), trans, ang, plain_iters + 1, gpu)
+    target = res_plain[plain_iters] * (1.0 + tol)
+    x = fbp_input(trans, ang, gpu)
+    warm = net.predict(x, batch=batch)
+    res_warm, _ = em_residuals(warm.clone(), trans, ang, max_iters + 1, gpu)
+    res_fbp, _ = em_residuals(fbp_start(x), trans, ang, max_iters + 1, gpu)
+    k_warm = _first_within(res_warm, target, max_iters)
+    k_fbp = _first_within(res_fbp, target, max_iters)
+    kw, kf = int(k_warm.max()), int(k_fbp.max())
+    # wall times (no metrics): warm-up once, then time
+    for _ in range(2):
+        t_plain = _em_timed(torch.ones((n, N, N), device=dev), trans, ang, plain_iters, gpu)
+    for _ in range(2):
+        e0, e1 = _events()
+        e0.record()
+        x = fbp_input(trans, ang, gpu)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        t_fbp = e0.elapsed_time(e1)
+        e0.record()
+        warm = net.predict(x, batch=batch)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        t_net = e0.elapsed_time(e1)
+        t_em_w = _em_timed(warm, trans, ang, min(kw, max_iters), gpu)
+        t_em_f = _em_timed(fbp_start(x), trans, ang, min(kf, max_iters), gpu)
+    t_learned = t_fbp + t_net + t_em_w
+    t_fbponly = t_fbp + t_em_f
+    return {"samples": n, "plain_iterations": plain_iters, "tol": tol,
+            "residual_plain_median": float(np.median(res_plain[plain_iters])),
+            "residual_start_uniform_median": float(np.median(res_plain[0])),
+            "residual_start_learned_median": float(np.median(res_warm[0])),
+            "residual_start_fbp_median": float(np.median(res_fbp[0])),
+            "learned_iterations_median": float(np.median(k_warm)), "learned_iterations_max": kw,
+            "learned_reached_fraction": float((k_warm <= max_iters).mean()),
+            "fbp_iterations_median": float(np.median(k_fbp)), "fbp_iterations_max": kf,
+            "fbp_reached_fraction": float((k_fbp <= max_iters).mean()),
+            "ms_plain": t_plain, "ms_fbp": t_fbp, "ms_unet": t_net, "ms_em_learned": t_em_w,
+            "ms_learned": t_learned, "ms_fbp_start": t_fbponly,
+            "speedup_learned_vs_plain": t_plain / t_learned, "speedup_fbp_start_vs_plain": t_plain / t_fbponly,
+            "all_reached": bool((k_warm <= max_iters).all())}
+
+
+TRAIN_SEED0 = 100_000       # training phantoms: seeds 100000 + i
+HELDOUT_SEED0 = 900_000     # evaluation phantoms: seeds 900000 + i (disjoint)
+
+
+def default_weights():
+    import os
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "unet_tem_512x720.npz")
+
+
+def train_recipe(pairs=20000, epochs=3, batch=16, lr=1e-3, N=512, A=720, em_iters=200, val=64, chunk=256,
+                 seed=0, device=None, log=print):
+    """The training recipe of the shipped weights: `pairs` (FBP, em_iters-tEM)
+    pairs from seeds TRAIN_SEED0 + i, Adam with cosine decay; validation MSE
+    (network vs FBP input, both against the label) on `val` held-out pairs."""
+    import torch
+    dev = device or torch.device("cuda", 0)
+    t0 = time.time()
+    inputs, labels, _, _ = make_pairs(pairs, TRAIN_SEED0, dev, N=N, A=A, em_iters=em_iters, chunk=chunk,
+                                      keep_trans=False)
+    vx, vy, _, _ = make_pairs(val, HELDOUT_SEED0 + 500_000, dev, N=N, A=A, em_iters=em_iters, chunk=val,
+                              keep_trans=False)
+    log(f"pairs: {pairs} + {val} in {time.time() - t0:.1f} s")
+    net = UNet(dev, seed=seed)
+
+    def val_mse():
+        sc = input_scale(vx)
+        out = torch.cat([net.forward(vx[i:i + batch].contiguous(), sc[i:i + batch]) for i in range(0, val, batch)])
+        return (float(((out - vy * sc[:, None, None]) ** 2).mean()),
+                float((((vx - vy) * sc[:, None, None]) ** 2).mean()))
+    log(f"val mse before: net {val_mse()[0]:.4g}, fbp input {val_mse()[1]:.4g}")
+    t0 = time.time()
+    losses = train(net, inputs, labels, epochs=epochs, batch=batch, lr=lr, log=log)
+    torch.cuda.synchronize(dev)
+    log(f"trained {len(losses)} steps in {time.time() - t0:.1f} s; val mse net {val_mse()[0]:.4g}")
+    meta = {"pairs": pairs, "epochs": epochs, "batch": batch, "lr": lr, "N": N, "A": A, "em_iters": em_iters,
+            "train_seed0": TRAIN_SEED0, "init_seed": seed, "final_train_loss": float(np.mean(losses[-50:])),
+            "val_mse": val_mse()[0], "val_mse_fbp_input": val_mse()[1]}
+    del inputs, labels
+    return net, meta
+
+
+def main(argv=None):
+    import argparse
+    import json
+    import torch
+    ap = argparse.ArgumentParser(description="train / evaluate the tEM warm-start U-Net")
+    ap.add_argument("cmd", choices=["train", "evaluate"])
+    ap.add_argument("--pairs", type=int, default=20000)
+    ap.add_argument("--epochs", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--em-iters", type=int, default=200)
+    ap.add_argument("--chunk", type=int, default=256)
+    ap.add_argument("--samples", type=int, default=256)
+    ap.add_argument("--weights", default=default_weights())
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    dev = torch.device("cuda", 0)
+    if a.cmd == "train":
+        net, meta = train_recipe(a.pairs, a.epochs, a.batch, a.lr, em_iters=a.em_iters, chunk=a.chunk, device=dev,
+                                 log=lambda m: print(m, flush=True))
+        net.save(a.out or a.weights, **meta)
+        print(json.dumps(meta), flush=True)
+    else:
+        net = UNet.from_file(a.weights, dev)
+        trans = torch.empty((a.samples, 720, 512), dtype=torch.float32, device=dev)
+        for c0 in range(0, a.samples, 64):
+            m = min(64, a.samples - c0)
+            make_transmissions(m, HELDOUT_SEED0 + c0, dev, chunk=m, out=trans[c0:c0 + m])
+        r = evaluate_wall(net, trans, S.uniform_angles(720))
+        print(json.dumps(r), flush=True)
+
+
+if __name__ == "__main__":
+    main()
