@@ -177,6 +177,28 @@ def run_tem(local, dev, nslices=EM_SLICES, iters=EM_ITERS, warm_iters=3):
             "metrics": "FP64 data residual ||flat*exp(-Ax)-y||/||y|| and Poisson NLL per iteration"}
 
 
+# ------------------------------------------------------- learned warm start --
+def run_warm(dev, samples=256):
+    """Learned warm start for tEM at 512^2 x 720 angles: the shipped U-Net
+    (trained on 20k (FBP, 200-iteration tEM) pairs) on `samples` held-out
+    seeds; wall time to the plain-EM-100 data residual (+1%), learned start
+    vs plain EM from the uniform start, with the FBP-only start beside it."""
+    import torch
+    from sscRaft import synthetic as S
+    from sscRaft import warmstart as W
+    net = W.UNet.from_file(W.default_weights(), dev)
+    trans = torch.empty((samples, 720, 512), dtype=torch.float32, device=dev)
+    for c0 in range(0, samples, 64):
+        m = min(64, samples - c0)
+        W.make_transmissions(m, W.HELDOUT_SEED0 + c0, dev, chunk=m, out=trans[c0:c0 + m])
+    r = W.evaluate_wall(net, trans, S.uniform_angles(720))
+    r["workload"] = (f"tEM warm start: {samples} held-out 512^2 ellipse+Perlin phantoms (seeds "
+                     f"{W.HELDOUT_SEED0}+i), 720 angles, I0 ~ U[1e3,1e5]; target = plain EM-100 residual +1%")
+    r["weights"] = os.path.relpath(W.default_weights(), REPO)
+    r["unet_params"] = net.n_params()
+    return r
+
+
 # ----------------------------------------------------------- ragged batch --
 def run_ragged(dev, nreq=96, seed=5_000_000, em_iters=30):
     """96 requests, side log-uniform in [256, 2048], angles U[180, 1800], bins =
@@ -453,6 +475,7 @@ def run_ours(args):
 
     em_result = None if args.no_em else run_tem(local, dev)
     ragged_result = None if args.no_ragged else run_ragged(dev)
+    warm_result = None if args.no_warm else run_warm(dev)
 
     if rank == 0:
         value = ws * nsl / (ms_dev / 1e3)
@@ -492,6 +515,7 @@ def run_ours(args):
             "autotune": autotune_table(),
             "em": em_result,
             "ragged": ragged_result,
+            "warm_start": warm_result,
             "clocks": clocks,
             "gpu_launches": int(launches),
         }
@@ -571,6 +595,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-em", action="store_true")
     ap.add_argument("--no-ragged", action="store_true")
+    ap.add_argument("--no-warm", action="store_true")
     ap.add_argument("--quick", action="store_true", help="device timing of one operator only (profiling)")
     ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "tem", "ragged"])
     args = ap.parse_args()

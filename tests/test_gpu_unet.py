@@ -140,3 +140,25 @@ def test_training_reduces_loss_and_warm_start_helps():
     # and reaches the plain-EM target residual in fewer iterations
     assert r["residual_start_warm_median"] < r["residual_start_plain_median"]
     assert r["warm_iterations_median"] < r["plain_iterations"]
+
+
+def test_shipped_weights_reach_plain_em100_residual():
+    """The shipped network (512^2 x 720 angles) on held-out seeds: its start
+    is within 1% of the plain 100-iteration EM residual after at most two EM
+    iterations, and FBP + U-Net + those iterations take at least 4x less
+    device time than plain EM-100."""
+    import os
+    import torch
+    from sscRaft import synthetic as S
+    from sscRaft import warmstart as ws
+    dev = torch.device("cuda", 0)
+    assert os.path.exists(ws.default_weights())
+    net = ws.UNet.from_file(ws.default_weights(), dev)
+    assert 1.9e6 < net.n_params() < 2.1e6
+    n = 16
+    trans = torch.empty((n, 720, 512), dtype=torch.float32, device=dev)
+    ws.make_transmissions(n, ws.HELDOUT_SEED0 + 1000, dev, chunk=n, out=trans)
+    r = ws.evaluate_wall(net, trans, S.uniform_angles(720), max_iters=20)
+    assert r["all_reached"] and r["learned_iterations_max"] <= 2, r
+    assert r["residual_start_learned_median"] < r["residual_start_fbp_median"], r
+    assert r["speedup_learned_vs_plain"] >= 4.0, r
