@@ -523,11 +523,9 @@ int raft_radon_device(int gpu, float *d_out, const float *d_phantom, const float
         cudaStream_t st = resolve_stream(ds, stream, ds.s_comp);
         float *d_ang = (float *)ds.angles.get(sizeof(float) * nangles);
         RAFT_CUDA(cudaMemcpyAsync(d_ang, angles, sizeof(float) * nangles, cudaMemcpyHostToDevice, st));
-        float *imgT = (float *)ds.imgT.get(sizeof(float) * (size_t)nx * ny * std::max(1, nslices));
-        launch_transpose(d_phantom, imgT, nx, ny, nslices, st);
+        void *scratch = ds.imgT.get(proj_scratch_bytes(nx, ny, nslices));
         ProjLaunch pl;
         pl.img = d_phantom;
-        pl.imgT = imgT;
         pl.out = d_out;
         pl.angles = d_ang;
         pl.nx = nx;
@@ -537,6 +535,7 @@ int raft_radon_device(int gpu, float *d_out, const float *d_phantom, const float
         pl.nslices = nslices;
         pl.ax = ax;
         pl.ay = ay;
+        stage_proj_images(pl, scratch, st);
         launch_project(pl, st);
         if (!stream) RAFT_CUDA(cudaStreamSynchronize(st));
     } catch (const CudaFail &) {

@@ -99,16 +99,16 @@ __device__ __forceinline__ void angle_param(const BpArgs &p, int a, int x0, int 
             for (int cx = 0; cx < 2; cx++) {
                 const int i = x0 + cx * (BP_TX - 1), j = y0 + cy * (BP_TY - 1);
                 int ti;
+                // the same expressions as the per-pixel index in bp_tile
                 if constexpr (GEOM == GEOM_FBP_REF) {
-                    const int ip = i + p.offo, jp = j + p.offo;
-                    float x = p.xmin + ip * p.dx;
-                    float y = p.ymin + jp * p.dy;
-                    float t = x * c - y * s;
+                    const float x = __fmaf_rn((float)(i + p.offo), p.dx, p.xmin);
+                    const float y = __fmaf_rn((float)(j + p.offo), p.dy, p.ymin);
+                    const float t = __fmaf_rn(x, c, -__fmul_rn(y, s));
                     ti = (int)((t - p.tmin) / p.dt);
                 } else {
-                    float x = p.xymin + i * p.dxy;
-                    float y = p.xymin + j * p.dxy;
-                    float t = x * c + y * s;
+                    const float x = __fmaf_rn((float)i, p.dxy, p.xymin);
+                    const float y = __fmaf_rn((float)j, p.dxy, p.xymin);
+                    const float t = __fmaf_rn(x, c, __fmul_rn(y, s));
                     ti = (int)((t - p.tmin) / p.dt);
                 }
                 tmin_i = min(tmin_i, ti);
@@ -223,14 +223,14 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &p, const int AB, const int
     float xr[4], yr[2];
     if constexpr (GEOM == GEOM_FBP_REF) {
 #pragma unroll
-        for (int i = 0; i < 4; i++) { const int ip = x0 + li[i] + p.offo; xr[i] = p.xmin + ip * p.dx; }
+        for (int i = 0; i < 4; i++) xr[i] = __fmaf_rn((float)(x0 + li[i] + p.offo), p.dx, p.xmin);
 #pragma unroll
-        for (int j = 0; j < 2; j++) { const int jp = y0 + lj[j] + p.offo; yr[j] = p.ymin + jp * p.dy; }
+        for (int j = 0; j < 2; j++) yr[j] = __fmaf_rn((float)(y0 + lj[j] + p.offo), p.dy, p.ymin);
     } else if constexpr (GEOM == GEOM_EM_REF) {
 #pragma unroll
-        for (int i = 0; i < 4; i++) { const int ip = x0 + li[i]; xr[i] = p.xymin + ip * p.dxy; }
+        for (int i = 0; i < 4; i++) xr[i] = __fmaf_rn((float)(x0 + li[i]), p.dxy, p.xymin);
 #pragma unroll
-        for (int j = 0; j < 2; j++) { const int jp = y0 + lj[j]; yr[j] = p.xymin + jp * p.dxy; }
+        for (int j = 0; j < 2; j++) yr[j] = __fmaf_rn((float)(y0 + lj[j]), p.dxy, p.xymin);
     } else {
 #pragma unroll
         for (int i = 0; i < 4; i++) xr[i] = (float)li[i];
@@ -272,18 +272,20 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &p, const int AB, const int
                 const float c = ap.a, sn = ap.b;
                 const int wbase = ap.d;
 #pragma unroll
-                for (int j = 0; j < 2; j++)
+                for (int j = 0; j < 2; j++) {
+                    // FBP: t = x*cos - y*sin, EM: t = x*cos + y*sin, each one fmaf
+                    // with y*sin rounded first (the reference build's contraction)
+                    const float ys = (GEOM == GEOM_FBP_REF) ? -__fmul_rn(yr[j], sn) : __fmul_rn(yr[j], sn);
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
-                        float t;
-                        if constexpr (GEOM == GEOM_FBP_REF) t = xr[i] * c - yr[j] * sn;
-                        else t = xr[i] * c + yr[j] * sn;
+                        const float t = __fmaf_rn(xr[i], c, ys);
                         int ti = (int)((t - p.tmin) / p.dt);
                         const unsigned k = min((unsigned)(ti - wbase), (unsigned)(W - 1));
                         const float *wk = reinterpret_cast<const float *>(w) + k;
 #pragma unroll
                         for (int q = 0; q < S; q++) acc[q][j][i] += wk[q * W];
                     }
+                }
             }
         }
         if (!__syncthreads_and(got)) {
@@ -318,8 +320,7 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &p, const int AB, const int
 
 
 template <int GEOM, int STORE, int S>
-__global__ void __launch_bounds__(BP_THREADS)
-bp_kernel(const BpArgs p, const int AB)
+__device__ __forceinline__ void bp_body(const BpArgs &p, const int AB)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
@@ -331,6 +332,20 @@ bp_kernel(const BpArgs p, const int AB)
     __syncthreads();
     uint32_t gstage = 0;
     bp_tile<GEOM, STORE, S>(p, AB, blockIdx.x * BP_TX, blockIdx.y * BP_TY, blockIdx.z * S, smem, gstage);
+}
+
+template <int GEOM, int STORE, int S>
+__global__ void __launch_bounds__(BP_THREADS) bp_kernel(const BpArgs p, const int AB)
+{
+    bp_body<GEOM, STORE, S>(p, AB);
+}
+
+// The S = 4 instance, held to 80 registers so that three CTAs fit an SM
+// (its shared memory allows three).
+template <int GEOM, int STORE>
+__global__ void __launch_bounds__(BP_THREADS, 3) bp_kernel_s4(const BpArgs p, const int AB)
+{
+    bp_body<GEOM, STORE, 4>(p, AB);
 }
 
 // ------------------------------------------------------------------------
@@ -490,14 +505,16 @@ static void launch_bp_s(const BpArgs &a, int AB, cudaStream_t st)
     static thread_local int configured = -1;
     int dev = 0;
     cudaGetDevice(&dev);
+    void (*kern)(const BpArgs, const int);
+    if constexpr (S == 4) kern = bp_kernel_s4<GEOM, STORE>;
+    else kern = bp_kernel<GEOM, STORE, S>;
     if (configured != dev) {
-        RAFT_CUDA(cudaFuncSetAttribute(bp_kernel<GEOM, STORE, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kBpSmemMax));
+        RAFT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBpSmemMax));
         configured = dev;
     }
     dim3 grid((a.No + BP_TX - 1) / BP_TX, (a.No + BP_TY - 1) / BP_TY, (a.nslices + S - 1) / S);
     ProfScope ps(PROF_BACKPROJECT, st);
-    bp_kernel<GEOM, STORE, S><<<grid, BP_THREADS, smem, st>>>(a, AB);
+    kern<<<grid, BP_THREADS, smem, st>>>(a, AB);
     RAFT_CUDA(cudaGetLastError());
 }
 

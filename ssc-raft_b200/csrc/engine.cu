@@ -386,12 +386,10 @@ void radon_host_slab(int device, float *proj, const float *img, const float *ang
     const size_t in_ps = (size_t)nx * ny * sizeof(float);
     const size_t out_ps = (size_t)nangles * nrays * sizeof(float);
     const int chunk = auto_chunk(nslices, std::max(in_ps, out_ps), 0);
-    float *imgT = (float *)ds.imgT.get(in_ps * chunk);
+    void *scratch = ds.imgT.get(proj_scratch_bytes(nx, ny, chunk));
     run_pipeline(ds, nslices, chunk, in_ps, out_ps, img, proj, [&](void *din, void *dout, int ns, cudaStream_t st) {
-        launch_transpose((const float *)din, imgT, nx, ny, ns, st);
         ProjLaunch pl;
         pl.img = (const float *)din;
-        pl.imgT = imgT;
         pl.out = (float *)dout;
         pl.angles = d_ang;
         pl.nx = nx;
@@ -402,6 +400,7 @@ void radon_host_slab(int device, float *proj, const float *img, const float *ang
         pl.ax = ax;
         pl.ay = ay;
         pl.em = 0;
+        stage_proj_images(pl, scratch, st);
         launch_project(pl, st);
     });
 }
@@ -466,10 +465,9 @@ void em_chunk(DeviceState &ds, const EmPrepared &ep, int kind, const float *d_da
     bl.den = nullptr;
     launch_backproject(bl, st);
 
-    float *imgT = (float *)ds.imgT.get((size_t)nslices * N * N * sizeof(float));
+    void *scratch = ds.imgT.get(proj_scratch_bytes(N, N, nslices));
     ProjLaunch pl;
     pl.img = d_obj;
-    pl.imgT = imgT;
     pl.out = rows;
     pl.angles = d_ang;
     pl.nx = N;
@@ -495,7 +493,7 @@ void em_chunk(DeviceState &ds, const EmPrepared &ep, int kind, const float *d_da
     auto body = [&]() {
         for (int it = 0; it < c.niter; it++) {
             pl.metrics = d_metrics ? d_metrics + (size_t)it * nslices * 3 : nullptr;
-            launch_transpose(d_obj, imgT, N, N, nslices, st);
+            stage_proj_images(pl, scratch, st);
             launch_project(pl, st);
             launch_backproject(bl, st);
         }

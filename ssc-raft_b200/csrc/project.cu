@@ -16,7 +16,11 @@
 //
 // The sample positions and indices are computed with the reference's FP32
 // expressions (this file is compiled with fast math, as the reference is),
-// so the nearest-pixel choice is the reference's.
+// so the nearest-pixel choice is the reference's.  The multiply-adds are
+// written out (t = i*d - a, x = t*c - s*sin, y = t*sin + s*c as single-rounding
+// fmaf with the product s*sin / s*c rounded first -- the contraction the
+// reference build produces) so that no template instance can contract them
+// differently.
 #include "raft.hpp"
 #include "profile.hpp"
 
@@ -36,10 +40,13 @@ __device__ __forceinline__ double warp_sum(double v)
 // geometry is the same for all slices).  Warps whose angle is steeper than
 // 45 degrees read a transposed copy of the images (imgT[x][y]) so that the
 // 32 rays of the warp touch consecutive addresses; the index arithmetic and
-// therefore the chosen pixels are unchanged.
-template <int EM, int EPI, int S>
+// therefore the chosen pixels are unchanged.  IL = 1 (S = 8) reads the
+// slice-interleaved copies instead (il[g][y][x][8], ilT[g][x][y][8]): one
+// sample's eight slice values are two 16-byte loads from one 32-byte sector.
+template <int EM, int EPI, int S, int IL>
 __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx, const int by, const int bz)
 {
+    static_assert(!IL || S == 8, "interleaved images hold groups of 8 slices");
     const int i = bx * PJ_RAYS + threadIdx.x;     // ray
     const int j = by * PJ_ANGLES + threadIdx.y;   // angle
     const int k0 = bz * S;                        // first slice
@@ -54,8 +61,9 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
         const float ang = p.angles[j];
         const float ctheta = __cosf(ang);
         const float stheta = __sinf(ang);
-        const bool steep = p.imgT && fabsf(stheta) > fabsf(ctheta);
-        const float *img = (steep ? p.imgT : p.img) + (size_t)k0 * plane;
+        const bool steep = (IL ? p.ilT : p.imgT) && fabsf(stheta) > fabsf(ctheta);
+        const float *img = IL ? (steep ? p.ilT : p.il) + (size_t)bz * plane * 8
+                              : (steep ? p.imgT : p.img) + (size_t)k0 * plane;
         // address = Y*nx + X (row-major) or X*ny + Y (transposed)
         const int sy = steep ? 1 : nx, sx = steep ? ny : 1;
         float linesum[S];
@@ -71,15 +79,25 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
                 float v[4][S];
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
-                    const float s = -ay0 + (m + u) * d0;
-                    const float x = t * ctheta - s * stheta;
-                    const float y = t * stheta + s * ctheta;
+                    const float s = __fmaf_rn((float)(m + u), d0, -ay0);
+                    const float x = __fmaf_rn(t, ctheta, -__fmul_rn(s, stheta));
+                    const float y = __fmaf_rn(t, stheta, __fmul_rn(s, ctheta));
                     const int X = (int)((x + 1) / ddx);
                     const int Y = (int)((y + 1) / ddy);
                     const bool in = (X >= 0) & (X < limx) & (Y >= 0) & (Y < limy);
-                    const float *pix = img + (size_t)(in ? Y : 0) * sy + (size_t)(in ? X : 0) * sx;
+                    const size_t off = (size_t)(in ? Y : 0) * sy + (size_t)(in ? X : 0) * sx;
+                    if constexpr (IL) {
+                        const float4 *px = reinterpret_cast<const float4 *>(img + off * 8);
+                        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+                        const float4 lo = in ? __ldg(px) : zero;
+                        const float4 hi = in ? __ldg(px + 1) : zero;
+                        v[u][0] = lo.x; v[u][1] = lo.y; v[u][2] = lo.z; v[u][3] = lo.w;
+                        v[u][4] = hi.x; v[u][5] = hi.y; v[u][6] = hi.z; v[u][7] = hi.w;
+                    } else {
+                        const float *pix = img + off;
 #pragma unroll
-                    for (int q = 0; q < S; q++) v[u][q] = (in && q < nsl) ? __ldg(pix + q * plane) : 0.f;
+                        for (int q = 0; q < S; q++) v[u][q] = (in && q < nsl) ? __ldg(pix + q * plane) : 0.f;
+                    }
                 }
 #pragma unroll
                 for (int u = 0; u < 4; u++)
@@ -87,16 +105,25 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
                     for (int q = 0; q < S; q++) linesum[q] += v[u][q];
             }
             for (; m < nsamp; m++) {
-                const float s = -ay0 + m * d0;
-                const float x = t * ctheta - s * stheta;
-                const float y = t * stheta + s * ctheta;
+                const float s = __fmaf_rn((float)m, d0, -ay0);
+                const float x = __fmaf_rn(t, ctheta, -__fmul_rn(s, stheta));
+                const float y = __fmaf_rn(t, stheta, __fmul_rn(s, ctheta));
                 const int X = (int)((x + 1) / ddx);
                 const int Y = (int)((y + 1) / ddy);
                 if ((X >= 0) & (X < limx) & (Y >= 0) & (Y < limy)) {
-                    const float *pix = img + (size_t)Y * sy + (size_t)X * sx;
+                    const size_t off = (size_t)Y * sy + (size_t)X * sx;
+                    if constexpr (IL) {
+                        const float4 *px = reinterpret_cast<const float4 *>(img + off * 8);
+                        const float4 lo = __ldg(px), hi = __ldg(px + 1);
+                        const float w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
 #pragma unroll
-                    for (int q = 0; q < S; q++)
-                        if (q < nsl) linesum[q] += __ldg(pix + q * plane);
+                        for (int q = 0; q < S; q++) linesum[q] += w[q];
+                    } else {
+                        const float *pix = img + off;
+#pragma unroll
+                        for (int q = 0; q < S; q++)
+                            if (q < nsl) linesum[q] += __ldg(pix + q * plane);
+                    }
                 }
             }
         };
@@ -105,14 +132,14 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
             // rays, samples and pixels; the image is N x N with N = nx
             const float a = p.ax;
             const float dt = (float)(2.0 * a / (p.nrays - 1));
-            const float t = -a + i * dt;
+            const float t = __fmaf_rn((float)i, dt, -a);
             sample_loop(t, dt, a, dt, dt, p.nrays, nx, nx);
 #pragma unroll
             for (int q = 0; q < S; q++) value[q] = linesum[q] * dt;
         } else {
             const float dx = 2.0f * p.ax / (float)(unsigned)(nx - 1);
             const float dy = 2.0f * p.ay / (float)(unsigned)(ny - 1);
-            const float t = -p.ax + i * dx;
+            const float t = __fmaf_rn((float)i, dx, -p.ax);
             sample_loop(t, dy, p.ay, dx, dy, ny, nx, ny);
 #pragma unroll
             for (int q = 0; q < S; q++) value[q] = linesum[q] * dy;
@@ -186,11 +213,11 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
     }
 }
 
-template <int EM, int EPI, int S>
+template <int EM, int EPI, int S, int IL>
 __global__ void __launch_bounds__(PJ_RAYS * PJ_ANGLES)
 project_kernel(const ProjLaunch p)
 {
-    project_block<EM, EPI, S>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    project_block<EM, EPI, S, IL>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Ragged projector: one launch over many single-slice requests of different
@@ -214,7 +241,7 @@ project_ragged_kernel(const ProjLaunch *__restrict__ reqs, const int *__restrict
     const ProjLaunch &p = reqs[r];
     const int local = blockIdx.x - blk_start[r];
     const int nbx = (p.nrays + PJ_RAYS - 1) / PJ_RAYS;
-    project_block<EM, EPI, 1>(p, local % nbx, local / nbx, 0);
+    project_block<EM, EPI, 1, 0>(p, local % nbx, local / nbx, 0);
 }
 
 void launch_project_ragged(const ProjLaunch *d_reqs, const int *d_blk_start, int nreq, int total_blocks, int em,
@@ -258,6 +285,77 @@ void launch_transpose(const float *in, float *out, int nx, int ny, int nslices, 
     RAFT_CUDA(cudaGetLastError());
 }
 
+// Slice-interleaved copies of groups of 8 planes, row-major and transposed:
+// il[g][y][x][s] = ilT[g][x][y][s] = in[8g + s][y][x] (zero where 8g + s is
+// past the last plane).  One 32 x 32 pixel tile of all 8 planes per block.
+__global__ void __launch_bounds__(256)
+interleave_kernel(const float *__restrict__ in, float *__restrict__ il, float *__restrict__ ilT, int nx, int ny,
+                  int nslices)
+{
+    __shared__ float tile[8][32][33];
+    const size_t plane = (size_t)nx * ny;
+    const int g = blockIdx.z, tx = threadIdx.x;
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+#pragma unroll
+    for (int s = 0; s < 8; s++) {
+        const int k = g * 8 + s;
+        for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+            const int y = by + r, x = bx + tx;
+            tile[s][r][tx] = (k < nslices && x < nx && y < ny) ? in[(size_t)k * plane + (size_t)y * nx + x] : 0.f;
+        }
+    }
+    __syncthreads();
+    float *o = il + (size_t)g * plane * 8;
+    float *oT = ilT + (size_t)g * plane * 8;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        int y = by + r, x = bx + tx;
+        if (x < nx && y < ny) {
+            float4 *d = reinterpret_cast<float4 *>(o + ((size_t)y * nx + x) * 8);
+            d[0] = make_float4(tile[0][r][tx], tile[1][r][tx], tile[2][r][tx], tile[3][r][tx]);
+            d[1] = make_float4(tile[4][r][tx], tile[5][r][tx], tile[6][r][tx], tile[7][r][tx]);
+        }
+        x = bx + r;
+        y = by + tx;
+        if (x < nx && y < ny) {
+            float4 *d = reinterpret_cast<float4 *>(oT + ((size_t)x * ny + y) * 8);
+            d[0] = make_float4(tile[0][tx][r], tile[1][tx][r], tile[2][tx][r], tile[3][tx][r]);
+            d[1] = make_float4(tile[4][tx][r], tile[5][tx][r], tile[6][tx][r], tile[7][tx][r]);
+        }
+    }
+}
+
+static bool use_interleaved(int nslices) { return nslices >= 8; }
+
+size_t proj_scratch_bytes(int nx, int ny, int nslices)
+{
+    const size_t plane = (size_t)nx * ny * sizeof(float);
+    if (nslices <= 0) return 16;
+    if (use_interleaved(nslices)) return 2 * (size_t)((nslices + 7) / 8) * 8 * plane;
+    return (size_t)nslices * plane;
+}
+
+void stage_proj_images(ProjLaunch &pl, void *scratch, cudaStream_t st)
+{
+    if (pl.nslices <= 0) return;
+    if (use_interleaved(pl.nslices)) {
+        const int G = (pl.nslices + 7) / 8;
+        float *il = (float *)scratch;
+        float *ilT = il + (size_t)G * 8 * pl.nx * pl.ny;
+        count_launch();
+        dim3 grid((pl.nx + 31) / 32, (pl.ny + 31) / 32, G);
+        interleave_kernel<<<grid, dim3(32, 8), 0, st>>>(pl.img, il, ilT, pl.nx, pl.ny, pl.nslices);
+        RAFT_CUDA(cudaGetLastError());
+        pl.il = il;
+        pl.ilT = ilT;
+        pl.imgT = nullptr;
+    } else {
+        float *t = (float *)scratch;
+        launch_transpose(pl.img, t, pl.nx, pl.ny, pl.nslices, st);
+        pl.imgT = t;
+        pl.il = pl.ilT = nullptr;
+    }
+}
+
 template <int EM, int EPI>
 static void launch_project_s(const ProjLaunch &pl, int S, cudaStream_t st)
 {
@@ -265,16 +363,18 @@ static void launch_project_s(const ProjLaunch &pl, int S, cudaStream_t st)
     dim3 grid((pl.nrays + PJ_RAYS - 1) / PJ_RAYS, (pl.nangles + PJ_ANGLES - 1) / PJ_ANGLES,
               (pl.nslices + S - 1) / S);
     ProfScope ps(PROF_PROJECT, st);
-    if (S == 4) project_kernel<EM, EPI, 4><<<grid, block, 0, st>>>(pl);
-    else if (S == 2) project_kernel<EM, EPI, 2><<<grid, block, 0, st>>>(pl);
-    else project_kernel<EM, EPI, 1><<<grid, block, 0, st>>>(pl);
+    if (S == 8) project_kernel<EM, EPI, 8, 1><<<grid, block, 0, st>>>(pl);
+    else if (S == 4) project_kernel<EM, EPI, 4, 0><<<grid, block, 0, st>>>(pl);
+    else if (S == 2) project_kernel<EM, EPI, 2, 0><<<grid, block, 0, st>>>(pl);
+    else project_kernel<EM, EPI, 1, 0><<<grid, block, 0, st>>>(pl);
     RAFT_CUDA(cudaGetLastError());
 }
 
 void launch_project(const ProjLaunch &pl, cudaStream_t st)
 {
     if (pl.nslices <= 0 || pl.nangles <= 0 || pl.nrays <= 0) return;
-    const int S = pl.nslices >= 4 ? 4 : (pl.nslices >= 2 ? 2 : 1);
+    RAFT_CHECK((pl.il == nullptr) == (pl.ilT == nullptr), "projector: interleaved copies come in pairs");
+    const int S = pl.il ? 8 : (pl.nslices >= 4 ? 4 : (pl.nslices >= 2 ? 2 : 1));
     if (!pl.em) {
         launch_project_s<0, 0>(pl, S, st);
     } else {

@@ -184,6 +184,8 @@ void launch_angle_tables(const float *d_angles, int nangles, float *d_cos, float
 struct ProjLaunch {
     const float *img = nullptr;     // [nslices][ny][nx]
     const float *imgT = nullptr;    // optional transposed copy [nslices][nx][ny] for steep angles
+    const float *il = nullptr;      // optional slice-interleaved copies (groups of 8 planes):
+    const float *ilT = nullptr;     //   il [G][ny][nx][8], ilT [G][nx][ny][8]; used instead of img/imgT
     float *out = nullptr;           // plain [nslices][nangles][nrays] or window rows
     const float *angles = nullptr;
     int nx = 0, ny = 0, nrays = 0, nangles = 0, nslices = 0;
@@ -206,6 +208,13 @@ void launch_project_ragged(const ProjLaunch *d_reqs, const int *d_blk_start, int
 
 // out[k][x][y] = in[k][y][x] for each of nslices planes.
 void launch_transpose(const float *in, float *out, int nx, int ny, int nslices, cudaStream_t st);
+
+// Scratch bytes the projector's re-laid-out images need for nslices planes.
+size_t proj_scratch_bytes(int nx, int ny, int nslices);
+// Write the re-laid-out copies of pl.img into `scratch` (proj_scratch_bytes):
+// slice-interleaved groups of 8 (pl.il / pl.ilT) when there are 8 or more
+// planes, else a transposed copy (pl.imgT).  Issued on st.
+void stage_proj_images(ProjLaunch &pl, void *scratch, cudaStream_t st);
 
 // Copy a plain sinogram into weighted window rows (EM: BP of the counts).
 void launch_to_window(const float *sino, float *rows, const float *wt, int nrows, int nangles,

@@ -115,3 +115,45 @@ def test_em_graph_equals_stream_and_metrics(oracle):
         np.testing.assert_allclose(got_res, res, rtol=2e-3)
         np.testing.assert_allclose(ma[k, :, 2], nll, rtol=1e-5)
         x = oracle.tem(counts, flat, ang, 1, obj=x, fwd_trig=F(ang), bp_trig=B(ang))
+
+
+def test_interleaved_projector_bit_identical():
+    """8 or more slices run the projector on slice-interleaved copies (groups of
+    8, a partial last group zero-filled); fewer run it on planar images.  The
+    samples and their summation order are the same, so 11 slices at once must
+    equal 4 + 7 slices bit for bit: Radon, tEM (with metrics) and eEM."""
+    import ctypes
+    import torch
+    from sscRaft import synthetic as S
+    from sscRaft.rafttypes import _ptr, libraft
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    N, A, n = 200, 150, 11
+    ang = (np.arange(A) * (np.pi / A)).astype(np.float32)
+    img = torch.stack([S.phantom_image(S.ellipse_params(700 + k, 8), N, xp=torch, device="cuda")
+                       for k in range(n)]).contiguous()
+    full = torch.empty((n, A, N), device="cuda")
+    assert libraft.raft_radon_device(0, p(full), p(img), _ptr(ang), N, N, N, A, n, 1.0, 1.0, None) == 0
+    parts = torch.empty_like(full)
+    for a, b in ((0, 4), (4, 11)):
+        assert libraft.raft_radon_device(0, p(parts[a:b]), p(img[a:b]), _ptr(ang), N, N, N, A, b - a, 1.0, 1.0,
+                                         None) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(full, parts)
+    trans = torch.exp(-full * (2.5 / full.amax())).contiguous()
+    flat = torch.ones((n, N), device="cuda")
+    for kind, data in ((0, trans), (1, full * (2.0 / (N - 1)))):
+        data = data.contiguous()
+        o_full = torch.ones((n, N, N), device="cuda")
+        m_full = torch.zeros((3, n, 3), dtype=torch.float64, device="cuda")
+        assert libraft.raft_em_device(kind, 0, p(o_full), p(data), p(flat), _ptr(ang), N, A, n, 3, p(m_full), 1,
+                                      None) == 0
+        o_part = torch.ones_like(o_full)
+        m_part = torch.zeros_like(m_full)
+        for a, b in ((0, 4), (4, 11)):
+            m = torch.zeros((3, b - a, 3), dtype=torch.float64, device="cuda")
+            assert libraft.raft_em_device(kind, 0, p(o_part[a:b]), p(data[a:b]), p(flat[a:b]), _ptr(ang), N, A,
+                                          b - a, 3, p(m), 1, None) == 0
+            m_part[:, a:b] = m
+        torch.cuda.synchronize()
+        assert torch.equal(o_full, o_part), kind
+        assert torch.allclose(m_full, m_part, rtol=1e-12, atol=0), kind
