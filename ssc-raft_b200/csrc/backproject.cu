@@ -99,16 +99,18 @@ __device__ __forceinline__ void angle_param(const BpArgs &p, int a, int x0, int 
             for (int cx = 0; cx < 2; cx++) {
                 const int i = x0 + cx * (BP_TX - 1), j = y0 + cy * (BP_TY - 1);
                 int ti;
-                // the same expressions as the per-pixel index in bp_tile
+                // the corner bins need not match bp_tile's per-pixel rounding
+                // exactly: the window starts one bin below the lowest corner
                 if constexpr (GEOM == GEOM_FBP_REF) {
-                    const float x = __fmaf_rn((float)(i + p.offo), p.dx, p.xmin);
-                    const float y = __fmaf_rn((float)(j + p.offo), p.dy, p.ymin);
-                    const float t = __fmaf_rn(x, c, -__fmul_rn(y, s));
+                    const int ip = i + p.offo, jp = j + p.offo;
+                    float x = p.xmin + ip * p.dx;
+                    float y = p.ymin + jp * p.dy;
+                    float t = x * c - y * s;
                     ti = (int)((t - p.tmin) / p.dt);
                 } else {
-                    const float x = __fmaf_rn((float)i, p.dxy, p.xymin);
-                    const float y = __fmaf_rn((float)j, p.dxy, p.xymin);
-                    const float t = __fmaf_rn(x, c, __fmul_rn(y, s));
+                    float x = p.xymin + i * p.dxy;
+                    float y = p.xymin + j * p.dxy;
+                    float t = x * c + y * s;
                     ti = (int)((t - p.tmin) / p.dt);
                 }
                 tmin_i = min(tmin_i, ti);
