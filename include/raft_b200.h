@@ -85,6 +85,21 @@ int raft_abi_version(void);
 int raft_fbp_ext(int *gpus, int ngpus, float *obj, const float *tomogram, const float *angles,
                  const float *paramf, const int *parami, int geometry, int store);
 
+/* Flat/dark correction of frames [nslices][nangles][nrays] in place:
+ * T = max(D - dark, 0.5) / max(flat - dark, 0.5), then T = -log(T) when is_log = 1;
+ * flat [nslices][numflats][nrays] (with two or more flats the first two are
+ * interpolated by angle index / nangles), dark [nslices][nrays].
+ * Reference: getBackgroundCorrectionMultiGPU, cuda/src/processing/background_correction.cu:144-178
+ * (kernel :15-47, -log opt.cu:196-214).  Errors via raft_last_error. */
+void getBackgroundCorrectionMultiGPU(int *gpus, int ngpus, float *frames, float *flat, float *dark,
+                                     int nrays, int nangles, int nslices, int numflats, int is_log,
+                                     int blocksize);
+
+/* getBackgroundCorrectionMultiGPU on device-resident buffers of one GPU (in place on
+ * d_frames), NULL stream as raft_fbp_device.  Returns 0 on success. */
+int raft_background_device(int gpu, float *d_frames, const float *d_flat, const float *d_dark, int nrays,
+                           int nangles, int nslices, int numflats, int is_log, void *stream);
+
 /* Streams of the device-pointer entry points below: work is issued on `stream`; NULL
  * means "ordered after everything already queued on the legacy default stream" (the
  * stream PyTorch uses by default): the library then runs on its own stream, made to

@@ -60,6 +60,7 @@ def lib():
         _lib.oracle_conv3x3_fwd.argtypes = [P, P, P, P, I, I, I, I, I, I]
         _lib.oracle_conv3x3_wgrad.argtypes = [P, P, P, I, I, I, I, I]
         _lib.oracle_conv3x3_dgrad.argtypes = [P, P, P, I, I, I, I, I]
+        _lib.oracle_background.argtypes = [P, P, P, I, I, I, I, I, P]
     return _lib
 
 
@@ -250,3 +251,16 @@ def conv3x3_dgrad(dy, w):
     dx = np.zeros((N, H, W, Cin))
     lib().oracle_conv3x3_dgrad(_p(dy), _p(w), _p(dx), N, H, W, Cin, Cout)
     return dx
+
+
+def background(frames, flat, dark, is_log):
+    """Flat/dark correction (+ -log), background_correction.cu:15-47 / opt.cu:196-214.
+    frames [B, A, N], flat [B, F, N] (or [B, N]), dark [B, N]; FP64 result."""
+    fr = _as3(_f32(frames))
+    B, A, N = fr.shape
+    fl = _f32(flat).reshape(B, -1, N)
+    dk = _f32(dark).reshape(B, N)
+    out = np.empty((B, A, N), np.float64)
+    lib().oracle_background(_p(fr), _p(np.ascontiguousarray(fl)), _p(dk), N, A, B, fl.shape[1], int(bool(is_log)),
+                            _p(out))
+    return out.reshape(np.shape(frames))

@@ -575,3 +575,27 @@ void oracle_conv3x3_dgrad(const double *dy, const double *w, double *dx, int N, 
                     dx[(((size_t)n * H + yy) * W + xx) * Cin + ci] = s;
                 }
 }
+
+/* Flat/dark correction, BackgroundCorrection (background_correction.cu:15-47),
+ * and -log, Klog (opt.cu:196-214), in FP64: per slice z, angle a, ray x
+ *   flat = F[z][0][x]                                      (one flat)
+ *        = F[z][0][x] (1 - a/A) + (a/A) F[z][1][x]         (two or more: first two)
+ *   t    = max(D - dark, 0.5) / max(flat - dark, 0.5),  t = -log(t) if is_log. */
+void oracle_background(const float *frames, const float *flat, const float *dark, int nrays, int nangles,
+                       int nslices, int numflats, int is_log, double *out)
+{
+#pragma omp parallel for collapse(2)
+    for (int z = 0; z < nslices; z++)
+        for (int a = 0; a < nangles; a++)
+            for (int x = 0; x < nrays; x++) {
+                const double dk = dark[(size_t)z * nrays + x];
+                double ft = flat[(size_t)z * numflats * nrays + x];
+                if (numflats > 1) {
+                    const double w = (double)a / (double)nangles;
+                    ft = ft * (1.0 - w) + w * flat[((size_t)z * numflats + 1) * nrays + x];
+                }
+                const size_t i = ((size_t)z * nangles + a) * nrays + x;
+                const double t = fmax(frames[i] - dk, 0.5) / fmax(ft - dk, 0.5);
+                out[i] = is_log ? -log(t) : t;
+            }
+}

@@ -320,6 +320,54 @@ void getFilterLowPassMultiGPU(int *gpus, int ngpus, float *tomogram, float *para
                 [&](int dev, int start, int n) { lowpass_host_slab(cfg, dev, tomogram + ps * start, n); });
 }
 
+// --- flat / dark correction ---------------------------------------------------
+// Reference: getBackgroundCorrectionMultiGPU, cuda/src/processing/background_correction.cu:144-178
+static bool check_background(int nrays, int nangles, int nslices, int numflats, int is_log)
+{
+    if (nrays < 1 || nangles < 1 || nslices < 0 || numflats < 1 || (is_log != 0 && is_log != 1)) {
+        set_error("background correction: need nrays, nangles, numflats >= 1, nslices >= 0, is_log 0 or 1");
+        return false;
+    }
+    return true;
+}
+
+void getBackgroundCorrectionMultiGPU(int *gpus, int ngpus, float *frames, float *flat, float *dark, int nrays,
+                                     int nangles, int nslices, int numflats, int is_log, int blocksize)
+{
+    clear_error();
+    if (!check_background(nrays, nangles, nslices, numflats, is_log)) return;
+    if (!check_gpus(gpus, ngpus)) return;
+    if (!frames || !flat || !dark) {
+        set_error("null data pointer");
+        return;
+    }
+    const size_t ps = (size_t)nangles * nrays;
+    split_slabs(gpus, ngpus, nslices, [&](int dev, int start, int n) {
+        background_host_slab(dev, frames + ps * start, flat + (size_t)numflats * nrays * start,
+                             dark + (size_t)nrays * start, nrays, nangles, n, numflats, is_log, blocksize);
+    });
+}
+
+// Device-resident flat/dark correction on one GPU, in place on d_frames.
+int raft_background_device(int gpu, float *d_frames, const float *d_flat, const float *d_dark, int nrays,
+                           int nangles, int nslices, int numflats, int is_log, void *stream)
+{
+    clear_error();
+    if (!check_background(nrays, nangles, nslices, numflats, is_log)) return 1;
+    if (!check_gpus(&gpu, 1)) return 1;
+    try {
+        DeviceState &ds = device_state(gpu);
+        std::lock_guard<std::mutex> lk(ds.mtx);
+        RAFT_CUDA(cudaSetDevice(gpu));
+        ds.ensure();
+        cudaStream_t st = resolve_stream(ds, stream, ds.s_comp);
+        launch_background(d_frames, d_frames, d_flat, d_dark, nrays, nangles, nslices, numflats, is_log, st);
+        if (!stream) RAFT_CUDA(cudaStreamSynchronize(st));
+    } catch (const CudaFail &) {
+    }
+    return has_error() ? 1 : 0;
+}
+
 // --- Radon ----------------------------------------------------------------
 // Reference: getRadonRTMultiGPU, cuda/src/geometries/parallel/forward_methods/radon_rt.cu:252-295
 void getRadonRTMultiGPU(int *gpus, int ngpus, float *tomogram, float *phantom, float *angles, int sizex, int sizey,

@@ -372,6 +372,35 @@ void lowpass_host_slab(const FbpConfig &cfg, int device, float *tomo, int nslice
     });
 }
 
+// ------------------------------------------------------ flat / dark --
+// getBackgroundCorrectionGPU (background_correction.cu:62-142): per device the
+// slab's flats and darks are uploaded once; frames stream through the
+// two-slot pipeline and come back corrected in place.
+void background_host_slab(int device, float *frames, const float *flat, const float *dark, int nrays, int nangles,
+                          int nslices, int numflats, int is_log, int blocksize)
+{
+    if (nslices <= 0) return;
+    DeviceState &ds = device_state(device);
+    std::lock_guard<std::mutex> lk(ds.mtx);
+    RAFT_CUDA(cudaSetDevice(device));
+    ds.ensure();
+    const size_t fl_bytes = (size_t)nslices * numflats * nrays * sizeof(float);
+    const size_t dk_bytes = (size_t)nslices * nrays * sizeof(float);
+    const size_t dk_off = (fl_bytes + 255) & ~(size_t)255;
+    char *aux = (char *)ds.flat.get(dk_off + dk_bytes);
+    float *d_flat = (float *)aux, *d_dark = (float *)(aux + dk_off);
+    RAFT_CUDA(cudaMemcpyAsync(d_flat, flat, fl_bytes, cudaMemcpyHostToDevice, ds.s_comp));
+    RAFT_CUDA(cudaMemcpyAsync(d_dark, dark, dk_bytes, cudaMemcpyHostToDevice, ds.s_comp));
+    const size_t ps = (size_t)nangles * nrays * sizeof(float);
+    const int chunk = auto_chunk(nslices, ps, blocksize);
+    int s0 = 0;   // first slice of the chunk being computed (chunks run in order)
+    run_pipeline(ds, nslices, chunk, ps, ps, frames, frames, [&](void *din, void *dout, int ns, cudaStream_t st) {
+        launch_background((const float *)din, (float *)dout, d_flat + (size_t)s0 * numflats * nrays,
+                          d_dark + (size_t)s0 * nrays, nrays, nangles, ns, numflats, is_log, st);
+        s0 += ns;
+    });
+}
+
 // ---------------------------------------------------------------- Radon --
 void radon_host_slab(int device, float *proj, const float *img, const float *angles, int nx, int ny, int nrays,
                      int nangles, int nslices, float ax, float ay)

@@ -87,6 +87,8 @@ void fbp_host_slab(const FbpConfig &cfg, int device, float *obj, const float *to
 
 // --- lowpass -------------------------------------------------------------
 void lowpass_host_slab(const FbpConfig &cfg, int device, float *tomo, int nslices);
+void background_host_slab(int device, float *frames, const float *flat, const float *dark, int nrays, int nangles,
+                          int nslices, int numflats, int is_log, int blocksize);
 
 // --- Radon ---------------------------------------------------------------
 void radon_host_slab(int device, float *proj, const float *img, const float *angles, int nx, int ny,

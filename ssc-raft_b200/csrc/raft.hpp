@@ -216,6 +216,11 @@ size_t proj_scratch_bytes(int nx, int ny, int nslices);
 // planes, else a transposed copy (pl.imgT).  Issued on st.
 void stage_proj_images(ProjLaunch &pl, void *scratch, cudaStream_t st);
 
+// Flat/dark correction (and -log when is_log) of frames [nslices][nangles][nrays]
+// from flat [nslices][numflats][nrays] and dark [nslices][nrays]; out may equal in.
+void launch_background(const float *in, float *out, const float *flat, const float *dark, int nrays, int nangles,
+                       int nslices, int numflats, int is_log, cudaStream_t st);
+
 // Copy a plain sinogram into weighted window rows (EM: BP of the counts).
 void launch_to_window(const float *sino, float *rows, const float *wt, int nrows, int nangles,
                       int nrays, int wlo, int Wg, cudaStream_t st);

@@ -1,1 +1,3 @@
-from .filters import *
+from .filters import *  # noqa: F401,F403
+from .background_correction import *  # noqa: F401,F403
+from .background_correction import _background_correctionGPU  # noqa: F401

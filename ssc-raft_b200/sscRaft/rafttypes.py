@@ -51,6 +51,8 @@ libraft.getBSTMultiGPU.argtypes = [_P, _I, _P, _P, _P, _P, _P, _I]
 libraft.getBSTMultiGPU.restype = None
 libraft.get_tEM_FQ_MultiGPU.argtypes = [_P, _I, _P, _P, _P, _P, _P, _P]
 libraft.get_tEM_FQ_MultiGPU.restype = None
+libraft.getBackgroundCorrectionMultiGPU.argtypes = [_P, _I, _P, _P, _P, _I, _I, _I, _I, _I, _I]
+libraft.getBackgroundCorrectionMultiGPU.restype = None
 # Extensions
 libraft.raft_last_error.argtypes = [ctypes.c_char_p, _I]
 libraft.raft_last_error.restype = _I
@@ -69,6 +71,8 @@ libraft.raft_em_ext.restype = _I
 libraft.raft_em_device.argtypes = [_I, _I, _P, _P, _P, _P, _I, _I, _I, _I, _P, _I, _P]
 libraft.raft_radon_device.argtypes = [_I, _P, _P, _P, _I, _I, _I, _I, _I, _F, _F, _P]
 libraft.raft_radon_device.restype = _I
+libraft.raft_background_device.argtypes = [_I, _P, _P, _P, _I, _I, _I, _I, _I, _P]
+libraft.raft_background_device.restype = _I
 libraft.raft_em_device.restype = _I
 
 libraft.raft_launch_count.argtypes = []

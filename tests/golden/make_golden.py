@@ -3,11 +3,12 @@
 Runs on a GPU box: loads oracle/_ref/libraft_ref.so (built from the
 reference sources by oracle/build_ref.sh) and calls its own C ABI
 (getFBPMultiGPU, getFilterLowPassMultiGPU, getRadonRTMultiGPU,
-get_tEM_RT_MultiGPU, get_eEM_RT_MultiGPU) with the packing of the reference
-Python wrappers, on small seeded inputs.  Inputs and outputs are saved
-together in tests/golden/ref_<case>.npz (or under --out).
+get_tEM_RT_MultiGPU, get_eEM_RT_MultiGPU, getBackgroundCorrectionMultiGPU)
+with the packing of the reference Python wrappers, on small seeded inputs.
+Inputs and outputs are saved together in tests/golden/ref_<case>.npz (or
+under --out); --only PREFIX writes only the cases whose names start with it.
 
-    python tests/golden/make_golden.py [--out DIR]
+    python tests/golden/make_golden.py [--out DIR] [--only PREFIX]
 """
 import argparse
 import ctypes
@@ -37,6 +38,7 @@ def load_ref():
     lib.getRadonRTMultiGPU.argtypes = [P, I, P, P, P, I, I, I, I, I, F, F]
     lib.get_tEM_RT_MultiGPU.argtypes = [P, I, P, P, P, P, P, P]
     lib.get_eEM_RT_MultiGPU.argtypes = [P, I, P, P, P, P, P]
+    lib.getBackgroundCorrectionMultiGPU.argtypes = [P, I, P, P, P, I, I, I, I, I, I]
     return lib
 
 
@@ -87,9 +89,29 @@ def index_probe(lib, N, pad, pixel, thetas):
                 out=np.stack(out), Np=Np)
 
 
+def background_case(lib, B, A, N, nflats, is_log, seed):
+    """Raw frames from a phantom's projections: dark + (flat - dark) * exp(-p)
+    plus noise, some samples below the dark (the 0.5 clamp) and above the flat."""
+    rng = np.random.default_rng(seed)
+    sino, ang = sino_case(N, A, B, seed=seed)
+    p = sino / max(float(sino.max()), 1e-6) * 2.5
+    flat = rng.uniform(800.0, 1200.0, (B, nflats, N)).astype(np.float32)
+    dark = rng.uniform(50.0, 150.0, (B, N)).astype(np.float32)
+    w = (np.arange(A, dtype=np.float64) / A)[None, :, None]
+    ft = flat[:, :1, :] * (1 - w) + w * flat[:, min(1, nflats - 1):min(1, nflats - 1) + 1, :]
+    frames = dark[:, None, :] + (ft - dark[:, None, :]) * np.exp(-p) + rng.normal(0, 5.0, (B, A, N))
+    frames[:, ::7, ::5] = dark[:, None, ::5] - 20.0        # below the dark: clamped to 0.5
+    frames[:, 3::11, 2::9] += 400.0                       # above the flat
+    frames = frames.astype(np.float32)
+    out = frames.copy()
+    lib.getBackgroundCorrectionMultiGPU(ptr(GPUS), 1, ptr(out), ptr(flat), ptr(dark), N, A, B, nflats, is_log, 0)
+    return dict(kind="background", frames=frames, flat=flat, dark=dark, is_log=is_log, out=out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
+    ap.add_argument("--only", default="")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     lib = load_ref()
@@ -139,6 +161,10 @@ def main():
     t = tomo.copy()
     lib.get_eEM_RT_MultiGPU(ptr(GPUS), 1, ptr(obj), ptr(t), ptr(ang), ptr(pf), ptr(pi))
     cases["eem_n48"] = dict(kind="eem", tomo=tomo, angles=ang, iterations=it, out=obj)
+    # flat/dark correction: two flats + log (odd row length), one flat no log, three flats + log
+    cases["bg_log_2flats"] = background_case(lib, 3, 50, 70, 2, 1, seed=700)
+    cases["bg_nolog_1flat"] = background_case(lib, 2, 33, 64, 1, 0, seed=701)
+    cases["bg_log_3flats"] = background_case(lib, 2, 20, 40, 3, 1, seed=702)
     # the fast-intrinsic sin/cos values the reference's index rules use, as data
     # for the oracle: kind 0 = __sinf/__cosf, kind 1 = __sincosf
     from sscRaft.rafttypes import fast_sincos
@@ -150,6 +176,7 @@ def main():
             allang = np.concatenate([[t, np.float32(t) + np.float32(2.0 ** -10)] for t in d["thetas"]])
             allang = allang.astype(np.float32)
             d["fcos"], d["fsin"] = fast_sincos(allang, 0)
+    cases = {k: v for k, v in cases.items() if k.startswith(args.only)}
     for name, d in cases.items():
         np.savez_compressed(os.path.join(args.out, f"ref_{name}.npz"), **d)
     print("wrote", len(cases), "fixtures to", args.out)

@@ -1,7 +1,8 @@
 """CPU tests of the Python drop-in layer (sscRaft): the packed parameter
 arrays it hands to the C ABI match the reference wrappers
 (sscRaft/geometries/parallel/fbp_methods.py:86-95, em_methods.py:55-65,136-145,
-radon_methods.py:42-58, processing/filters.py:75-87 of cnpem/ssc-raft).
+radon_methods.py:42-58, processing/filters.py:75-87,
+processing/background_correction.py:6-106 of cnpem/ssc-raft).
 The library is replaced by a recording fake; no GPU is touched."""
 import ctypes
 
@@ -37,9 +38,9 @@ def arr(p, n, ct):
 def fake(monkeypatch):
     import sscRaft
     from sscRaft.geometries.parallel import fbp_methods, em_methods, radon_methods
-    from sscRaft.processing import filters
+    from sscRaft.processing import filters, background_correction
     f = Fake(sscRaft.rafttypes.libraft)
-    for m in (fbp_methods, em_methods, radon_methods, filters):
+    for m in (fbp_methods, em_methods, radon_methods, filters, background_correction):
         monkeypatch.setattr(m, "libraft", f)
     sscRaft.rafttypes.libraft.raft_clear_error()
     return f
@@ -134,3 +135,33 @@ def test_lowpass_inplace(fake):
     assert out is t and name == "getFilterLowPassMultiGPU"
     assert list(arr(a[4], 10, ctypes.c_int32)) == [16, 5, 2, 16, 1, 0, 0, 6, 0, 0]
     assert arr(a[3], 7, ctypes.c_float)[6] == 0.0      # axis offset forced to 0
+
+
+def test_background_packing_and_layouts(fake):
+    import sscRaft
+    fr = np.zeros((3, 7, 16), np.float32)
+    fl = np.ones((3, 2, 16), np.float32)
+    dk = np.zeros((3, 1, 16), np.float32)               # [slices, 1, rays] is accepted
+    out = sscRaft.correct_background(fr, fl, dk, gpus=[0], is_log=True, blocksize=4)
+    name, a = fake.calls[-1]
+    assert out is fr and name == "getBackgroundCorrectionMultiGPU"
+    assert a[5:] == (16, 7, 3, 2, 1, 4)
+    # correct_projections takes [angles, slices, rays] and returns [slices, angles, rays]
+    raw = np.zeros((7, 3, 16), np.float32)
+    out = sscRaft.correct_projections(raw, np.ones((1, 3, 16), np.float32), np.zeros((1, 3, 16), np.float32),
+                                      {"gpu": [0], "uselog": False})
+    name, a = fake.calls[-1]
+    assert out.shape == (3, 7, 16) and a[5:] == (16, 7, 3, 1, 0, 0)
+
+
+def test_background_shape_errors(fake):
+    import sscRaft
+    fr = np.zeros((3, 7, 16), np.float32)
+    with pytest.raises(ValueError):
+        sscRaft.correct_background(fr, np.ones((2, 1, 16), np.float32), np.zeros((3, 16), np.float32))
+    with pytest.raises(ValueError):
+        sscRaft.correct_background(fr, np.ones((3, 1, 16), np.float32), np.zeros((3, 15), np.float32))
+    with pytest.raises(ValueError):
+        sscRaft.correct_background(np.zeros((1, 3, 7, 16), np.float32), np.ones((3, 1, 16), np.float32),
+                                   np.zeros((3, 16), np.float32))
+    assert not [c for c in fake.calls if c[0] == "getBackgroundCorrectionMultiGPU"]
