@@ -453,6 +453,27 @@ def run_ours(args):
         launches = libraft.raft_launch_count() - n0
         return ranks_max(e0.elapsed_time(e1) / K), launches
 
+    def bst_step():
+        st = torch.cuda.current_stream(dev).cuda_stream
+        rc = libraft.raft_bst_device(local, ctypes.c_void_p(img.data_ptr()), ctypes.c_void_p(sino.data_ptr()),
+                                     _ptr(pf), _ptr(pi), ctypes.c_void_p(st))
+        if rc:
+            check_error("raft_bst_device")
+
+    def time_bst(K, W):
+        for _ in range(W):
+            bst_step()
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(K):
+            bst_step()
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        return ranks_max(e0.elapsed_time(e1) / K)
+
     def profile_bp(geometry, store):
         libraft.raft_profile_enable(1)
         device_step(geometry, store)
@@ -468,6 +489,12 @@ def run_ours(args):
         r = run_ragged(dev)
         if rank == 0:
             print(json.dumps({"quick": True, "op": "ragged", **r}), flush=True)
+        return
+    if args.quick and args.op == "bst":
+        ms = time_bst(args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({"quick": True, "op": "bst", "slices": nsl, "ms_per_step": ms,
+                              "slices_per_s": ws * nsl / (ms / 1e3)}), flush=True)
         return
     if args.quick and args.op == "flat_dark":
         r = run_flat_dark(dev, sino, reps=args.steps, hbm_peak=hbm_peak)
@@ -515,6 +542,10 @@ def run_ours(args):
         for name, g, s in (("linear_fp32", 1, 1), ("linear_bf16", 1, 2)):
             ms_v, _ = time_device(g, s, max(1, args.steps), max(3, args.warmup))
             variants[name] = {"value": ws * nsl / (ms_v / 1e3), "ms_per_step": ms_v}
+        ms_b = time_bst(max(1, args.steps), max(3, args.warmup))
+        variants["bst"] = {"value": ws * nsl / (ms_b / 1e3), "ms_per_step": ms_b,
+                           "operator": "backprojection slice theorem (Fourier regridding), Hann, axis offset "
+                                       "truncated to 3 as the reference does, padding 2 (6144-point transforms)"}
     clocks = clk.summary()
 
     # dominant kernel: the backprojector; one profiled pass of the headline operator
@@ -667,7 +698,7 @@ def main():
     ap.add_argument("--no-warm", action="store_true")
     ap.add_argument("--no-flat-dark", action="store_true")
     ap.add_argument("--quick", action="store_true", help="device timing of one operator only (profiling)")
-    ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "tem", "ragged", "flat_dark"])
+    ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "tem", "ragged", "flat_dark", "bst"])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

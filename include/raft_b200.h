@@ -62,11 +62,22 @@ void get_tEM_RT_MultiGPU(int *gpus, int ngpus, float *obj, float *count, float *
 void get_eEM_RT_MultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *angles,
                          float *paramf, int *parami);
 
-/* Adjacent reference exports kept as stubs that record "not implemented".
- * getBSTMultiGPU: cuda/src/geometries/parallel/reconstruction_methods/bst.cu:674-734 (rafttypes.py:161-173).
- * get_tEM_FQ_MultiGPU: .../reconstruction_methods/em_frequency.cu:339 (rafttypes.py:149-159). */
+/* FBP by the backprojection slice theorem (Fourier regridding), packing as getFBPMultiGPU
+ * (object N x N).  Angles are taken as uniform over [0, pi), as the reference's regridding
+ * assumes (the Python wrapper passes linspace(0, pi, A)); `angles` and `nstreams` are unused.
+ * Requires N*(1+pad) with prime factors 2, 3, 5, 7 only and <= 9472.
+ * Replaces getBSTMultiGPU, cuda/src/geometries/parallel/reconstruction_methods/bst.cu:674-734
+ * (rafttypes.py:161-173). */
 void getBSTMultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *angles, float *paramf,
                     int *parami, int nstreams);
+
+/* getBSTMultiGPU on device-resident buffers of one GPU; NULL stream as raft_fbp_device.
+ * Returns 0 on success. */
+int raft_bst_device(int gpu, float *d_obj, const float *d_tomogram, const float *paramf, const int *parami,
+                    void *stream);
+
+/* Adjacent reference export kept as a stub that records "not implemented":
+ * get_tEM_FQ_MultiGPU: .../reconstruction_methods/em_frequency.cu:339 (rafttypes.py:149-159). */
 void get_tEM_FQ_MultiGPU(int *gpus, int ngpus, float *obj, float *count, float *flat, float *angles,
                          float *paramf, int *parami);
 

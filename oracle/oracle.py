@@ -61,6 +61,7 @@ def lib():
         _lib.oracle_conv3x3_wgrad.argtypes = [P, P, P, I, I, I, I, I]
         _lib.oracle_conv3x3_dgrad.argtypes = [P, P, P, I, I, I, I, I]
         _lib.oracle_background.argtypes = [P, P, P, I, I, I, I, I, P]
+        _lib.oracle_bst.argtypes = [P, I, I, I, I, I, D, D, I, F, P]
     return _lib
 
 
@@ -264,3 +265,15 @@ def background(frames, flat, dark, is_log):
     lib().oracle_background(_p(fr), _p(np.ascontiguousarray(fl)), _p(dk), N, A, B, fl.shape[1], int(bool(is_log)),
                             _p(out))
     return out.reshape(np.shape(frames))
+
+
+def bst(tomo, ftype, pad, paganin=0.0, reg=0.0, offset=0, pixel=1.0):
+    """FBP by the backprojection slice theorem (bst.cu:251-312, 534-642 and
+    filters.cu:295-390); tomo [B, A, N] -> [B, N, N] FP64.  offset: integer
+    axis offset (the reference truncates it)."""
+    t = _as3(_f32(tomo))
+    B, A, N = t.shape
+    out = np.empty((B, N, N), np.float64)
+    lib().oracle_bst(_p(t), N, A, B, int(pad), int(ftype), float(paganin), float(reg), int(offset), float(pixel),
+                     _p(out))
+    return out if np.ndim(tomo) == 3 else out[0]

@@ -599,3 +599,110 @@ void oracle_background(const float *frames, const float *flat, const float *dark
                 out[i] = is_log ? -log(t) : t;
             }
 }
+
+/* FBP by the backprojection slice theorem: getBST (bst.cu:251-312) on the
+ * padded tomogram of getBSTGPU (bst.cu:534-642), BSTFilter / BandFilterC2C
+ * (filters.cu:295-390), sino2p / convBST / polar2cartesian_fourier
+ * (bst.cu:22-98).  Transforms and accumulation in FP64; the regridding
+ * geometry (radius, arc index and their fractions) in float, as the
+ * reference computes it.  The half-rays are zero-padded (the reference's
+ * buffer is not cleared) and all A rows are padded (the reference's padding
+ * call covers N rows; identical when A == N).  csino: integer axis offset. */
+void oracle_bst(const float *tomo, int N, int A, int B, int pad, int ftype, double paganin, double reg, int csino,
+                float pixel, double *out)
+{
+    const int Np = N * (1 + pad), L = Np, S = Np, off = (pad * N) / 2, half = Np / 2, c = Np / 2;
+    const int twoA = 2 * A;
+    cplx *G = (cplx *)malloc(sizeof(cplx) * Np);
+    for (int k = 0; k < Np; k++) {
+        double w = ref_apply(ftype, (double)(k < Np - k ? k : Np - k) / (double)Np, paganin, reg);
+        double ph = -2.0 * PI_D * (double)csino * (double)k / (double)Np;
+        G[k] = w * (cos(ph) + I * sin(ph));
+    }
+    cplx *rfwd = make_roots(Np, -1), *rinv = make_roots(Np, +1);
+    const float scale = (float)Np * pixel * 4.0f;
+    for (int z = 0; z < B; z++) {
+        double *rows = (double *)malloc(sizeof(double) * (size_t)A * Np);
+        cplx *P = (cplx *)malloc(sizeof(cplx) * (size_t)twoA * L);
+        cplx *cart = (cplx *)calloc((size_t)S * S, sizeof(cplx));
+#pragma omp parallel
+        {
+            cplx *a = (cplx *)malloc(sizeof(cplx) * Np);
+            cplx *b = (cplx *)malloc(sizeof(cplx) * Np);
+            cplx *scratch = (cplx *)malloc(sizeof(cplx) * (size_t)(2 * Np + 8));
+#pragma omp for schedule(dynamic, 4)
+            for (int r = 0; r < A; r++) {
+                double *row = rows + (size_t)r * Np;
+                pad_row(tomo + ((size_t)z * A + r) * N, N, pad, Np, row);
+                if (ftype != 0) {
+                    for (int i = 0; i < Np; i++) a[i] = row[i];
+                    fft(Np, a, b, rfwd, scratch);
+                    for (int k = 0; k < Np; k++) b[k] *= G[k];
+                    fft(Np, b, a, rinv, scratch);
+                    for (int i = 0; i < Np; i++) row[i] = creal(a[i]);
+                }
+                for (int side = 0; side < 2; side++) {
+                    for (int idx = 0; idx < L; idx++) {
+                        double v = 0.0;
+                        if (idx < half) {
+                            double w = idx == 0 ? 2.0 : 4.0;
+                            v = w * (side == 0 ? row[c - 1 - idx] : row[c + idx]);
+                        }
+                        a[idx] = v;
+                    }
+                    fft(L, a, b, rfwd, scratch);
+                    cplx *dst = P + (size_t)(side == 0 ? r : A + r) * L;
+                    for (int k = 0; k < L; k++) {
+                        double m = (double)(k < L - k ? k : L - k);
+                        dst[k] = b[k] * (2.0 / ((double)L * (m > 0.5 ? m : 0.5)));
+                    }
+                }
+            }
+            free(a); free(b); free(scratch);
+        }
+#pragma omp parallel for schedule(dynamic, 8)
+        for (int ty = 0; ty < S; ty++)
+            for (int tx = 0; tx < S; tx++) {
+                int posx = tx - S / 2, posy = ty - S / 2;
+                float rho = (float)L * hypotf((float)posx, (float)posy) / (float)S;
+                float angle = (float)twoA * (0.5f * atan2f((float)posy, (float)posx) / (float)PI_D + 0.5f);
+                int irho = (int)rho;
+                int iarc = (int)angle;
+                cplx v = 0;
+                if (irho < L / 2 - 1) {
+                    float pfrac = rho - (float)irho;
+                    float tfrac = (float)iarc - angle;
+                    iarc = iarc % twoA;
+                    int uarc = (iarc + 1) % twoA;
+                    const cplx *q0 = P + (size_t)iarc * L + irho, *q1 = P + (size_t)uarc * L + irho;
+                    cplx i0 = q0[0] * (double)(1.0f - pfrac) + q0[1] * (double)pfrac;
+                    cplx i1 = q1[0] * (double)(1.0f - pfrac) + q1[1] * (double)pfrac;
+                    v = i0 * (double)tfrac + i1 * (double)(1.0f - tfrac);
+                }
+                float sgn = 4.0f * ((float)(tx % 2) - 0.5f) * ((float)(ty % 2) - 0.5f);
+                cart[(size_t)((ty + S / 2) % S) * S + (tx + S / 2) % S] = v * (double)sgn;
+            }
+        /* S x S inverse transform (unnormalised): rows, then the crop columns */
+#pragma omp parallel
+        {
+            cplx *a = (cplx *)malloc(sizeof(cplx) * S);
+            cplx *b = (cplx *)malloc(sizeof(cplx) * S);
+            cplx *scratch = (cplx *)malloc(sizeof(cplx) * (size_t)(2 * S + 8));
+#pragma omp for schedule(dynamic, 8)
+            for (int y = 0; y < S; y++) {
+                fft(S, cart + (size_t)y * S, b, rinv, scratch);
+                memcpy(cart + (size_t)y * S, b, sizeof(cplx) * S);
+            }
+#pragma omp for schedule(dynamic, 8)
+            for (int i = 0; i < N; i++) {
+                for (int y = 0; y < S; y++) a[y] = cart[(size_t)y * S + off + i];
+                fft(S, a, b, rinv, scratch);
+                for (int j = 0; j < N; j++)
+                    out[((size_t)z * N + j) * N + i] = creal(b[off + j]) / (double)scale;
+            }
+            free(a); free(b); free(scratch);
+        }
+        free(rows); free(P); free(cart);
+    }
+    free(G); free(rfwd); free(rinv);
+}

@@ -591,16 +591,68 @@ int raft_radon_device(int gpu, float *d_out, const float *d_phantom, const float
     return has_error() ? 1 : 0;
 }
 
-// Adjacent reference exports that this library does not implement: they
-// record an error instead of running (rafttypes.py binds them if present).
+// --- BST ------------------------------------------------------------------
+// Reference: getBSTMultiGPU, cuda/src/geometries/parallel/reconstruction_methods/bst.cu:674-734
+// (packing as getFBPMultiGPU; the object is N x N; angles are taken as uniform
+// over [0, pi) as the reference's regridding assumes, so `angles` is unused;
+// nstreams only chose the reference's stream count).
+static bool parse_bst(const float *paramf, const int *parami, FbpConfig &cfg)
+{
+    if (!parse_fbp_arrays(paramf, parami, cfg, true)) return false;
+    if (cfg.objsize != cfg.nrays) {
+        set_error("BST: the object size must equal nrays");
+        return false;
+    }
+    BstPlanShape sh;
+    if (!bst_plan_shape(sh, cfg.nrays, cfg.nangles, cfg.pad)) {
+        set_error("BST: the padded length N*(1+pad) must have only the prime factors 2, 3, 5, 7 and be at most 9472");
+        return false;
+    }
+    return true;
+}
+
 void getBSTMultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *angles, float *paramf, int *parami,
                     int nstreams)
 {
-    (void)gpus; (void)ngpus; (void)obj; (void)tomogram; (void)angles; (void)paramf; (void)parami; (void)nstreams;
+    (void)angles;
+    (void)nstreams;
     clear_error();
-    set_error("getBSTMultiGPU is not implemented by this library (use method='RT')");
+    FbpConfig cfg;
+    if (!parse_bst(paramf, parami, cfg)) return;
+    if (!check_gpus(gpus, ngpus)) return;
+    if (!obj || !tomogram) {
+        set_error("null data pointer");
+        return;
+    }
+    const size_t tps = (size_t)cfg.nangles * cfg.nrays, ops = (size_t)cfg.nrays * cfg.nrays;
+    split_slabs(gpus, ngpus, cfg.nslices, [&](int dev, int start, int n) {
+        bst_host_slab(cfg, dev, obj + ops * start, tomogram + tps * start, n);
+    });
 }
 
+// Device-resident BST on one GPU (d_obj [nslices][N][N], d_tomogram [nslices][A][N]).
+int raft_bst_device(int gpu, float *d_obj, const float *d_tomogram, const float *paramf, const int *parami,
+                    void *stream)
+{
+    clear_error();
+    FbpConfig cfg;
+    if (!parse_bst(paramf, parami, cfg)) return 1;
+    if (!check_gpus(&gpu, 1)) return 1;
+    try {
+        DeviceState &ds = device_state(gpu);
+        std::lock_guard<std::mutex> lk(ds.mtx);
+        RAFT_CUDA(cudaSetDevice(gpu));
+        ds.ensure();
+        cudaStream_t st = resolve_stream(ds, stream, ds.s_comp);
+        bst_device(cfg, gpu, d_obj, d_tomogram, cfg.nslices, st);
+        if (!stream) RAFT_CUDA(cudaStreamSynchronize(st));
+    } catch (const CudaFail &) {
+    }
+    return has_error() ? 1 : 0;
+}
+
+// Adjacent reference export that this library does not implement: it
+// records an error instead of running (rafttypes.py binds it if present).
 void get_tEM_FQ_MultiGPU(int *gpus, int ngpus, float *obj, float *count, float *flat, float *angles, float *paramf,
                          int *parami)
 {

@@ -1,0 +1,286 @@
+// bst.cu -- FBP by the backprojection slice theorem (BST), Fourier regridding.
+//
+// Reference (cnpem/ssc-raft): getBST / getBSTGPU,
+// cuda/src/geometries/parallel/reconstruction_methods/bst.cu:251-312,534-642,
+// BSTFilter + BandFilterC2C, cuda/src/processing/filters/filters.cu:295-390.
+// Per slice, with N rays, A angles (uniform over [0, pi)), Np = N (1 + pad):
+//   1. rows edge-padded to Np (padding.cu:140-178);
+//   2. unless the filter is 'none': row <- Re IFFT_unnormalised( FFT(row)
+//      * apply(min(k, Np-k)/Np) * exp(-2 pi i c k / Np) ), c = integer axis offset;
+//   3. each row split at its centre Np/2 into two half-rays of Np/2 samples,
+//      the left one reversed (the ray at theta + pi), scaled by 4 (2 at the
+//      centre sample), zero-padded to L = Np (sino2p, bst.cu:22-48);
+//   4. L-point FFT of each half-ray, times 2 / (L max(min(k, L-k), 1/2)) (convBST);
+//   5. polar -> Cartesian on an S x S grid (S = Np): radius rho = L |p| / S,
+//      arc index 2A (atan2(p) / 2 pi + 1/2), linear in rho and, with the
+//      reference's weights (t = iarc - angle, w0 = t, w1 = 1 - t), across the
+//      two arcs, zero beyond rho >= L/2 - 1; times (-1)^(x+y) and stored
+//      fft-shifted (polar2cartesian_fourier, bst.cu:59-98);
+//   6. S x S inverse FFT, real part / (Np pixel 4), centre N x N crop.
+// Two deviations, both for the reference's uninitialised or mis-sized
+// buffers: step 3's zero padding is explicit (the reference leaves it to
+// freshly allocated memory), and all A rows are padded (the reference's
+// padding call is sized by N rows; identical when A == N).
+//
+// B200 design, three kernels per batch of slices, all transforms in shared
+// memory (fft.cuh), no cuFFT and no S x S intermediate in HBM:
+//   bst_rows_kernel    two projection rows per CTA: pad, filter (the two rows
+//                      as one complex sequence), split, and one complex FFT per
+//                      row carrying both half-rays (separated by symmetry);
+//                      writes only the L/2 radial bins step 5 can read;
+//   bst_regrid_kernel  one Cartesian row per CTA: interpolates the row from
+//                      the polar data straight into shared memory, inverse
+//                      FFT along x, keeps the N crop columns;
+//   bst_cols_kernel    one crop column per CTA: inverse FFT along y, keeps
+//                      the N crop rows, scales.
+// This file is compiled with fast math, as the reference is, so the regrid
+// geometry (hypotf, atan2f, the divisions) follows its rounding.
+#include "raft.hpp"
+#include "profile.hpp"
+#include "fft.cuh"
+
+#include <cmath>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+namespace raft {
+
+namespace {
+
+struct BstArgs {
+    const float *tomo;      // [B][A][N]
+    float2 *polar;          // [B][2A][Lh]
+    float2 *T;              // [B][S][N]: rows inverse-transformed along x, crop columns
+    float *obj;             // [B][N][N]
+    const float2 *tw;       // exp(-2 pi i k / Np)
+    const float2 *G;        // filter weights [Np], or null for 'none'
+    RadixList rl;
+    int N, A, Np, L, Lh, S, off;
+    float scale;
+};
+
+__global__ void __launch_bounds__(512) bst_rows_kernel(const BstArgs p)
+{
+    extern __shared__ float2 sm_bst[];
+    float2 *z = sm_bst;
+    const int slice = blockIdx.y;
+    const int a0 = 2 * blockIdx.x, a1 = a0 + 1;
+    const bool has1 = a1 < p.A;
+    const float *s0 = p.tomo + ((size_t)slice * p.A + a0) * p.N;
+    const float *s1 = s0 + p.N;
+    for (int n = threadIdx.x; n < p.Np; n += blockDim.x) {
+        const int i = min(max(n - p.off, 0), p.N - 1);
+        z[n] = make_float2(__ldg(s0 + i), has1 ? __ldg(s1 + i) : 0.f);
+    }
+    __syncthreads();
+    float sgn1 = 1.f;   // the second row is sgn1 * z.y
+    if (p.G) {
+        float2 *r = fft_forward(z, sm_bst + p.Np, p.Np, p.rl, p.tw);
+        for (int k = threadIdx.x; k < p.Np; k += blockDim.x) {
+            const float2 g = cmul(r[k], __ldg(&p.G[k]));
+            r[k] = make_float2(g.x, -g.y);
+        }
+        __syncthreads();
+        // forward transform of the conjugate = conjugate of the inverse
+        z = fft_forward(r, r == sm_bst ? sm_bst + p.Np : sm_bst, p.Np, p.rl, p.tw);
+        sgn1 = -1.f;
+    }
+    float2 *fa = (z == sm_bst) ? sm_bst + p.Np : sm_bst;
+    float2 *fb = sm_bst + 2 * p.Np;
+    const int c = p.Np / 2, half = p.Np / 2;
+    const size_t pb = (size_t)slice * 2 * p.A * p.Lh;
+    for (int r = 0; r < (has1 ? 2 : 1); r++) {
+        for (int idx = threadIdx.x; idx < p.L; idx += blockDim.x) {
+            float2 h = make_float2(0.f, 0.f);
+            if (idx < half) {
+                const float w = idx == 0 ? 2.f : 4.f;
+                const float2 lft = z[c - 1 - idx], rgt = z[c + idx];
+                h = r == 0 ? make_float2(w * lft.x, w * rgt.x) : make_float2(w * sgn1 * lft.y, w * sgn1 * rgt.y);
+            }
+            fa[idx] = h;
+        }
+        __syncthreads();
+        const float2 *H = fft_forward(fa, fb, p.L, p.rl, p.tw);
+        float2 *frow = p.polar + pb + (size_t)(a0 + r) * p.Lh;           // left half-ray (theta + pi)
+        float2 *rrow = p.polar + pb + (size_t)(p.A + a0 + r) * p.Lh;     // right half-ray (theta)
+        for (int k = threadIdx.x; k < p.Lh; k += blockDim.x) {
+            const float2 Zk = H[k], Zm = H[k == 0 ? 0 : p.L - k];
+            const float sig = 2.f / ((float)p.L * fmaxf((float)k, 0.5f));
+            // Z = FFT(f + i g): F(f) = (Z_k + conj Z_-k)/2, F(g) = (Z_k - conj Z_-k)/(2i)
+            frow[k] = make_float2(0.5f * (Zk.x + Zm.x) * sig, 0.5f * (Zk.y - Zm.y) * sig);
+            rrow[k] = make_float2(0.5f * (Zk.y + Zm.y) * sig, -0.5f * (Zk.x - Zm.x) * sig);
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(512) bst_regrid_kernel(const BstArgs p)
+{
+    extern __shared__ float2 sm_bst[];
+    const int slice = blockIdx.y, Y = blockIdx.x;
+    const int S = p.S, h = S / 2, twoA = 2 * p.A;
+    const int ty = (Y - h + S) % S;            // array row Y holds grid row ty (stored shifted by S/2)
+    const float posy = (float)(ty - h);
+    const float sy = 4.f * ((float)(ty % 2) - 0.5f);
+    const float2 *pol = p.polar + (size_t)slice * twoA * p.Lh;
+    const int rmax = p.L / 2 - 1;
+    for (int X = threadIdx.x; X < S; X += blockDim.x) {
+        const int tx = (X - h + S) % S;
+        const float posx = (float)(tx - h);
+        const float rho = (float)p.L * hypotf(posx, posy) / (float)S;
+        const float angle = (float)twoA * (0.5f * atan2f(posy, posx) / (float)M_PI + 0.5f);
+        const int irho = (int)rho;
+        int iarc = (int)angle;
+        float2 v = make_float2(0.f, 0.f);
+        if (irho < rmax) {
+            const float pfrac = rho - (float)irho;
+            const float tfrac = (float)iarc - angle;
+            iarc = iarc % twoA;
+            const int uarc = (iarc + 1) % twoA;
+            const float2 *q0 = pol + (size_t)iarc * p.Lh + irho;
+            const float2 *q1 = pol + (size_t)uarc * p.Lh + irho;
+            const float2 c00 = __ldg(q0), c01 = __ldg(q0 + 1), c10 = __ldg(q1), c11 = __ldg(q1 + 1);
+            const float2 i0 = make_float2(c00.x * (1.f - pfrac) + c01.x * pfrac, c00.y * (1.f - pfrac) + c01.y * pfrac);
+            const float2 i1 = make_float2(c10.x * (1.f - pfrac) + c11.x * pfrac, c10.y * (1.f - pfrac) + c11.y * pfrac);
+            v = make_float2(i0.x * tfrac + i1.x * (1.f - tfrac), i0.y * tfrac + i1.y * (1.f - tfrac));
+        }
+        const float sgn = sy * ((float)(tx % 2) - 0.5f);
+        sm_bst[X] = make_float2(v.x * sgn, -v.y * sgn);   // conjugated: see bst_cols_kernel
+    }
+    __syncthreads();
+    const float2 *r = fft_forward(sm_bst, sm_bst + S, S, p.rl, p.tw);
+    float2 *trow = p.T + ((size_t)slice * S + Y) * p.N;
+    for (int i = threadIdx.x; i < p.N; i += blockDim.x) trow[i] = r[p.off + i];
+}
+
+// T holds conj(IFFT_x(grid)); its forward transform along y is the conjugate
+// of the 2-D inverse transform, whose real part is the image.
+__global__ void __launch_bounds__(512) bst_cols_kernel(const BstArgs p)
+{
+    extern __shared__ float2 sm_bst[];
+    const int slice = blockIdx.y, i = blockIdx.x;
+    const float2 *tcol = p.T + (size_t)slice * p.S * p.N + i;
+    for (int Y = threadIdx.x; Y < p.S; Y += blockDim.x) sm_bst[Y] = tcol[(size_t)Y * p.N];
+    __syncthreads();
+    const float2 *r = fft_forward(sm_bst, sm_bst + p.S, p.S, p.rl, p.tw);
+    float *o = p.obj + (size_t)slice * p.N * p.N + i;
+    for (int j = threadIdx.x; j < p.N; j += blockDim.x) o[(size_t)j * p.N] = r[p.off + j].x / p.scale;
+}
+
+struct BstPlanDev {
+    BstPlanShape shape;
+    RadixList rl;
+    float2 *tw = nullptr, *G = nullptr;
+    ~BstPlanDev()
+    {
+        if (tw) cudaFree(tw);
+        if (G) cudaFree(G);
+    }
+};
+
+using BstKey = std::tuple<int, int, int, int, double, double, int>;
+std::mutex g_bst_mtx;
+std::map<BstKey, std::unique_ptr<BstPlanDev>> g_bst_plans;
+
+}  // namespace
+
+constexpr size_t kBstSmemMax = 227 * 1024;
+
+bool bst_plan_shape(BstPlanShape &s, int N, int A, int pad)
+{
+    s.N = N;
+    s.A = A;
+    s.Np = N * (1 + pad);
+    s.L = s.Np;
+    s.Lh = s.L / 2;
+    s.S = s.Np;
+    s.off = (pad * N) / 2;
+    int radix[24], nr = 0;
+    s.threads = fft_threads(s.Np);
+    return N >= 2 && A >= 1 && factorize(s.Np, radix, nr) && 3 * (size_t)s.Np * sizeof(float2) <= kBstSmemMax;
+}
+
+size_t bst_workspace_bytes(const BstPlanShape &s, int nslices)
+{
+    const size_t polar = (size_t)nslices * 2 * s.A * s.Lh * sizeof(float2);
+    const size_t T = (size_t)nslices * s.S * s.N * sizeof(float2);
+    return ((polar + 255) & ~(size_t)255) + T;
+}
+
+void launch_bst(int device, const FbpConfig &cfg, const float *d_tomo, float *d_obj, int nslices, void *workspace,
+                cudaStream_t st)
+{
+    BstPlanShape shape;
+    RAFT_CHECK(bst_plan_shape(shape, cfg.nrays, cfg.nangles, cfg.pad),
+               "BST: the padded length N*(1+pad) must have only the prime factors 2, 3, 5, 7 and be at most 9472");
+    const int c = (int)cfg.offset;   // the reference passes the axis offset to an int (filters.cu:345-390)
+    BstPlanDev *plan;
+    {
+        std::lock_guard<std::mutex> lk(g_bst_mtx);
+        const BstKey key(device, shape.Np, cfg.filter, c, cfg.paganin, cfg.reg, 0);
+        auto &slot = g_bst_plans[key];
+        if (!slot) {
+            auto pl = std::make_unique<BstPlanDev>();
+            pl->shape = shape;
+            factorize(shape.Np, pl->rl.r, pl->rl.n);
+            const std::vector<float2> tw = fft_twiddles(shape.Np);
+            RAFT_CUDA(cudaMalloc(&pl->tw, sizeof(float2) * shape.Np));
+            RAFT_CUDA(cudaMemcpy(pl->tw, tw.data(), sizeof(float2) * shape.Np, cudaMemcpyHostToDevice));
+            if (cfg.filter != FILTER_NONE) {
+                std::vector<float2> G(shape.Np);
+                for (int k = 0; k < shape.Np; k++) {
+                    const double w = filter_apply_ref(cfg.filter, (double)std::min(k, shape.Np - k) / shape.Np,
+                                                      cfg.paganin, cfg.reg);
+                    const double ph = -2.0 * M_PI * (double)c * (double)k / (double)shape.Np;
+                    G[k] = make_float2((float)(w * std::cos(ph)), (float)(w * std::sin(ph)));
+                }
+                RAFT_CUDA(cudaMalloc(&pl->G, sizeof(float2) * shape.Np));
+                RAFT_CUDA(cudaMemcpy(pl->G, G.data(), sizeof(float2) * shape.Np, cudaMemcpyHostToDevice));
+            }
+            slot = std::move(pl);
+        }
+        plan = slot.get();
+    }
+    if (nslices <= 0) return;
+    BstArgs a;
+    a.tomo = d_tomo;
+    a.polar = (float2 *)workspace;
+    const size_t polar = (size_t)nslices * 2 * shape.A * shape.Lh * sizeof(float2);
+    a.T = (float2 *)((char *)workspace + ((polar + 255) & ~(size_t)255));
+    a.obj = d_obj;
+    a.tw = plan->tw;
+    a.G = plan->G;
+    a.rl = plan->rl;
+    a.N = shape.N;
+    a.A = shape.A;
+    a.Np = shape.Np;
+    a.L = shape.L;
+    a.Lh = shape.Lh;
+    a.S = shape.S;
+    a.off = shape.off;
+    a.scale = (float)shape.Np * cfg.pixel_x * 4.0f;
+    const size_t sm3 = 3 * (size_t)shape.Np * sizeof(float2), sm2 = 2 * (size_t)shape.Np * sizeof(float2);
+    static thread_local int configured = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured != dev) {
+        RAFT_CUDA(cudaFuncSetAttribute(bst_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBstSmemMax));
+        RAFT_CUDA(cudaFuncSetAttribute(bst_regrid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBstSmemMax));
+        RAFT_CUDA(cudaFuncSetAttribute(bst_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBstSmemMax));
+        configured = dev;
+    }
+    ProfScope ps(PROF_OTHER, st);   // counts the first of the three launches
+    bst_rows_kernel<<<dim3((shape.A + 1) / 2, nslices), shape.threads, sm3, st>>>(a);
+    RAFT_CUDA(cudaGetLastError());
+    count_launch();
+    bst_regrid_kernel<<<dim3(shape.S, nslices), shape.threads, sm2, st>>>(a);
+    RAFT_CUDA(cudaGetLastError());
+    count_launch();
+    bst_cols_kernel<<<dim3(shape.N, nslices), shape.threads, sm2, st>>>(a);
+    RAFT_CUDA(cudaGetLastError());
+}
+
+}  // namespace raft

@@ -348,6 +348,53 @@ void fbp_host_slab(const FbpConfig &cfg, int device, float *obj, const float *to
     check_device_flag(tb.err, "FBP");
 }
 
+// ------------------------------------------------------------------ BST --
+// getBSTGPU (bst.cu:534-642): slices stream through the two-slot pipeline;
+// each chunk runs the three BST kernels (bst.cu in this library).
+static int bst_chunk_slices(const BstPlanShape &sh, int nslices, int blocksize)
+{
+    // keep the per-chunk workspace near 4 GB (polar rows + crop columns)
+    const size_t per = bst_workspace_bytes(sh, 1);
+    int c = (int)std::max<size_t>(1, ((size_t)4 << 30) / std::max<size_t>(per, 1));
+    c = std::min(c, 32);
+    if (blocksize > 0) c = std::min(c, blocksize);
+    return std::max(1, std::min(c, nslices));
+}
+
+void bst_host_slab(const FbpConfig &cfg, int device, float *obj, const float *tomo, int nslices)
+{
+    if (nslices <= 0) return;
+    BstPlanShape sh;
+    RAFT_CHECK(bst_plan_shape(sh, cfg.nrays, cfg.nangles, cfg.pad),
+               "BST: the padded length N*(1+pad) must have only the prime factors 2, 3, 5, 7 and be at most 9472");
+    DeviceState &ds = device_state(device);
+    std::lock_guard<std::mutex> lk(ds.mtx);
+    RAFT_CUDA(cudaSetDevice(device));
+    ds.ensure();
+    const size_t in_ps = (size_t)cfg.nangles * cfg.nrays * sizeof(float);
+    const size_t out_ps = (size_t)cfg.nrays * cfg.nrays * sizeof(float);
+    const int chunk = bst_chunk_slices(sh, nslices, cfg.blocksize);
+    void *ws = ds.rows.get(bst_workspace_bytes(sh, chunk));
+    run_pipeline(ds, nslices, chunk, in_ps, out_ps, tomo, obj, [&](void *din, void *dout, int ns, cudaStream_t st) {
+        launch_bst(device, cfg, (const float *)din, (float *)dout, ns, ws, st);
+    });
+}
+
+void bst_device(const FbpConfig &cfg, int device, float *d_obj, const float *d_tomo, int nslices, cudaStream_t st)
+{
+    BstPlanShape sh;
+    RAFT_CHECK(bst_plan_shape(sh, cfg.nrays, cfg.nangles, cfg.pad),
+               "BST: the padded length N*(1+pad) must have only the prime factors 2, 3, 5, 7 and be at most 9472");
+    DeviceState &ds = device_state(device);
+    const int chunk = bst_chunk_slices(sh, nslices, cfg.blocksize);
+    void *ws = ds.rows.get(bst_workspace_bytes(sh, chunk));
+    const size_t tps = (size_t)cfg.nangles * cfg.nrays, ops = (size_t)cfg.nrays * cfg.nrays;
+    for (int s0 = 0; s0 < nslices; s0 += chunk) {
+        const int ns = std::min(chunk, nslices - s0);
+        launch_bst(device, cfg, d_tomo + tps * s0, d_obj + ops * s0, ns, ws, st);
+    }
+}
+
 // -------------------------------------------------------------- lowpass --
 void lowpass_host_slab(const FbpConfig &cfg, int device, float *tomo, int nslices)
 {

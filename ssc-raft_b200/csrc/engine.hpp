@@ -86,6 +86,9 @@ void fbp_host_slab(const FbpConfig &cfg, int device, float *obj, const float *to
                    int nslices);
 
 // --- lowpass -------------------------------------------------------------
+void bst_host_slab(const FbpConfig &cfg, int device, float *obj, const float *tomo, int nslices);
+// Device-resident BST on st (caller holds the device lock).
+void bst_device(const FbpConfig &cfg, int device, float *d_obj, const float *d_tomo, int nslices, cudaStream_t st);
 void lowpass_host_slab(const FbpConfig &cfg, int device, float *tomo, int nslices);
 void background_host_slab(int device, float *frames, const float *flat, const float *dark, int nrays, int nangles,
                           int nslices, int numflats, int is_log, int blocksize);

@@ -1,0 +1,213 @@
+// fft.cuh -- the self-sorting (Stockham) mixed-radix complex FFT shared by the
+// filter, BST and rotation-axis kernels.
+//
+// A CTA transforms one length-n sequence held in shared memory, ping-ponging
+// between two buffers; radices 2, 3, 4, 5, 7, 8 (lengths whose other prime
+// factors are rejected on the host).  Twiddles exp(-2 pi i k / n) come from a
+// table built in FP64 on the host.  Only the forward transform exists: an
+// inverse is the forward transform of the conjugate, conjugated.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+namespace raft {
+
+// ---------------------------------------------------------------- host --
+// Radices of n, largest first among the powers of two; false if n has a prime
+// factor above 7 or needs more than 24 passes.
+static inline bool factorize(int n, int *radix, int &nradix)
+{
+    nradix = 0;
+    int e2 = 0;
+    while (n % 2 == 0) { n /= 2; e2++; }
+    while (e2 >= 3) { radix[nradix++] = 8; e2 -= 3; }
+    if (e2 == 2) radix[nradix++] = 4;
+    if (e2 == 1) radix[nradix++] = 2;
+    for (int p : {3, 5, 7})
+        while (n % p == 0) { n /= p; radix[nradix++] = p; }
+    return n == 1 && nradix <= 24;
+}
+
+// exp(-2 pi i k / n), k < n, rounded from FP64.
+static inline std::vector<float2> fft_twiddles(int n)
+{
+    std::vector<float2> tw(n);
+    for (int k = 0; k < n; k++) {
+        const double a = -2.0 * M_PI * (double)k / (double)n;
+        tw[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    return tw;
+}
+
+// Threads per CTA for one length-n transform: about 8 butterflies of the
+// smallest radix per thread, 128..512 threads.
+static inline int fft_threads(int n)
+{
+    int T = ((n / 16 + 31) / 32) * 32;
+    return T < 128 ? 128 : (T > 512 ? 512 : T);
+}
+
+// -------------------------------------------------------------- device --
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// multiply by -i
+__device__ __forceinline__ float2 cmni(float2 a) { return make_float2(a.y, -a.x); }
+
+// forward DFTs (exp(-2 pi i rq/R)) on registers
+template <int R> struct Dft;
+
+template <> struct Dft<2> {
+    static __device__ __forceinline__ void run(float2 *v)
+    {
+        float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    }
+};
+template <> struct Dft<4> {
+    static __device__ __forceinline__ void run(float2 *v)
+    {
+        float2 s0 = cadd(v[0], v[2]), d0 = csub(v[0], v[2]);
+        float2 s1 = cadd(v[1], v[3]), d1 = cmni(csub(v[1], v[3]));
+        v[0] = cadd(s0, s1);
+        v[2] = csub(s0, s1);
+        v[1] = cadd(d0, d1);
+        v[3] = csub(d0, d1);
+    }
+};
+template <> struct Dft<8> {
+    static __device__ __forceinline__ void run(float2 *v)
+    {
+        const float r = 0.70710678118654752f;
+        float2 e[4] = {v[0], v[2], v[4], v[6]};
+        float2 o[4] = {v[1], v[3], v[5], v[7]};
+        Dft<4>::run(e);
+        Dft<4>::run(o);
+        // twiddles exp(-2 pi i k/8), k = 0..3
+        float2 t1 = make_float2(r * (o[1].x + o[1].y), r * (o[1].y - o[1].x));
+        float2 t2 = cmni(o[2]);
+        float2 t3 = make_float2(r * (o[3].y - o[3].x), -r * (o[3].x + o[3].y));
+        v[0] = cadd(e[0], o[0]);
+        v[4] = csub(e[0], o[0]);
+        v[1] = cadd(e[1], t1);
+        v[5] = csub(e[1], t1);
+        v[2] = cadd(e[2], t2);
+        v[6] = csub(e[2], t2);
+        v[3] = cadd(e[3], t3);
+        v[7] = csub(e[3], t3);
+    }
+};
+// odd radices: direct sum with constant roots cos/sin(2 pi m / R)
+template <int R> struct Roots;
+template <> struct Roots<3> {
+    static __device__ __forceinline__ float c(int m) { return m == 0 ? 1.f : -0.5f; }
+    static __device__ __forceinline__ float s(int m) { return m == 0 ? 0.f : (m == 1 ? 0.86602540378443865f : -0.86602540378443865f); }
+};
+template <> struct Roots<5> {
+    static __device__ __forceinline__ float c(int m)
+    {
+        return m == 0 ? 1.f : (m == 1 || m == 4) ? 0.30901699437494745f : -0.80901699437494742f;
+    }
+    static __device__ __forceinline__ float s(int m)
+    {
+        return m == 0 ? 0.f : m == 1 ? 0.95105651629515357f : m == 2 ? 0.58778525229247314f
+             : m == 3 ? -0.58778525229247314f : -0.95105651629515357f;
+    }
+};
+template <> struct Roots<7> {
+    static __device__ __forceinline__ float c(int m)
+    {
+        return m == 0 ? 1.f : (m == 1 || m == 6) ? 0.62348980185873353f
+             : (m == 2 || m == 5) ? -0.22252093395631440f : -0.90096886790241913f;
+    }
+    static __device__ __forceinline__ float s(int m)
+    {
+        return m == 0 ? 0.f : m == 1 ? 0.78183148246802981f : m == 2 ? 0.97492791218182361f
+             : m == 3 ? 0.43388373911755812f : m == 4 ? -0.43388373911755812f
+             : m == 5 ? -0.97492791218182361f : -0.78183148246802981f;
+    }
+};
+template <int R> struct DftOdd {
+    static __device__ __forceinline__ void run(float2 *v)
+    {
+        float2 in[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) in[r] = v[r];
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+            float2 acc = in[0];
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                const int m = (r * q) % R;
+                // exp(-2 pi i m / R) = c(m) - i s(m)
+                const float c = Roots<R>::c(m), s = Roots<R>::s(m);
+                acc.x += in[r].x * c + in[r].y * s;
+                acc.y += in[r].y * c - in[r].x * s;
+            }
+            v[q] = acc;
+        }
+    }
+};
+template <> struct Dft<3> { static __device__ __forceinline__ void run(float2 *v) { DftOdd<3>::run(v); } };
+template <> struct Dft<5> { static __device__ __forceinline__ void run(float2 *v) { DftOdd<5>::run(v); } };
+template <> struct Dft<7> { static __device__ __forceinline__ void run(float2 *v) { DftOdd<7>::run(v); } };
+
+// One Stockham pass of radix R from src to dst (both Np complex values in
+// shared memory).  Only one butterfly's R values are live per thread.
+template <int R>
+__device__ __noinline__ void fft_pass(const float2 *__restrict__ src, float2 *__restrict__ dst, int Np,
+                                      int Ns, const float2 *__restrict__ tw)
+{
+    const int nb = Np / R;
+    const int twstep = Np / (Ns * R);
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+        const int k = j % Ns;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            float2 x = src[j + r * nb];
+            if (r > 0 && k > 0) x = cmul(x, __ldg(&tw[r * k * twstep]));
+            v[r] = x;
+        }
+        Dft<R>::run(v);
+        const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) dst[base + r * Ns] = v[r];
+    }
+    __syncthreads();
+}
+
+struct RadixList {
+    int n;
+    int r[24];
+};
+
+// Forward FFT of a[0..Np); the result ends in a or b, which is returned.
+__device__ __forceinline__ float2 *fft_forward(float2 *a, float2 *b, int Np, const RadixList &rl,
+                                               const float2 *tw)
+{
+    int Ns = 1;
+    for (int p = 0; p < rl.n; p++) {
+        switch (rl.r[p]) {
+        case 2: fft_pass<2>(a, b, Np, Ns, tw); break;
+        case 3: fft_pass<3>(a, b, Np, Ns, tw); break;
+        case 4: fft_pass<4>(a, b, Np, Ns, tw); break;
+        case 5: fft_pass<5>(a, b, Np, Ns, tw); break;
+        case 7: fft_pass<7>(a, b, Np, Ns, tw); break;
+        default: fft_pass<8>(a, b, Np, Ns, tw); break;
+        }
+        Ns *= rl.r[p];
+        float2 *t = a; a = b; b = t;
+    }
+    return a;
+}
+
+
+}  // namespace raft

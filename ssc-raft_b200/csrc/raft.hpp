@@ -88,6 +88,8 @@ struct FilterPlan {
 bool build_filter_plan(FilterPlan &plan, int geometry, int ftype, int N, int pad, double paganin,
                        double reg, double offset, double pixel, int device);
 void release_filter_plan(FilterPlan &plan);
+// Filter::apply of the reference (filters.cu:395-438) at weight w, in FP64.
+double filter_apply_ref(int type, double w, double paganin, double reg);
 void filter_spectrum_host(int geometry, int ftype, int Np, double paganin, double reg,
                           double offset, double pixel, double *hre, double *him);
 
@@ -239,6 +241,22 @@ struct FbpConfig {
     int geometry = GEOM_FBP_REF;   // GEOM_FBP_REF or GEOM_FBP_LIN
     int store = STORE_F32;
 };
+
+// --- BST (backprojection slice theorem) ------------------------------------
+struct BstPlanShape {
+    int N = 0, A = 0, Np = 0, L = 0, Lh = 0, S = 0, off = 0, threads = 0;
+};
+// Sizes of the BST transforms for N rays, A angles, padding pad; false when
+// the padded length N*(1+pad) has a prime factor above 7 or exceeds the
+// shared-memory limit of the row kernel (3 complex rows of Np).
+bool bst_plan_shape(BstPlanShape &s, int N, int A, int pad);
+// Device workspace bytes for nslices slices at once.
+size_t bst_workspace_bytes(const BstPlanShape &s, int nslices);
+// BST reconstruction of nslices slices (d_tomo [nslices][A][N] -> d_obj
+// [nslices][N][N]) on st; cfg gives N, A, pad, filter, paganin, reg, axis
+// offset, pixel.
+void launch_bst(int device, const FbpConfig &cfg, const float *d_tomo, float *d_obj, int nslices, void *workspace,
+                cudaStream_t st);
 
 // EM configuration (setEMRTParameters, parameters.cu:8-59).
 struct EmConfig {

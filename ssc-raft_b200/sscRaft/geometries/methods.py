@@ -8,8 +8,9 @@ import numpy
 
 def fbp(tomogram, angles=None, obj=None, dic=None, nstreams=0, **kwargs):
     """Filtered backprojection of a parallel-beam tomogram [slices, angles, rays].
-    Same dictionary and defaults as the reference (methods.py:54-56); method
-    'RT' only."""
+    Same dictionary and defaults as the reference (methods.py:54-56); methods
+    'RT' (ray-traced backprojection) and 'BST' (backprojection slice theorem,
+    uniform angles over [0, pi) assumed)."""
     required = ('gpu',)
     optional = ('filter', 'rotation axis offset', 'padding', 'regularization', 'beta/delta',
                 'blocksize', 'energy[eV]', 'z2[m]', 'method', 'detectorPixel[m]')

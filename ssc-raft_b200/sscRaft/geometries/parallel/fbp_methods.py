@@ -67,5 +67,40 @@ def fbpGPU(tomogram, angles, gpus, dic, obj=None):
 
 
 def bstGPU(tomogram, angles, gpus, dic, obj=None, nstreams=0):
-    """FBP by the Backprojection Slice Theorem: not provided by this library."""
-    raise NotImplementedError("bstGPU (method='BST') is outside this library's scope; use method='RT'")
+    """FBP by the Backprojection Slice Theorem (fbp_methods.py:105-205 of the
+    reference): same dictionary as fbpGPU; the rotation axis offset is
+    truncated to an integer and the angles must be uniform over [0, pi)
+    (fbp() passes linspace(0, pi, A, endpoint=False)).  The padded length
+    N*(1+padding) must have only the prime factors 2, 3, 5, 7 (and be at most
+    9472).  Returns obj [slices, N, N] (written in place when given)."""
+    gpus_arr, ngpus = _gpus(gpus)
+    nrays = tomogram.shape[-1]
+    nangles = tomogram.shape[-2]
+    nslices = 1 if len(tomogram.shape) == 2 else tomogram.shape[0]
+    filter_type = FilterNumber(dic['filter'])
+    beta_delta = dic['beta/delta']
+    regularization = dic['regularization']
+    offset = int(dic['rotation axis offset'])
+    blocksize = dic['blocksize']
+    energy = dic['energy[eV]']
+    z2 = dic['z2[m]']
+    pixelx, pixely = dic['detectorPixel[m]'], dic['detectorPixel[m]']
+    if beta_delta != 0.0:
+        beta_delta = 1.0 / beta_delta
+    else:
+        beta_delta, z2, energy = 0.0, 0.0, 1.0
+    padx, pady, padz = dic['padding'], 0, 0
+    objsize = nrays
+    tomogram = CNICE(tomogram)
+    if obj is None:
+        obj = numpy.zeros([nslices, objsize, objsize], dtype=numpy.float32)
+    obj = CNICE(obj)
+    angles = CNICE(numpy.array(angles))
+    param_int = CNICE(numpy.array([nrays, nangles, nslices, objsize, padx, pady, padz, filter_type, 0,
+                                   blocksize]), numpy.int32)
+    param_float = CNICE(numpy.array([beta_delta, regularization, energy, z2, pixelx, pixely, offset]),
+                        numpy.float32)
+    libraft.getBSTMultiGPU(_ptr(gpus_arr), ngpus, _ptr(obj), _ptr(tomogram), _ptr(angles), _ptr(param_float),
+                           _ptr(param_int), int(nstreams))
+    check_error("bstGPU")
+    return obj

@@ -39,6 +39,7 @@ def load_ref():
     lib.get_tEM_RT_MultiGPU.argtypes = [P, I, P, P, P, P, P, P]
     lib.get_eEM_RT_MultiGPU.argtypes = [P, I, P, P, P, P, P]
     lib.getBackgroundCorrectionMultiGPU.argtypes = [P, I, P, P, P, I, I, I, I, I, I]
+    lib.getBSTMultiGPU.argtypes = [P, I, P, P, P, P, P, I]
     return lib
 
 
@@ -108,11 +109,49 @@ def background_case(lib, B, A, N, nflats, is_log, seed):
     return dict(kind="background", frames=frames, flat=flat, dark=dark, is_log=is_log, out=out)
 
 
+# BST cases (name, N, nslices, pad, ftype, integer offset, reg); nangles == N, the
+# setting in which the reference's padding call (sized by N rows) covers every row.
+BST_CASES = [
+    ("bst_ramp_n64", 64, 2, 2, 7, 0, 0.0),
+    ("bst_hann_off2_n96", 96, 1, 2, 5, 2, 0.0),
+    ("bst_none_pad1_n64", 64, 1, 1, 0, 0, 0.0),
+    ("bst_gauss_n80", 80, 1, 2, 1, -1, 2.0),
+]
+
+
+def bst_case(lib, name, N, B, pad, ftype, offset, reg, seed):
+    """One BST case through the reference's getBSTMultiGPU.  Run in a fresh
+    process: the reference zero-pads its half-rays with freshly allocated,
+    never-cleared device memory, which a new process receives zeroed."""
+    A = N
+    ang = np.linspace(0.0, np.pi, A, endpoint=False).astype(np.float32)
+    sino, _ = sino_case(N, A, B, seed=seed, angles=ang)
+    pf, pi = fbp_params(N, A, B, pad=pad, ftype=ftype, offset=float(offset), reg=reg)
+    obj = np.zeros((B, N, N), np.float32)
+    t = sino.copy()
+    lib.getBSTMultiGPU(ptr(GPUS), 1, ptr(obj), ptr(t), ptr(ang), ptr(pf), ptr(pi), 0)
+    return dict(kind="bst", sino=sino, angles=ang, paramf=pf, parami=pi, out=obj)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--only", default="")
+    ap.add_argument("--bst-case", default="", help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.bst_case:
+        i = [c[0] for c in BST_CASES].index(args.bst_case)
+        d = bst_case(load_ref(), *BST_CASES[i], seed=800 + i)
+        np.savez_compressed(os.path.join(args.out, f"ref_{args.bst_case}.npz"), **d)
+        return
+    if args.only.startswith("bst"):
+        import subprocess
+        for c in BST_CASES:
+            if c[0].startswith(args.only):
+                subprocess.run([sys.executable, os.path.abspath(__file__), "--out", args.out, "--bst-case", c[0]],
+                               check=True)
+        print("wrote", len([c for c in BST_CASES if c[0].startswith(args.only)]), "BST fixtures to", args.out)
+        return
     os.makedirs(args.out, exist_ok=True)
     lib = load_ref()
     cases = {}

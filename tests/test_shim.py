@@ -76,8 +76,14 @@ def test_fbp_defaults_and_filter_names(fake):
     np.testing.assert_allclose(pf, [0, 0, 1, 0, 1, 1, 0])      # beta/delta 0 -> z2 0, energy 1
     with pytest.raises(ValueError):
         sscRaft.fbp(t, dic={"angles[rad]": np.zeros(10)})     # 'gpu' is required
-    with pytest.raises(NotImplementedError):
-        sscRaft.fbp(t, dic={"gpu": [0], "method": "BST"})
+    # BST: the reference packing (bstGPU, fbp_methods.py:152-201), offset truncated to an integer
+    sscRaft.fbp(np.zeros((2, 10, 16), np.float32), dic={"gpu": [0], "method": "BST", "filter": "hann",
+                                                         "rotation axis offset": 2.7, "padding": 1})
+    name, a = fake.calls[-1]
+    assert name == "getBSTMultiGPU" and a[7] == 0
+    assert list(arr(a[6], 10, ctypes.c_int32)) == [16, 10, 2, 16, 1, 0, 0, 5, 0, 0]
+    np.testing.assert_allclose(arr(a[5], 7, ctypes.c_float), [0, 0, 1, 0, 1, 1, 2.0])
+    np.testing.assert_allclose(arr(a[4], 10, ctypes.c_float), np.linspace(0, np.pi, 10, endpoint=False), rtol=1e-6)
 
 
 def test_fbp_extension_keys(fake):
