@@ -29,6 +29,9 @@
 #ifndef RAFT_B200_H
 #define RAFT_B200_H
 
+#include <stddef.h>
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -61,6 +64,35 @@ void get_tEM_RT_MultiGPU(int *gpus, int ngpus, float *obj, float *count, float *
  * Replaces get_eEM_RT_MultiGPU, em_rt.cu:201-262 (rafttypes.py:138-147). */
 void get_eEM_RT_MultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *angles,
                          float *paramf, int *parami);
+
+/* Rotation-axis offset from the 0 and 180 degree frames [sizey][sizex] (host arrays) by
+ * phase correlation, the reference's integer / sub-pixel searches (their candidate sets kept
+ * as they are), on the calling thread's current device.  Frame sides must have only the
+ * prime factors 2, 3, 5, 7.  Errors via raft_last_error (result 0).
+ * Replace findcentersino / findcentersino_subpixel / findcentersino16,
+ * cuda/src/processing/rotation_axis.cu:429-451 (rafttypes.py:201-219). */
+int findcentersino(float *frame0, float *frame180, float *dark, float *flat, int sizex, int sizey);
+float findcentersino_subpixel(float *frame0, float *frame180, float *dark, float *flat, int sizex, int sizey);
+int findcentersino16(uint16_t *frame0, uint16_t *frame180, uint16_t *dark, uint16_t *flat, int sizex,
+                     int sizey);
+
+/* findcentersino(_subpixel) on device frames of one GPU; *result gets the offset.
+ * NULL stream as raft_fbp_device.  Returns 0 on success. */
+int raft_centersino_device(int gpu, const float *d_frame0, const float *d_frame180, const float *d_dark,
+                           const float *d_flat, int sizex, int sizey, int subpixel, double *result, void *stream);
+
+/* Sub-pixel rotation-axis correction in place: every row edge-padded to 3 nrays, shifted by
+ * axis_offset samples with a Fourier phase ramp, cropped back.
+ * Replaces getRotAxisCorrectionMultiGPU, cuda/src/processing/rotation_axis.cu:591-643
+ * (rafttypes.py:233-241). */
+void getRotAxisCorrectionMultiGPU(int *gpus, int ngpus, float *tomogram, float axis_offset, int nrays,
+                                  int nangles, int nslices, int blocksize);
+
+/* Integer shift of every row by `deviation` samples (right if positive) with zero fill,
+ * on the host; tomoout may equal tomoin.  Replaces correctRotationAxis,
+ * cuda/src/processing/rotation_axis.cu:396-426 (whose ctypes binding in rafttypes.py:222-231
+ * declares one pointer too few; this library binds both). */
+void correctRotationAxis(float *tomoin, float *tomoout, int sizex, int sizey, int sizez, int deviation);
 
 /* FBP by the backprojection slice theorem (Fourier regridding), packing as getFBPMultiGPU
  * (object N x N).  Angles are taken as uniform over [0, pi), as the reference's regridding

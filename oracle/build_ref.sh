@@ -1,6 +1,6 @@
 #!/usr/bin/env bash
 # Builds the reference ssc-raft CUDA library (parallel-beam FBP / EM / Radon /
-# lowpass / flat-dark / BST path only) from its own sources, for sm_100a, into oracle/_ref/.
+# lowpass / flat-dark / BST / rotation-axis path only) from its own sources, for sm_100a, into oracle/_ref/.
 #
 # The reference is compiled where it lies (read-only tree); nothing is copied
 # into this repository.  Flags follow the reference CMakeLists.txt:8-17
@@ -29,6 +29,7 @@ SRCS=(
   cuda/src/processing/filters/filters.cu
   cuda/src/processing/filters/low_pass.cu
   cuda/src/processing/background_correction.cu
+  cuda/src/processing/rotation_axis.cu
   cuda/src/geometries/parallel/reconstruction_methods/parameters.cu
   cuda/src/geometries/parallel/reconstruction_methods/fbp.cu
   cuda/src/geometries/parallel/reconstruction_methods/bst.cu

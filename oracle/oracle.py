@@ -62,6 +62,9 @@ def lib():
         _lib.oracle_conv3x3_dgrad.argtypes = [P, P, P, I, I, I, I, I]
         _lib.oracle_background.argtypes = [P, P, P, I, I, I, I, I, P]
         _lib.oracle_bst.argtypes = [P, I, I, I, I, I, D, D, I, F, P]
+        _lib.oracle_centersino.argtypes = [P, P, P, P, I, I, I]
+        _lib.oracle_centersino.restype = D
+        _lib.oracle_rotaxis.argtypes = [P, I, I, F, P]
     return _lib
 
 
@@ -277,3 +280,21 @@ def bst(tomo, ftype, pad, paganin=0.0, reg=0.0, offset=0, pixel=1.0):
     lib().oracle_bst(_p(t), N, A, B, int(pad), int(ftype), float(paganin), float(reg), int(offset), float(pixel),
                      _p(out))
     return out if np.ndim(tomo) == 3 else out[0]
+
+
+def centersino(frame0, frame180, dark, flat, subpixel=False):
+    """Rotation-axis offset by phase correlation (rotation_axis.cu:14-46,221-360):
+    the reference's integer (int) or sub-pixel (float) result."""
+    fr = [_f32(a) for a in (frame0, frame180, dark, flat)]
+    sy, sx = fr[0].shape
+    v = lib().oracle_centersino(*[_p(a) for a in fr], sx, sy, int(bool(subpixel)))
+    return float(v) if subpixel else int(v)
+
+
+def rotaxis(tomo, offset):
+    """Sub-pixel axis shift of every row (rotation_axis.cu:455-526); FP64 result."""
+    t = _f32(tomo)
+    N = t.shape[-1]
+    out = np.empty(t.shape, np.float64)
+    lib().oracle_rotaxis(_p(t), N, int(t.size // N), float(offset), _p(out))
+    return out

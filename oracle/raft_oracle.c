@@ -706,3 +706,155 @@ void oracle_bst(const float *tomo, int N, int A, int B, int pad, int ftype, doub
     }
     free(G); free(rfwd); free(rinv);
 }
+
+/* 2-D transform in place of a [ny][nx] complex array: rows, then columns. */
+static void fft2_inplace(cplx *d, int nx, int ny, int sign)
+{
+    cplx *rx = make_roots(nx, sign), *ry = make_roots(ny, sign);
+    cplx *a = (cplx *)malloc(sizeof(cplx) * (size_t)(nx > ny ? nx : ny));
+    cplx *b = (cplx *)malloc(sizeof(cplx) * (size_t)(nx > ny ? nx : ny));
+    int m = nx > ny ? nx : ny;
+    cplx *scratch = (cplx *)malloc(sizeof(cplx) * (size_t)(2 * m + 8));
+    for (int y = 0; y < ny; y++) {
+        fft(nx, d + (size_t)y * nx, b, rx, scratch);
+        memcpy(d + (size_t)y * nx, b, sizeof(cplx) * nx);
+    }
+    for (int x = 0; x < nx; x++) {
+        for (int y = 0; y < ny; y++) a[y] = d[(size_t)y * nx + x];
+        fft(ny, a, b, ry, scratch);
+        for (int y = 0; y < ny; y++) d[(size_t)y * nx + x] = b[y];
+    }
+    free(rx); free(ry); free(a); free(b); free(scratch);
+}
+
+/* Rotation-axis offset by phase correlation: getCentersino / getCentersino_subpixel
+ * (rotation_axis.cu:14-46,221-360): transforms in FP64, the correlation then
+ * rounded to float and searched exactly as the reference's host loops do
+ * (float |c|^2, the integer search over x = 0, 4, ... then the remainder, the
+ * sub-pixel search over x = i * 0.01 with abs2InterpCubic's float weights). */
+double oracle_centersino(const float *frame0, const float *frame180, const float *dark, const float *flat,
+                         int sizex, int sizey, int subpixel)
+{
+    size_t plane = (size_t)sizex * sizey;
+    cplx *F = (cplx *)malloc(sizeof(cplx) * plane), *G = (cplx *)malloc(sizeof(cplx) * plane);
+    for (int y = 0; y < sizey; y++)
+        for (int x = 0; x < sizex; x++) {
+            size_t i = (size_t)y * sizex + x;
+            double dk = dark[i], ft = flat[i], q = fmax(ft - dk, 0.5);
+            F[i] = -log(fmax(frame0[i] - dk, 0.5) / q);
+            G[(size_t)y * sizex + (sizex - 1 - x)] = -log(fmax(frame180[i] - dk, 0.5) / q);
+        }
+    fft2_inplace(F, sizex, sizey, -1);
+    fft2_inplace(G, sizex, sizey, -1);
+    for (int y = 0; y < sizey; y++)
+        for (int x = 0; x < sizex; x++) {
+            size_t i = (size_t)y * sizex + x;
+            double xx = fmin((double)(sizex - x), (double)x) / sizex;
+            double yy = fmin((double)(sizey - y), (double)y) / sizey;
+            double gauss = exp(-20.0 * (xx * xx + yy * yy));
+            cplx fg = F[i] * conj(G[i]);
+            F[i] = fg * gauss / cabs(fg);
+        }
+    fft2_inplace(F, sizex, sizey, +1);
+    float *re = (float *)malloc(sizeof(float) * plane), *im = (float *)malloc(sizeof(float) * plane);
+    for (size_t i = 0; i < plane; i++) { re[i] = (float)creal(F[i]); im[i] = (float)cimag(F[i]); }
+#define ABS2(i) (re[i] * re[i] + im[i] * im[i])
+    float maxx = 0.0f;
+    double result;
+    if (!subpixel) {
+        int posx = 0;
+        int irange = (sizex >> 2) << 2;
+        for (int j = 0; j < sizey; j++) {
+            for (int i = 0; i < irange; i += 4) {
+                float bbs = ABS2((size_t)j * sizex + i);
+                if (bbs > maxx) { maxx = bbs; posx = i; }
+            }
+            for (int i = irange; i < sizex; i++) {
+                float bbs = ABS2((size_t)j * sizex + i);
+                if (bbs > maxx) { maxx = bbs; posx = i; }
+            }
+        }
+        if (posx > (float)sizex / 2) posx -= sizex;
+        result = (double)(-posx / 2);
+    } else {
+        float bestpos = 0.0f;
+        const float di = 0.01f;
+        for (int j = 0; j < sizey; j++)
+            for (float i = 0; i < (float)sizex; i++) {
+                float posx = i * di, posy = (float)j;
+                int x0 = (int)floorf(posx), y0 = (int)floorf(posy);
+                int x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, y1 = y0 + 1, y2 = y0 + 2, y3 = y0 + 3;
+                int xs[4] = {x0, x1, x2, x3}, ys[4] = {y0, y1, y2, y3};
+                float v[4][4];
+                for (int a = 0; a < 4; a++)
+                    for (int b = 0; b < 4; b++)
+                        v[a][b] = (ys[a] >= 0 && ys[a] < sizey && xs[b] >= 0 && xs[b] < sizex)
+                                      ? ABS2((size_t)ys[a] * sizex + xs[b]) : 0.0f;
+                /* abs2InterpCubic (rotation_axis.cu:155-220): term order v00, v10, v20, v30, v01, ... */
+                float s = 0.0f;
+                int first = 1;
+                for (int b = 0; b < 4; b++)
+                    for (int a = 0; a < 4; a++) {
+                        float num = 1.0f;
+                        int den = 1;
+                        int firstf = 1;
+                        for (int m = 0; m < 4; m++)
+                            if (m != b) {
+                                float t = (float)xs[m] - posx;
+                                num = firstf ? t : num * t;
+                                firstf = 0;
+                                den *= xs[m] - xs[b];
+                            }
+                        for (int m = 0; m < 4; m++)
+                            if (m != a) {
+                                num = num * ((float)ys[m] - posy);
+                                den *= ys[m] - ys[a];
+                            }
+                        float term = (num / (float)den) * v[a][b];
+                        s = first ? term : s + term;
+                        first = 0;
+                    }
+                if (s > maxx) { maxx = s; bestpos = i * di; }
+            }
+        if (bestpos > (float)sizex / 2.0f) bestpos -= (float)sizex;
+        result = (double)(-bestpos / 2.0f);
+    }
+#undef ABS2
+    free(F); free(G); free(re); free(im);
+    return result;
+}
+
+/* getRotAxisCorrection (rotation_axis.cu:455-526): rows edge-padded to Np = 3N,
+ * R2C, times exp(-i 2 pi / (2M - 2) offset k) with M = Np/2 + 1 (the Nyquist bin
+ * of an even Np keeps only the real part, as C2R reads it), C2R, / Np, centre crop. */
+void oracle_rotaxis(const float *tomo, int nrays, int nrows, float offset, double *out)
+{
+    int pad = 2, Np = nrays * (1 + pad), off = (pad * nrays) / 2, M = Np / 2 + 1;
+    cplx *H = (cplx *)malloc(sizeof(cplx) * Np);
+    for (int k = 0; k < Np; k++) {
+        int kk = k <= Np / 2 ? k : Np - k;
+        double ph = 2.0 * PI_D / (double)(2 * M - 2) * (double)offset * kk;
+        double re = cos(ph), im = -sin(ph);
+        if (k > Np / 2) im = -im;
+        if (Np % 2 == 0 && k == Np / 2) im = 0.0;
+        H[k] = (re + I * im) / (double)Np;
+    }
+    cplx *rf = make_roots(Np, -1), *ri = make_roots(Np, +1);
+#pragma omp parallel
+    {
+        double *row = (double *)malloc(sizeof(double) * Np);
+        cplx *a = (cplx *)malloc(sizeof(cplx) * Np), *b = (cplx *)malloc(sizeof(cplx) * Np);
+        cplx *scratch = (cplx *)malloc(sizeof(cplx) * (size_t)(2 * Np + 8));
+#pragma omp for
+        for (int r = 0; r < nrows; r++) {
+            pad_row(tomo + (size_t)r * nrays, nrays, pad, Np, row);
+            for (int i = 0; i < Np; i++) a[i] = row[i];
+            fft(Np, a, b, rf, scratch);
+            for (int k = 0; k < Np; k++) b[k] *= H[k];
+            fft(Np, b, a, ri, scratch);
+            for (int i = 0; i < nrays; i++) out[(size_t)r * nrays + i] = creal(a[off + i]);
+        }
+        free(row); free(a); free(b); free(scratch);
+    }
+    free(H); free(rf); free(ri);
+}

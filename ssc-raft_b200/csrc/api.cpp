@@ -184,6 +184,32 @@ bool check_gpu_id(int gpu) { return check_gpus(&gpu, 1); }
 
 using namespace raft;
 
+template <typename T>
+static double centersino_entry(const T *frame0, const T *frame180, const T *dark, const T *flat, int sizex, int sizey,
+                               int subpixel, const char *name)
+{
+    clear_error();
+    if (!frame0 || !frame180 || !dark || !flat) {
+        set_error(std::string(name) + ": null frame pointer");
+        return 0.0;
+    }
+    if (!centersino_shape_ok(sizex, sizey)) {
+        set_error(std::string(name) + ": frame sides must have only the prime factors 2, 3, 5, 7 (at most 14528)");
+        return 0.0;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        dev = 0;
+    }
+    if (!check_gpu_id(dev)) return 0.0;
+    try {
+        return centersino_host<T>(dev, frame0, frame180, dark, flat, sizex, sizey, subpixel);
+    } catch (const CudaFail &) {
+    }
+    return 0.0;
+}
+
 extern "C" {
 
 int raft_last_error(char *buf, int len)
@@ -589,6 +615,92 @@ int raft_radon_device(int gpu, float *d_out, const float *d_phantom, const float
     } catch (const CudaFail &) {
     }
     return has_error() ? 1 : 0;
+}
+
+// --- rotation axis --------------------------------------------------------------
+// Reference: findcentersino / findcentersino_subpixel / findcentersino16,
+// cuda/src/processing/rotation_axis.cu:429-451 (host frames [sizey][sizex], the
+// calling thread's current device); getRotAxisCorrectionMultiGPU :591-643;
+// correctRotationAxis (host shift) :396-426.
+int findcentersino(float *frame0, float *frame180, float *dark, float *flat, int sizex, int sizey)
+{
+    return (int)centersino_entry<float>(frame0, frame180, dark, flat, sizex, sizey, 0, "findcentersino");
+}
+
+float findcentersino_subpixel(float *frame0, float *frame180, float *dark, float *flat, int sizex, int sizey)
+{
+    return (float)centersino_entry<float>(frame0, frame180, dark, flat, sizex, sizey, 1, "findcentersino_subpixel");
+}
+
+int findcentersino16(uint16_t *frame0, uint16_t *frame180, uint16_t *dark, uint16_t *flat, int sizex, int sizey)
+{
+    return (int)centersino_entry<uint16_t>(frame0, frame180, dark, flat, sizex, sizey, 0, "findcentersino16");
+}
+
+// Device-resident frames on `gpu`; *result receives the integer (subpixel = 0)
+// or sub-pixel (1) offset.  Returns 0 on success.
+int raft_centersino_device(int gpu, const float *d_frame0, const float *d_frame180, const float *d_dark,
+                           const float *d_flat, int sizex, int sizey, int subpixel, double *result, void *stream)
+{
+    clear_error();
+    if (!result || !centersino_shape_ok(sizex, sizey)) {
+        set_error("raft_centersino_device: null result or unsupported frame size");
+        return 1;
+    }
+    if (!check_gpus(&gpu, 1)) return 1;
+    try {
+        DeviceState &ds = device_state(gpu);
+        std::lock_guard<std::mutex> lk(ds.mtx);
+        RAFT_CUDA(cudaSetDevice(gpu));
+        ds.ensure();
+        cudaStream_t st = resolve_stream(ds, stream, ds.s_comp);
+        void *ws = ds.img[0].get(centersino_workspace_bytes(sizex, sizey));
+        *result = centersino_device<float>(gpu, d_frame0, d_frame180, d_dark, d_flat, sizex, sizey, subpixel ? 1 : 0,
+                                           ws, st);
+    } catch (const CudaFail &) {
+    }
+    return has_error() ? 1 : 0;
+}
+
+void getRotAxisCorrectionMultiGPU(int *gpus, int ngpus, float *tomogram, float axis_offset, int nrays, int nangles,
+                                  int nslices, int blocksize)
+{
+    clear_error();
+    if (nrays < 2 || nangles < 1 || nslices < 0) {
+        set_error("getRotAxisCorrectionMultiGPU: invalid sizes");
+        return;
+    }
+    if (!check_gpus(gpus, ngpus)) return;
+    if (!tomogram) {
+        set_error("null data pointer");
+        return;
+    }
+    const size_t ps = (size_t)nangles * nrays;
+    split_slabs(gpus, ngpus, nslices, [&](int dev, int start, int n) {
+        rotaxis_host_slab(dev, tomogram + ps * start, axis_offset, nrays, nangles, n, blocksize);
+    });
+}
+
+void correctRotationAxis(float *tomoin, float *tomoout, int sizex, int sizey, int sizez, int deviation)
+{
+    clear_error();
+    if (!tomoin || !tomoout || sizex < 0 || sizey < 0 || sizez < 0) {
+        set_error("correctRotationAxis: null pointer or negative size");
+        return;
+    }
+    const int offset = deviation < 0 ? -deviation : deviation;
+    for (size_t z = 0; z < (size_t)sizez; ++z)
+        for (size_t y = 0; y < (size_t)sizey; ++y) {
+            const float *in = tomoin + (z * sizey + y) * sizex;
+            float *out = tomoout + (z * sizey + y) * sizex;
+            if (deviation > 0) {            // shift right, zero fill (in place allowed)
+                for (int x = sizex - 1; x >= offset; --x) out[x] = in[x - offset];
+                for (int x = std::min(offset, sizex) - 1; x >= 0; --x) out[x] = 0.0f;
+            } else if (deviation < 0) {     // shift left
+                for (int x = 0; x < sizex - offset; ++x) out[x] = in[x + offset];
+                for (int x = std::max(sizex - offset, 0); x < sizex; ++x) out[x] = 0.0f;
+            }
+        }
 }
 
 // --- BST ------------------------------------------------------------------

@@ -348,6 +348,59 @@ void fbp_host_slab(const FbpConfig &cfg, int device, float *obj, const float *to
     check_device_flag(tb.err, "FBP");
 }
 
+// ------------------------------------------------------- rotation axis --
+// getRotAxisCorrectionGPU (rotation_axis.cu:529-589): each row is edge-padded
+// to 3N, shifted by a Fourier phase ramp and cropped back; the FBP filter's
+// lowpass output path with a phase-only spectrum does exactly that.
+void rotaxis_host_slab(int device, float *tomo, float axis_offset, int nrays, int nangles, int nslices,
+                       int blocksize)
+{
+    if (nslices <= 0) return;
+    DeviceState &ds = device_state(device);
+    std::lock_guard<std::mutex> lk(ds.mtx);
+    RAFT_CUDA(cudaSetDevice(device));
+    ds.ensure();
+    const int pad = 2;   // rotation_axis.cu:471
+    // pixel 1: the spectrum's normalisation is then 1/Np, as opt::scale divides by nrays
+    const FilterPlan &plan = cached_filter_plan(device, GEOM_FBP_REF, FILTER_AXIS_SHIFT, nrays, pad, 0.0, 0.0,
+                                                (double)axis_offset, 1.0);
+    const size_t ps = (size_t)nangles * nrays * sizeof(float);
+    const int chunk = auto_chunk(nslices, ps, blocksize);
+    run_pipeline(ds, nslices, chunk, ps, ps, tomo, tomo, [&](void *din, void *dout, int ns, cudaStream_t st) {
+        FilterLaunch fl;
+        fl.sino = (const float *)din;
+        fl.out = dout;
+        fl.nrows = ns * nangles;
+        fl.nangles = nangles;
+        fl.out_padded = 1;
+        launch_filter(plan, fl, st);
+    });
+}
+
+// Frames on the host -> the reference's integer or sub-pixel search result.
+template <typename T>
+double centersino_host(int device, const T *frame0, const T *frame1, const T *dark, const T *flat, int sizex,
+                       int sizey, int subpixel)
+{
+    DeviceState &ds = device_state(device);
+    std::lock_guard<std::mutex> lk(ds.mtx);
+    RAFT_CUDA(cudaSetDevice(device));
+    ds.ensure();
+    const size_t plane = (size_t)sizex * sizey;
+    T *d = (T *)ds.sino[0].get(4 * plane * sizeof(T));
+    cudaStream_t st = ds.s_comp;
+    const T *src[4] = {frame0, frame1, dark, flat};
+    for (int k = 0; k < 4; k++)
+        RAFT_CUDA(cudaMemcpyAsync(d + k * plane, src[k], plane * sizeof(T), cudaMemcpyHostToDevice, st));
+    void *ws = ds.img[0].get(centersino_workspace_bytes(sizex, sizey));
+    return centersino_device<T>(device, d, d + plane, d + 2 * plane, d + 3 * plane, sizex, sizey, subpixel, ws, st);
+}
+
+template double centersino_host<float>(int, const float *, const float *, const float *, const float *, int, int,
+                                       int);
+template double centersino_host<uint16_t>(int, const uint16_t *, const uint16_t *, const uint16_t *,
+                                          const uint16_t *, int, int, int);
+
 // ------------------------------------------------------------------ BST --
 // getBSTGPU (bst.cu:534-642): slices stream through the two-slot pipeline;
 // each chunk runs the three BST kernels (bst.cu in this library).

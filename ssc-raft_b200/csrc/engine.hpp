@@ -89,6 +89,11 @@ void fbp_host_slab(const FbpConfig &cfg, int device, float *obj, const float *to
 void bst_host_slab(const FbpConfig &cfg, int device, float *obj, const float *tomo, int nslices);
 // Device-resident BST on st (caller holds the device lock).
 void bst_device(const FbpConfig &cfg, int device, float *d_obj, const float *d_tomo, int nslices, cudaStream_t st);
+void rotaxis_host_slab(int device, float *tomo, float axis_offset, int nrays, int nangles, int nslices,
+                       int blocksize);
+template <typename T>
+double centersino_host(int device, const T *frame0, const T *frame1, const T *dark, const T *flat, int sizex,
+                       int sizey, int subpixel);
 void lowpass_host_slab(const FbpConfig &cfg, int device, float *tomo, int nslices);
 void background_host_slab(int device, float *frames, const float *flat, const float *dark, int nrays, int nangles,
                           int nslices, int numflats, int is_log, int blocksize);

@@ -95,6 +95,11 @@ void filter_spectrum_host(int geometry, int ftype, int Np, double paganin, doubl
         if (geometry == GEOM_FBP_LIN) {
             w = lin_apply(ftype, 2.0 * kk / (double)Np, paganin, reg);
             phase = 2.0 * M_PI * offset * kk / (double)Np;
+        } else if (ftype == FILTER_AXIS_SHIFT) {
+            // rot_axis_correction_kernel (rotation_axis.cu:455-465): pure phase,
+            // the same 2M-2 denominator; the inverse is divided by Np only
+            w = pixel;
+            phase = 2.0 * M_PI / (double)(2 * M - 2) * offset * kk;
         } else {
             const double tent = 0.5 * std::fmin((double)kk, (double)(M - kk)) / (double)M;
             w = ref_apply(ftype, tent, paganin, reg);

@@ -70,6 +70,9 @@ enum FilterType : int {
     FILTER_NONE = 0, FILTER_GAUSSIAN = 1, FILTER_LORENTZ = 2, FILTER_COSINE = 3,
     FILTER_RECTANGLE = 4, FILTER_HANN = 5, FILTER_HAMMING = 6, FILTER_RAMP = 7,
     FILTER_DIFFERENTIAL = 8, FILTER_SHEPP_LOGAN = 9,
+    // internal: weight 1 and normalisation 1/Np only -- the rotation-axis shift
+    // of getRotAxisCorrection (rotation_axis.cu:455-526)
+    FILTER_AXIS_SHIFT = 100,
 };
 
 // ----------------------------------------------------------- filter plan --
@@ -241,6 +244,17 @@ struct FbpConfig {
     int geometry = GEOM_FBP_REF;   // GEOM_FBP_REF or GEOM_FBP_LIN
     int store = STORE_F32;
 };
+
+// --- rotation axis -----------------------------------------------------------
+// Shapes the phase-correlation finder supports (lengths with prime factors
+// 2, 3, 5, 7 that fit the shared-memory transform).
+bool centersino_shape_ok(int sizex, int sizey);
+size_t centersino_workspace_bytes(int sizex, int sizey);
+// Rotation-axis offset from the 0/180 degree frames (device arrays [sizey][sizex]):
+// the reference's integer (subpixel = 0) or sub-pixel (1) search; synchronises st.
+template <typename T>
+double centersino_device(int device, const T *d_frame0, const T *d_frame1, const T *d_dark, const T *d_flat,
+                         int sizex, int sizey, int subpixel, void *workspace, cudaStream_t st);
 
 // --- BST (backprojection slice theorem) ------------------------------------
 struct BstPlanShape {

@@ -40,6 +40,13 @@ def load_ref():
     lib.get_eEM_RT_MultiGPU.argtypes = [P, I, P, P, P, P, P]
     lib.getBackgroundCorrectionMultiGPU.argtypes = [P, I, P, P, P, I, I, I, I, I, I]
     lib.getBSTMultiGPU.argtypes = [P, I, P, P, P, P, P, I]
+    lib.findcentersino.argtypes = [P, P, P, P, I, I]
+    lib.findcentersino.restype = I
+    lib.findcentersino16.argtypes = [P, P, P, P, I, I]
+    lib.findcentersino16.restype = I
+    lib.findcentersino_subpixel.argtypes = [P, P, P, P, I, I]
+    lib.findcentersino_subpixel.restype = F
+    lib.getRotAxisCorrectionMultiGPU.argtypes = [P, I, P, F, I, I, I, I]
     return lib
 
 
@@ -133,6 +140,49 @@ def bst_case(lib, name, N, B, pad, ftype, offset, reg, seed):
     return dict(kind="bst", sino=sino, angles=ang, paramf=pf, parami=pi, out=obj)
 
 
+def frame_pair(sizex, sizey, axis, seed):
+    """Raw 0 and 180 degree frames [sizey][sizex] of a smooth random object whose
+    rotation axis sits at ray `axis` (the 180 degree frame is the 0 degree one
+    mirrored about it), with flat 1e4 + 100, dark 100 and Poisson noise."""
+    rng = np.random.default_rng(seed)
+    x = np.arange(sizex, dtype=np.float64)
+    p0 = np.zeros((sizey, sizex))
+    for _ in range(6):
+        c, w, a = rng.uniform(0.3, 0.7) * sizex, rng.uniform(4, 20), rng.uniform(0.2, 1.0)
+        tilt = rng.uniform(0.5, 1.5, sizey)[:, None]
+        p0 += a * tilt * np.exp(-((x[None, :] - c) ** 2) / (2 * w * w))
+    p180 = np.array([np.interp(2 * axis - x, x, r) for r in p0])
+    dark = np.full((sizey, sizex), 100.0)
+    flat = dark + 1e4
+    f0 = dark + rng.poisson(1e4 * np.exp(-p0))
+    f1 = dark + rng.poisson(1e4 * np.exp(-p180))
+    return [a.astype(np.float32) for a in (f0, f1, dark, flat)]
+
+
+ROT_CASES = [("rot_256x128", 256, 128, 131.0), ("rot_240x96", 240, 96, 111.5), ("rot_160x64", 160, 64, 84.0)]
+
+
+def rot_case(lib, name, sizex, sizey, axis, seed):
+    f0, f1, dk, ft = frame_pair(sizex, sizey, axis, seed)
+    c = lib.findcentersino(ptr(f0), ptr(f1), ptr(dk), ptr(ft), sizex, sizey)
+    sp = lib.findcentersino_subpixel(ptr(f0), ptr(f1), ptr(dk), ptr(ft), sizex, sizey)
+    u = [a.astype(np.uint16) for a in (f0, f1, dk, ft)]
+    c16 = lib.findcentersino16(*[ptr(a) for a in u], sizex, sizey)
+    return dict(kind="centersino", frame0=f0, frame180=f1, dark=dk, flat=ft, out=np.int32(c),
+                out_subpixel=np.float32(sp), out16=np.int32(c16))
+
+
+def rotaxis_case(lib, seed):
+    tomo, _ = sino_case(64, 10, 2, seed=seed)
+    out = {}
+    for off in (1.7, -2.3):
+        t = tomo.copy()
+        lib.getRotAxisCorrectionMultiGPU(ptr(GPUS), 1, ptr(t), off, 64, 10, 2, 0)
+        out[f"out_{off:+.1f}"] = t
+    return dict(kind="rotaxis", tomo=tomo, offsets=np.array([1.7, -2.3], np.float32),
+                out_a=out["out_+1.7"], out_b=out["out_-2.3"])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
@@ -204,6 +254,10 @@ def main():
     cases["bg_log_2flats"] = background_case(lib, 3, 50, 70, 2, 1, seed=700)
     cases["bg_nolog_1flat"] = background_case(lib, 2, 33, 64, 1, 0, seed=701)
     cases["bg_log_3flats"] = background_case(lib, 2, 20, 40, 3, 1, seed=702)
+    # rotation axis: finders on frame pairs with known axes, sub-pixel axis correction
+    for i, (name, sx, sy, axis) in enumerate(ROT_CASES):
+        cases[name] = rot_case(lib, name, sx, sy, axis, seed=900 + i)
+    cases["rotaxis_n64"] = rotaxis_case(lib, seed=950)
     # the fast-intrinsic sin/cos values the reference's index rules use, as data
     # for the oracle: kind 0 = __sinf/__cosf, kind 1 = __sincosf
     from sscRaft.rafttypes import fast_sincos

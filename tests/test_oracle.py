@@ -145,6 +145,8 @@ def test_oracle_pinned_to_reference_outputs(path, oracle):
     kind = str(d["kind"])
     if kind == "index_probe":
         pytest.skip("geometry probe: checked in test_oracle_index_probe")
+    if kind in ("centersino", "rotaxis"):
+        pytest.skip("rotation axis: checked in test_oracle_rotation_axis")
     out = _run_oracle(d, oracle, use_tables=True)
     err = rel_l2(out, d["out"])
     assert err <= TIGHT[kind], (kind, err)
@@ -176,3 +178,21 @@ def test_oracle_index_probe(oracle):
         # pixel sizes: only samples on a bin boundary may differ (division)
         allowed = 0 if pixel == 1.0 else 0.05 * total
         assert mism <= allowed, (os.path.basename(f), mism, total)
+
+
+def test_oracle_rotation_axis(oracle):
+    """Phase-correlation finders: the reference's integer results exactly,
+    its sub-pixel result to within one step of its 0.01-ray grid; the
+    sub-pixel axis correction to float rounding."""
+    files = [f for f in FIXTURES if "ref_rot" in f]
+    if not files:
+        pytest.skip("no fixtures")
+    for f in files:
+        d = np.load(f)
+        if str(d["kind"]) == "centersino":
+            args = (d["frame0"], d["frame180"], d["dark"], d["flat"])
+            assert oracle.centersino(*args) == int(d["out"]), os.path.basename(f)
+            assert abs(oracle.centersino(*args, subpixel=True) - float(d["out_subpixel"])) <= 0.0051
+        else:
+            for off, key in zip(d["offsets"], ("out_a", "out_b")):
+                assert rel_l2(oracle.rotaxis(d["tomo"], float(off)), d[key]) <= 1e-6
