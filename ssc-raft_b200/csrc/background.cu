@@ -63,21 +63,24 @@ __device__ __forceinline__ void background_row(const float *src, float *dst, con
 // every angle of a slice, stay in L2.  `in` and `out` may be the same array
 // (each element is read, then written, by one thread), so they are not
 // declared __restrict__.
+// Row counts (slices x angles) fit 32 bits, so the slice / angle split of a
+// row index is a 32-bit division (a 64-bit one is an emulated routine that
+// dominated the kernel's instruction count).
 template <int V>
 __global__ void __launch_bounds__(256)
 background_kernel(const float *in, float *out, const float *__restrict__ flat, const float *__restrict__ dark,
-                  int nrays, int nangles, long long nrows, int numflats, int is_log)
+                  int nrays, int nangles, unsigned nrows, int numflats, int is_log)
 {
     const int nv = nrays / V;                         // vectors per row
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nv) return;
-    for (long long row0 = 2LL * blockIdx.y; row0 < nrows; row0 += 2LL * gridDim.y) {
+    for (unsigned row0 = 2u * blockIdx.y; row0 < nrows; row0 += 2u * gridDim.y) {
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            const long long row = row0 + h;
+            const unsigned row = row0 + h;
             if (row >= nrows) break;
-            const int z = (int)(row / nangles);
-            const int a = (int)(row - (long long)z * nangles);
+            const int z = (int)(row / (unsigned)nangles);
+            const int a = (int)(row - (unsigned)z * (unsigned)nangles);
             const float interp = (float)a / (float)nangles;
             const float *fb = flat + (size_t)z * numflats * nrays;
             background_row<V>(in + (size_t)row * nrays, out + (size_t)row * nrays, fb, fb + nrays,
@@ -94,14 +97,15 @@ void launch_background(const float *in, float *out, const float *flat, const flo
     const long long nrows = (long long)nslices * nangles;
     if (nrows <= 0 || nrays <= 0) return;
     RAFT_CHECK(numflats >= 1, "background correction: at least one flat is needed");
+    RAFT_CHECK(nrows < (1LL << 31), "background correction: slices x angles must be below 2^31");
     const bool vec = nrays % 4 == 0 && aligned16(in) && aligned16(out) && aligned16(flat) && aligned16(dark);
     const int V = vec ? 4 : 1;
     const int nv = nrays / V;
     dim3 block(256);
     dim3 grid((nv + 255) / 256, (unsigned)std::min<long long>((nrows + 1) / 2, 65535));
     count_launch();
-    if (vec) background_kernel<4><<<grid, block, 0, st>>>(in, out, flat, dark, nrays, nangles, nrows, numflats, is_log);
-    else background_kernel<1><<<grid, block, 0, st>>>(in, out, flat, dark, nrays, nangles, nrows, numflats, is_log);
+    if (vec) background_kernel<4><<<grid, block, 0, st>>>(in, out, flat, dark, nrays, nangles, (unsigned)nrows, numflats, is_log);
+    else background_kernel<1><<<grid, block, 0, st>>>(in, out, flat, dark, nrays, nangles, (unsigned)nrows, numflats, is_log);
     RAFT_CUDA(cudaGetLastError());
 }
 
