@@ -108,10 +108,21 @@ void getBSTMultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *an
 int raft_bst_device(int gpu, float *d_obj, const float *d_tomogram, const float *paramf, const int *parami,
                     void *stream);
 
-/* Adjacent reference export kept as a stub that records "not implemented":
- * get_tEM_FQ_MultiGPU: .../reconstruction_methods/em_frequency.cu:339 (rafttypes.py:149-159). */
-void get_tEM_FQ_MultiGPU(int *gpus, int ngpus, float *obj, float *count, float *flat, float *angles,
+/* Transmission EM with the Fourier-slice projector and the BST back-projector (tEMFQ).
+ * count [nslices][nangles][nrays] photon counts (read only), obj [nslices][N][N] initial
+ * guess in / result out, angles uniform over [0, pi), flat [nslices][nrays];
+ * parami = [nrays, nangles, nslices, objsize (= nrays), zpad, 0, 0, nflats, iterations,
+ * interpolation (0 nearest, 1 bilinear), blocksize], paramf = [detector pixel x, y, tv (unused,
+ * as in the reference)].  N even; N(1+zpad) and N(1+zpad)/2 with prime factors 2, 3, 5, 7.
+ * Replaces get_tEM_FQ_MultiGPU, cuda/src/geometries/parallel/reconstruction_methods/
+ * em_frequency.cu:333-398 (rafttypes.py:149-159). */
+void get_tEM_FQ_MultiGPU(int *gpus, int ngpus, float *count, float *obj, float *angles, float *flat,
                          float *paramf, int *parami);
+
+/* get_tEM_FQ_MultiGPU on device-resident buffers of one GPU (angles host; d_counts is not
+ * modified).  NULL stream as raft_fbp_device.  Returns 0 on success. */
+int raft_temfq_device(int gpu, float *d_obj, const float *d_counts, const float *d_flat, const float *angles,
+                      const float *paramf, const int *parami, void *stream);
 
 /* Status of the last call on this thread: returns 0 if it succeeded, 1 and
  * the message (truncated to len-1 chars) otherwise.  Replaces the reference's

@@ -1,6 +1,6 @@
 #!/usr/bin/env bash
 # Builds the reference ssc-raft CUDA library (parallel-beam FBP / EM / Radon /
-# lowpass / flat-dark / BST / rotation-axis path only) from its own sources, for sm_100a, into oracle/_ref/.
+# lowpass / flat-dark / BST / rotation-axis / tEMFQ path only) from its own sources, for sm_100a, into oracle/_ref/.
 #
 # The reference is compiled where it lies (read-only tree); nothing is copied
 # into this repository.  Flags follow the reference CMakeLists.txt:8-17
@@ -35,7 +35,10 @@ SRCS=(
   cuda/src/geometries/parallel/reconstruction_methods/bst.cu
   cuda/src/geometries/parallel/reconstruction_methods/em_rt.cu
   cuda/src/geometries/parallel/reconstruction_methods/kernels/em_RT_kernel.cu
+  cuda/src/geometries/parallel/reconstruction_methods/em_frequency.cu
   cuda/src/geometries/parallel/forward_methods/radon_rt.cu
+  cuda/src/geometries/parallel/forward_methods/radon_fst.cu
+  cuda/src/geometries/parallel/forward_methods/kernels/radon_fst_kernel.cu
 )
 FLAGS=(-std=c++17 -O3 -use_fast_math --expt-extended-lambda -Xcompiler -fPIC
        -gencode arch=compute_100a,code=sm_100a
@@ -52,5 +55,5 @@ for s in "${SRCS[@]}"; do
   fi
 done
 for p in "${pids[@]}"; do wait "$p"; done
-nvcc -shared "${objs[@]}" -lcufft -lcublas -o "$OUT/libraft_ref.so"
+nvcc -shared -gencode arch=compute_100a,code=sm_100a "${objs[@]}" -lcufft -lcublas -o "$OUT/libraft_ref.so"
 echo "built $OUT/libraft_ref.so"

@@ -65,6 +65,7 @@ def lib():
         _lib.oracle_centersino.argtypes = [P, P, P, P, I, I, I]
         _lib.oracle_centersino.restype = D
         _lib.oracle_rotaxis.argtypes = [P, I, I, F, P]
+        _lib.oracle_temfq.argtypes = [P, P, P, P, I, I, I, I, I, I, F, P]
     return _lib
 
 
@@ -298,3 +299,20 @@ def rotaxis(tomo, offset):
     out = np.empty(t.shape, np.float64)
     lib().oracle_rotaxis(_p(t), N, int(t.size // N), float(offset), _p(out))
     return out
+
+
+def temfq(counts, flat, angles, zpad, interp, niter, obj=None, dx=0.0, trig=None):
+    """tEMFQ (em_frequency.cu:13-87 with radon_fst.cu:544-637 and bst.cu:100-249):
+    counts [B, A, N], flat [B, N], niter iterations from obj (default ones);
+    trig = (cos, sin) of the angles as the GPU computes them (default libm's)."""
+    c = _as3(_f32(counts))
+    B, A, N = c.shape
+    fl = _f32(flat).reshape(B, N)
+    if trig is None:
+        a = np.asarray(angles, np.float32)
+        cs, sn = np.cos(a).astype(np.float32), np.sin(a).astype(np.float32)
+    else:
+        cs, sn = _f32(trig[0]), _f32(trig[1])
+    x = np.ones((B, N, N), np.float64) if obj is None else _f64(obj).reshape(B, N, N).copy()
+    lib().oracle_temfq(_p(c), _p(fl), _p(cs), _p(sn), N, A, B, int(zpad), int(interp), int(niter), float(dx), _p(x))
+    return x

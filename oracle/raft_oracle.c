@@ -600,6 +600,89 @@ void oracle_background(const float *frames, const float *flat, const float *dark
             }
 }
 
+/* The BST operator on one slice of prepared rows [A][Np] (bst.cu:22-98):
+ * half-rays of Np/2 samples split at Np/2 (the left one reversed), weighted by
+ * w_half (half of it at the centre), zero-padded to L, L-point FFT times
+ * 2 / (L max(min(k, L-k), 1/2)); polar -> Cartesian on an S x S grid with the
+ * reference's float geometry and arc weights (t = iarc - angle on the lower
+ * arc); S x S inverse transform (unnormalised); out[j][i] =
+ * Re(grid[j+off][i+off]) / scale for i, j < ncrop. */
+static void bst_slice(const double *rows, int A, int Np, int L, int S, int off, int ncrop, double w_half,
+                      float scale, double *out, const cplx *rootsL, const cplx *rinvS)
+{
+    const int half = Np / 2, c = Np / 2, twoA = 2 * A;
+    cplx *P = (cplx *)malloc(sizeof(cplx) * (size_t)twoA * L);
+    cplx *cart = (cplx *)calloc((size_t)S * S, sizeof(cplx));
+#pragma omp parallel
+    {
+        cplx *a = (cplx *)malloc(sizeof(cplx) * L);
+        cplx *b = (cplx *)malloc(sizeof(cplx) * L);
+        cplx *scratch = (cplx *)malloc(sizeof(cplx) * (size_t)(2 * L + 8));
+#pragma omp for schedule(dynamic, 4)
+        for (int r = 0; r < A; r++) {
+            const double *row = rows + (size_t)r * Np;
+            for (int side = 0; side < 2; side++) {
+                for (int idx = 0; idx < L; idx++) {
+                    double v = 0.0;
+                    if (idx < half) {
+                        double w = idx == 0 ? 0.5 * w_half : w_half;
+                        v = w * (side == 0 ? row[c - 1 - idx] : row[c + idx]);
+                    }
+                    a[idx] = v;
+                }
+                fft(L, a, b, rootsL, scratch);
+                cplx *dst = P + (size_t)(side == 0 ? r : A + r) * L;
+                for (int k = 0; k < L; k++) {
+                    double m = (double)(k < L - k ? k : L - k);
+                    dst[k] = b[k] * (2.0 / ((double)L * (m > 0.5 ? m : 0.5)));
+                }
+            }
+        }
+        free(a); free(b); free(scratch);
+    }
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int ty = 0; ty < S; ty++)
+        for (int tx = 0; tx < S; tx++) {
+            int posx = tx - S / 2, posy = ty - S / 2;
+            float rho = (float)L * hypotf((float)posx, (float)posy) / (float)S;
+            float angle = (float)twoA * (0.5f * atan2f((float)posy, (float)posx) / (float)PI_D + 0.5f);
+            int irho = (int)rho;
+            int iarc = (int)angle;
+            cplx v = 0;
+            if (irho < L / 2 - 1) {
+                float pfrac = rho - (float)irho;
+                float tfrac = (float)iarc - angle;
+                iarc = iarc % twoA;
+                int uarc = (iarc + 1) % twoA;
+                const cplx *q0 = P + (size_t)iarc * L + irho, *q1 = P + (size_t)uarc * L + irho;
+                cplx i0 = q0[0] * (double)(1.0f - pfrac) + q0[1] * (double)pfrac;
+                cplx i1 = q1[0] * (double)(1.0f - pfrac) + q1[1] * (double)pfrac;
+                v = i0 * (double)tfrac + i1 * (double)(1.0f - tfrac);
+            }
+            float sgn = 4.0f * ((float)(tx % 2) - 0.5f) * ((float)(ty % 2) - 0.5f);
+            cart[(size_t)((ty + S / 2) % S) * S + (tx + S / 2) % S] = v * (double)sgn;
+        }
+#pragma omp parallel
+    {
+        cplx *a = (cplx *)malloc(sizeof(cplx) * S);
+        cplx *b = (cplx *)malloc(sizeof(cplx) * S);
+        cplx *scratch = (cplx *)malloc(sizeof(cplx) * (size_t)(2 * S + 8));
+#pragma omp for schedule(dynamic, 8)
+        for (int y = 0; y < S; y++) {
+            fft(S, cart + (size_t)y * S, b, rinvS, scratch);
+            memcpy(cart + (size_t)y * S, b, sizeof(cplx) * S);
+        }
+#pragma omp for schedule(dynamic, 8)
+        for (int i = 0; i < ncrop; i++) {
+            for (int y = 0; y < S; y++) a[y] = cart[(size_t)y * S + off + i];
+            fft(S, a, b, rinvS, scratch);
+            for (int j = 0; j < ncrop; j++) out[(size_t)j * ncrop + i] = creal(b[off + j]) / (double)scale;
+        }
+        free(a); free(b); free(scratch);
+    }
+    free(P); free(cart);
+}
+
 /* FBP by the backprojection slice theorem: getBST (bst.cu:251-312) on the
  * padded tomogram of getBSTGPU (bst.cu:534-642), BSTFilter / BandFilterC2C
  * (filters.cu:295-390), sino2p / convBST / polar2cartesian_fourier
@@ -611,8 +694,7 @@ void oracle_background(const float *frames, const float *flat, const float *dark
 void oracle_bst(const float *tomo, int N, int A, int B, int pad, int ftype, double paganin, double reg, int csino,
                 float pixel, double *out)
 {
-    const int Np = N * (1 + pad), L = Np, S = Np, off = (pad * N) / 2, half = Np / 2, c = Np / 2;
-    const int twoA = 2 * A;
+    const int Np = N * (1 + pad), off = (pad * N) / 2;
     cplx *G = (cplx *)malloc(sizeof(cplx) * Np);
     for (int k = 0; k < Np; k++) {
         double w = ref_apply(ftype, (double)(k < Np - k ? k : Np - k) / (double)Np, paganin, reg);
@@ -621,10 +703,8 @@ void oracle_bst(const float *tomo, int N, int A, int B, int pad, int ftype, doub
     }
     cplx *rfwd = make_roots(Np, -1), *rinv = make_roots(Np, +1);
     const float scale = (float)Np * pixel * 4.0f;
+    double *rows = (double *)malloc(sizeof(double) * (size_t)A * Np);
     for (int z = 0; z < B; z++) {
-        double *rows = (double *)malloc(sizeof(double) * (size_t)A * Np);
-        cplx *P = (cplx *)malloc(sizeof(cplx) * (size_t)twoA * L);
-        cplx *cart = (cplx *)calloc((size_t)S * S, sizeof(cplx));
 #pragma omp parallel
         {
             cplx *a = (cplx *)malloc(sizeof(cplx) * Np);
@@ -641,70 +721,12 @@ void oracle_bst(const float *tomo, int N, int A, int B, int pad, int ftype, doub
                     fft(Np, b, a, rinv, scratch);
                     for (int i = 0; i < Np; i++) row[i] = creal(a[i]);
                 }
-                for (int side = 0; side < 2; side++) {
-                    for (int idx = 0; idx < L; idx++) {
-                        double v = 0.0;
-                        if (idx < half) {
-                            double w = idx == 0 ? 2.0 : 4.0;
-                            v = w * (side == 0 ? row[c - 1 - idx] : row[c + idx]);
-                        }
-                        a[idx] = v;
-                    }
-                    fft(L, a, b, rfwd, scratch);
-                    cplx *dst = P + (size_t)(side == 0 ? r : A + r) * L;
-                    for (int k = 0; k < L; k++) {
-                        double m = (double)(k < L - k ? k : L - k);
-                        dst[k] = b[k] * (2.0 / ((double)L * (m > 0.5 ? m : 0.5)));
-                    }
-                }
             }
             free(a); free(b); free(scratch);
         }
-#pragma omp parallel for schedule(dynamic, 8)
-        for (int ty = 0; ty < S; ty++)
-            for (int tx = 0; tx < S; tx++) {
-                int posx = tx - S / 2, posy = ty - S / 2;
-                float rho = (float)L * hypotf((float)posx, (float)posy) / (float)S;
-                float angle = (float)twoA * (0.5f * atan2f((float)posy, (float)posx) / (float)PI_D + 0.5f);
-                int irho = (int)rho;
-                int iarc = (int)angle;
-                cplx v = 0;
-                if (irho < L / 2 - 1) {
-                    float pfrac = rho - (float)irho;
-                    float tfrac = (float)iarc - angle;
-                    iarc = iarc % twoA;
-                    int uarc = (iarc + 1) % twoA;
-                    const cplx *q0 = P + (size_t)iarc * L + irho, *q1 = P + (size_t)uarc * L + irho;
-                    cplx i0 = q0[0] * (double)(1.0f - pfrac) + q0[1] * (double)pfrac;
-                    cplx i1 = q1[0] * (double)(1.0f - pfrac) + q1[1] * (double)pfrac;
-                    v = i0 * (double)tfrac + i1 * (double)(1.0f - tfrac);
-                }
-                float sgn = 4.0f * ((float)(tx % 2) - 0.5f) * ((float)(ty % 2) - 0.5f);
-                cart[(size_t)((ty + S / 2) % S) * S + (tx + S / 2) % S] = v * (double)sgn;
-            }
-        /* S x S inverse transform (unnormalised): rows, then the crop columns */
-#pragma omp parallel
-        {
-            cplx *a = (cplx *)malloc(sizeof(cplx) * S);
-            cplx *b = (cplx *)malloc(sizeof(cplx) * S);
-            cplx *scratch = (cplx *)malloc(sizeof(cplx) * (size_t)(2 * S + 8));
-#pragma omp for schedule(dynamic, 8)
-            for (int y = 0; y < S; y++) {
-                fft(S, cart + (size_t)y * S, b, rinv, scratch);
-                memcpy(cart + (size_t)y * S, b, sizeof(cplx) * S);
-            }
-#pragma omp for schedule(dynamic, 8)
-            for (int i = 0; i < N; i++) {
-                for (int y = 0; y < S; y++) a[y] = cart[(size_t)y * S + off + i];
-                fft(S, a, b, rinv, scratch);
-                for (int j = 0; j < N; j++)
-                    out[((size_t)z * N + j) * N + i] = creal(b[off + j]) / (double)scale;
-            }
-            free(a); free(b); free(scratch);
-        }
-        free(rows); free(P); free(cart);
+        bst_slice(rows, A, Np, Np, Np, off, N, 4.0, scale, out + (size_t)z * N * N, rfwd, rinv);
     }
-    free(G); free(rfwd); free(rinv);
+    free(rows); free(G); free(rfwd); free(rinv);
 }
 
 /* 2-D transform in place of a [ny][nx] complex array: rows, then columns. */
@@ -857,4 +879,100 @@ void oracle_rotaxis(const float *tomo, int nrays, int nrows, float offset, doubl
         free(row); free(a); free(b); free(scratch);
     }
     free(H); free(rf); free(ri);
+}
+
+
+/* Fourier-slice projection of one N x N slice into counts (pst_counts_real,
+ * radon_fst.cu:544-637): fftshift, corners of an L x L zero grid, 2-D FFT,
+ * fftshift; per angle the polar samples (cos t, sin t) (r - L/2), nearest
+ * (interp 0, round half to even) or the reference's bilinear variant (1);
+ * fftshift, 1-D inverse FFT (unnormalised), fftshift, centre N, times scale;
+ * counts = flat where p < 0, else flat exp(-p).  cs / sn: the cosine and sine
+ * the reference computes (GPU fast intrinsics, given as data). */
+static void fst_counts(const double *x, int N, int A, int L, int interp, float scale, const float *cs,
+                       const float *sn, const float *flat, double *counts, const cplx *rfwdL, const cplx *rinvL)
+{
+    cplx *W = (cplx *)calloc((size_t)L * L, sizeof(cplx));
+    for (int j = 0; j < N; j++)
+        for (int i = 0; i < N; i++) {
+            int r = j < N / 2 ? j : j + L - N, c = i < N / 2 ? i : i + L - N;
+            W[(size_t)r * L + c] = x[(size_t)((j + N / 2) % N) * N + (i + N / 2) % N];
+        }
+    fft2_inplace(W, L, L, -1);
+    const long long LL = (long long)L * L;
+#define SPEC(idx) W[(size_t)(((long long)(idx) / L + L / 2) % L) * L + (size_t)((((long long)(idx) % L) + L / 2) % L)]
+#pragma omp parallel
+    {
+        cplx *h = (cplx *)malloc(sizeof(cplx) * L), *H = (cplx *)malloc(sizeof(cplx) * L);
+        cplx *scratch = (cplx *)malloc(sizeof(cplx) * (size_t)(2 * L + 8));
+#pragma omp for schedule(dynamic, 4)
+        for (int a = 0; a < A; a++) {
+            for (int q = 0; q < L; q++) {
+                int r = (q + L / 2) % L;
+                float rho = (float)((double)r - (double)L / 2.0);
+                float xpos = cs[a] * rho, ypos = sn[a] * rho;
+                cplx v = 0;
+                if (interp == 0) {
+                    long long xi = (long long)rintf(xpos) + L / 2, yi = (long long)rintf(ypos) + L / 2;
+                    long long idx = yi * L + xi;
+                    if (idx < LL) v = SPEC(idx);
+                } else {
+                    long long xd = (long long)floorf(xpos) + L / 2, xu = (long long)ceilf(xpos) + L / 2;
+                    long long yd = (long long)floorf(ypos) + L / 2, yu = (long long)ceilf(ypos) + L / 2;
+                    cplx fdd = SPEC(yd * L + xd), fdu = SPEC(yu * L + xd);
+                    cplx fud = SPEC(yd * L + xu), fuu = SPEC(yu * L + xu);
+                    float xd_pos = (float)xd - L / 2, xu_pos = (float)xu - L / 2;
+                    float yd_pos = (float)yd - L / 2, yu_pos = (float)yu - L / 2;
+                    if (xd == xu && yd == yu) v = fdd;
+                    else if (xd == xu) v = (double)(yu_pos - ypos) * fdd + (double)(ypos - yd_pos) * fuu;
+                    else if (yd == yu) v = (double)(xu_pos - xpos) * fdd + (double)(xpos - xd_pos) * fuu;
+                    else
+                        v = (double)(yu_pos - ypos) * ((double)(xu_pos - xpos) * fdd + (double)(xpos - xd_pos) * fud) +
+                            (double)(ypos - yd_pos) * ((double)(xu_pos - xpos) * fdu + (double)(xpos - xd_pos) * fuu);
+                }
+                h[q] = v;
+            }
+            fft(L, h, H, rinvL, scratch);
+            for (int i = 0; i < N; i++) {
+                double p = creal(H[((L - N) / 2 + i + L / 2) % L]) * (double)scale;
+                counts[(size_t)a * N + i] = p < 0 ? flat[i] : flat[i] * exp(-p);
+            }
+        }
+        free(h); free(H); free(scratch);
+    }
+#undef SPEC
+    free(W);
+    (void)rfwdL;
+}
+
+/* tEMFQ (get_tEM_FQ, em_frequency.cu:13-87): backcounts = 1 / BST(counts);
+ * niter times: model = FST(x); x <- x * (BST(model) * backcounts).  The BST
+ * here is EMFQ_BST (bst.cu:100-249): no filter and no padding of the rows,
+ * half-rays N/2 zero-padded to N (zpad+1)/2 with weight (zpad+1)^2, an N x N
+ * grid, scale 1.  obj: initial guess in, result out ([B][N][N], FP64). */
+void oracle_temfq(const float *counts, const float *flat, const float *cs, const float *sn, int N, int A, int B,
+                  int zpad, int interp, int niter, float dx, double *obj)
+{
+    const int L = N * (1 + zpad), pad0 = zpad + 1, Lb = N * pad0 / 2;
+    const float scale = dx > 0.f ? dx / (float)L : (float)(1.0 / (float)L);
+    cplx *rfL = make_roots(L, -1), *riL = make_roots(L, +1);
+    cplx *rfLb = make_roots(Lb, -1), *riN = make_roots(N, +1);
+    double *rows = (double *)malloc(sizeof(double) * (size_t)A * N);
+    double *inv = (double *)malloc(sizeof(double) * (size_t)N * N);
+    double *back = (double *)malloc(sizeof(double) * (size_t)N * N);
+    double *model = (double *)malloc(sizeof(double) * (size_t)A * N);
+    for (int z = 0; z < B; z++) {
+        double *x = obj + (size_t)z * N * N;
+        const float *fl = flat + (size_t)z * N;
+        for (size_t i = 0; i < (size_t)A * N; i++) rows[i] = counts[(size_t)z * A * N + i];
+        bst_slice(rows, A, N, Lb, N, 0, N, (double)(pad0 * pad0), 1.0f, inv, rfLb, riN);
+        for (size_t i = 0; i < (size_t)N * N; i++) inv[i] = 1.0 / inv[i];
+        for (int k = 0; k < niter; k++) {
+            fst_counts(x, N, A, L, interp, scale, cs, sn, fl, model, rfL, riL);
+            bst_slice(model, A, N, Lb, N, 0, N, (double)(pad0 * pad0), 1.0f, back, rfLb, riN);
+            for (size_t i = 0; i < (size_t)N * N; i++) x[i] *= back[i] * inv[i];
+        }
+    }
+    free(rows); free(inv); free(back); free(model);
+    free(rfL); free(riL); free(rfLb); free(riN);
 }

@@ -763,14 +763,83 @@ int raft_bst_device(int gpu, float *d_obj, const float *d_tomogram, const float 
     return has_error() ? 1 : 0;
 }
 
-// Adjacent reference export that this library does not implement: it
-// records an error instead of running (rafttypes.py binds it if present).
-void get_tEM_FQ_MultiGPU(int *gpus, int ngpus, float *obj, float *count, float *flat, float *angles, float *paramf,
+// --- tEMFQ -------------------------------------------------------------------
+// Reference: get_tEM_FQ_MultiGPU, cuda/src/geometries/parallel/reconstruction_methods/em_frequency.cu:333-398
+// (argument order count, obj, angles, flat as there); parami = [nrays, nangles,
+// nslices, objsize, zpad, 0, 0, nflats, iterations, interpolation (0 nearest,
+// 1 bilinear), blocksize], paramf = [detector pixel x, y, tv] (setEMFQParameters,
+// parameters.cu:72-114; the total-variation weight is not used there either).
+static bool parse_temfq(const float *paramf, const int *parami, TemfqConfig &c)
+{
+    if (!paramf || !parami) {
+        set_error("null parameter array");
+        return false;
+    }
+    c.nrays = parami[0];
+    c.nangles = parami[1];
+    c.nslices = parami[2];
+    c.zpad = parami[4];
+    c.niter = parami[8];
+    c.interpolation = parami[9];
+    c.blocksize = parami[10];
+    c.dx = paramf[0];
+    if (parami[3] != c.nrays) {
+        set_error("tEMFQ: the object size must equal nrays");
+        return false;
+    }
+    if (c.nslices < 0 || c.niter < 0 || (c.interpolation != 0 && c.interpolation != 1) ||
+        !temfq_shape_ok(c.nrays, c.nangles, c.zpad)) {
+        set_error("tEMFQ: unsupported sizes (N even; N(1+zpad) and N(1+zpad)/2 with prime factors 2, 3, 5, 7 "
+                  "only; N(1+zpad) <= 14528), or iterations < 0, or interpolation not 0/1");
+        return false;
+    }
+    return true;
+}
+
+void get_tEM_FQ_MultiGPU(int *gpus, int ngpus, float *count, float *obj, float *angles, float *flat, float *paramf,
                          int *parami)
 {
-    (void)gpus; (void)ngpus; (void)obj; (void)count; (void)flat; (void)angles; (void)paramf; (void)parami;
     clear_error();
-    set_error("get_tEM_FQ_MultiGPU is not implemented by this library (use method='tEMRT')");
+    TemfqConfig cfg;
+    if (!parse_temfq(paramf, parami, cfg)) return;
+    if (!check_gpus(gpus, ngpus)) return;
+    if (!count || !obj || !angles || !flat) {
+        set_error("null data pointer");
+        return;
+    }
+    const size_t cps = (size_t)cfg.nangles * cfg.nrays, ops = (size_t)cfg.nrays * cfg.nrays;
+    split_slabs(gpus, ngpus, cfg.nslices, [&](int dev, int start, int n) {
+        temfq_host_slab(cfg, dev, obj + ops * start, count + cps * start, flat + (size_t)cfg.nrays * start, angles, n);
+    });
+}
+
+// Device-resident tEMFQ on one GPU: d_obj [nslices][N][N] in/out, d_counts
+// [nslices][A][N] (not modified), d_flat [nslices][N], angles host.
+int raft_temfq_device(int gpu, float *d_obj, const float *d_counts, const float *d_flat, const float *angles,
+                      const float *paramf, const int *parami, void *stream)
+{
+    clear_error();
+    TemfqConfig cfg;
+    if (!parse_temfq(paramf, parami, cfg)) return 1;
+    if (!check_gpus(&gpu, 1)) return 1;
+    try {
+        DeviceState &ds = device_state(gpu);
+        std::lock_guard<std::mutex> lk(ds.mtx);
+        RAFT_CUDA(cudaSetDevice(gpu));
+        ds.ensure();
+        cudaStream_t st = resolve_stream(ds, stream, ds.s_comp);
+        const int A = cfg.nangles;
+        float *d_ang = (float *)ds.angles.get(sizeof(float) * A);
+        char *tb = (char *)ds.tabs.get(sizeof(float) * 3 * A + 64);
+        float *cs = (float *)tb, *sn = cs + A, *wt = sn + A;
+        RAFT_CUDA(cudaMemcpyAsync(d_ang, angles, sizeof(float) * A, cudaMemcpyHostToDevice, st));
+        launch_angle_tables(d_ang, A, cs, sn, wt, 0, st);
+        void *ws = ds.rows.get(temfq_workspace_bytes(cfg.nrays, A, cfg.zpad, std::max(1, cfg.nslices)));
+        temfq_run(gpu, cfg, d_obj, d_counts, d_flat, cs, sn, cfg.nslices, ws, st);
+        if (!stream) RAFT_CUDA(cudaStreamSynchronize(st));
+    } catch (const CudaFail &) {
+    }
+    return has_error() ? 1 : 0;
 }
 
 }  // extern "C"

@@ -55,10 +55,13 @@ struct BstArgs {
     float2 *polar;          // [B][2A][Lh]
     float2 *T;              // [B][S][N]: rows inverse-transformed along x, crop columns
     float *obj;             // [B][N][N]
-    const float2 *tw;       // exp(-2 pi i k / Np)
+    const float2 *tw;       // exp(-2 pi i k / Np)   (filter transforms)
+    const float2 *twL;      // exp(-2 pi i k / L)    (half-ray transforms)
+    const float2 *twS;      // exp(-2 pi i k / S)    (grid transforms)
     const float2 *G;        // filter weights [Np], or null for 'none'
-    RadixList rl;
-    int N, A, Np, L, Lh, S, off;
+    RadixList rl, rlL, rlS;
+    int N, A, Np, L, Lh, S, off, M;   // M = max(Np, L): shared-memory buffer length of the row kernel
+    float w_half;           // half-ray weight (the centre sample gets half of it)
     float scale;
 };
 
@@ -78,32 +81,32 @@ __global__ void __launch_bounds__(512) bst_rows_kernel(const BstArgs p)
     __syncthreads();
     float sgn1 = 1.f;   // the second row is sgn1 * z.y
     if (p.G) {
-        float2 *r = fft_forward(z, sm_bst + p.Np, p.Np, p.rl, p.tw);
+        float2 *r = fft_forward(z, sm_bst + p.M, p.Np, p.rl, p.tw);
         for (int k = threadIdx.x; k < p.Np; k += blockDim.x) {
             const float2 g = cmul(r[k], __ldg(&p.G[k]));
             r[k] = make_float2(g.x, -g.y);
         }
         __syncthreads();
         // forward transform of the conjugate = conjugate of the inverse
-        z = fft_forward(r, r == sm_bst ? sm_bst + p.Np : sm_bst, p.Np, p.rl, p.tw);
+        z = fft_forward(r, r == sm_bst ? sm_bst + p.M : sm_bst, p.Np, p.rl, p.tw);
         sgn1 = -1.f;
     }
-    float2 *fa = (z == sm_bst) ? sm_bst + p.Np : sm_bst;
-    float2 *fb = sm_bst + 2 * p.Np;
+    float2 *fa = (z == sm_bst) ? sm_bst + p.M : sm_bst;
+    float2 *fb = sm_bst + 2 * p.M;
     const int c = p.Np / 2, half = p.Np / 2;
     const size_t pb = (size_t)slice * 2 * p.A * p.Lh;
     for (int r = 0; r < (has1 ? 2 : 1); r++) {
         for (int idx = threadIdx.x; idx < p.L; idx += blockDim.x) {
             float2 h = make_float2(0.f, 0.f);
             if (idx < half) {
-                const float w = idx == 0 ? 2.f : 4.f;
+                const float w = idx == 0 ? 0.5f * p.w_half : p.w_half;
                 const float2 lft = z[c - 1 - idx], rgt = z[c + idx];
                 h = r == 0 ? make_float2(w * lft.x, w * rgt.x) : make_float2(w * sgn1 * lft.y, w * sgn1 * rgt.y);
             }
             fa[idx] = h;
         }
         __syncthreads();
-        const float2 *H = fft_forward(fa, fb, p.L, p.rl, p.tw);
+        const float2 *H = fft_forward(fa, fb, p.L, p.rlL, p.twL);
         float2 *frow = p.polar + pb + (size_t)(a0 + r) * p.Lh;           // left half-ray (theta + pi)
         float2 *rrow = p.polar + pb + (size_t)(p.A + a0 + r) * p.Lh;     // right half-ray (theta)
         for (int k = threadIdx.x; k < p.Lh; k += blockDim.x) {
@@ -151,7 +154,7 @@ __global__ void __launch_bounds__(512) bst_regrid_kernel(const BstArgs p)
         sm_bst[X] = make_float2(v.x * sgn, -v.y * sgn);   // conjugated: see bst_cols_kernel
     }
     __syncthreads();
-    const float2 *r = fft_forward(sm_bst, sm_bst + S, S, p.rl, p.tw);
+    const float2 *r = fft_forward(sm_bst, sm_bst + S, S, p.rlS, p.twS);
     float2 *trow = p.T + ((size_t)slice * S + Y) * p.N;
     for (int i = threadIdx.x; i < p.N; i += blockDim.x) trow[i] = r[p.off + i];
 }
@@ -165,29 +168,71 @@ __global__ void __launch_bounds__(512) bst_cols_kernel(const BstArgs p)
     const float2 *tcol = p.T + (size_t)slice * p.S * p.N + i;
     for (int Y = threadIdx.x; Y < p.S; Y += blockDim.x) sm_bst[Y] = tcol[(size_t)Y * p.N];
     __syncthreads();
-    const float2 *r = fft_forward(sm_bst, sm_bst + p.S, p.S, p.rl, p.tw);
+    const float2 *r = fft_forward(sm_bst, sm_bst + p.S, p.S, p.rlS, p.twS);
     float *o = p.obj + (size_t)slice * p.N * p.N + i;
     for (int j = threadIdx.x; j < p.N; j += blockDim.x) o[(size_t)j * p.N] = r[p.off + j].x / p.scale;
 }
 
-struct BstPlanDev {
-    BstPlanShape shape;
-    RadixList rl;
-    float2 *tw = nullptr, *G = nullptr;
-    ~BstPlanDev()
-    {
-        if (tw) cudaFree(tw);
-        if (G) cudaFree(G);
-    }
-};
-
-using BstKey = std::tuple<int, int, int, int, double, double, int>;
+using BstKey = std::tuple<int, int, int, int, double, double>;
 std::mutex g_bst_mtx;
-std::map<BstKey, std::unique_ptr<BstPlanDev>> g_bst_plans;
+std::map<BstKey, float2 *> g_bst_filters;   // filter weights per (device, Np, type, offset, paganin, reg)
+
+const float2 *bst_filter_weights(int device, int Np, int ftype, int c, double paganin, double reg)
+{
+    std::lock_guard<std::mutex> lk(g_bst_mtx);
+    float2 *&slot = g_bst_filters[BstKey(device, Np, ftype, c, paganin, reg)];
+    if (!slot) {
+        std::vector<float2> G(Np);
+        for (int k = 0; k < Np; k++) {
+            const double w = filter_apply_ref(ftype, (double)std::min(k, Np - k) / Np, paganin, reg);
+            const double ph = -2.0 * M_PI * (double)c * (double)k / (double)Np;
+            G[k] = make_float2((float)(w * std::cos(ph)), (float)(w * std::sin(ph)));
+        }
+        RAFT_CUDA(cudaMalloc(&slot, sizeof(float2) * Np));
+        RAFT_CUDA(cudaMemcpy(slot, G.data(), sizeof(float2) * Np, cudaMemcpyHostToDevice));
+    }
+    return slot;
+}
+
+std::mutex g_fft_mtx;
+std::map<std::pair<int, int>, std::unique_ptr<FftTable>> g_fft_tables;
 
 }  // namespace
 
+const FftTable &fft_table(int device, int n)
+{
+    std::lock_guard<std::mutex> lk(g_fft_mtx);
+    auto &slot = g_fft_tables[{device, n}];
+    if (!slot) {
+        auto t = std::make_unique<FftTable>();
+        RAFT_CHECK(factorize(n, t->rl.r, t->rl.n), "FFT length with a prime factor above 7");
+        const std::vector<float2> h = fft_twiddles(n);
+        RAFT_CUDA(cudaMalloc(&t->tw, sizeof(float2) * n));
+        RAFT_CUDA(cudaMemcpy(t->tw, h.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+        slot = std::move(t);
+    }
+    return *slot;
+}
+
+FftTable::~FftTable()
+{
+    if (tw) cudaFree(tw);
+}
+
 constexpr size_t kBstSmemMax = 227 * 1024;
+
+static bool fft_len_ok(int n)
+{
+    int r[24], nr = 0;
+    return n >= 1 && factorize(n, r, nr);
+}
+
+bool bst_core_ok(const BstCore &c)
+{
+    return c.N >= 2 && c.A >= 1 && c.L >= 2 && c.S >= 2 && fft_len_ok(c.L) && fft_len_ok(c.S) &&
+           (!c.filtered || fft_len_ok(c.Np)) && 3 * (size_t)c.M * sizeof(float2) <= kBstSmemMax &&
+           2 * (size_t)c.S * sizeof(float2) <= kBstSmemMax;
+}
 
 bool bst_plan_shape(BstPlanShape &s, int N, int A, int pad)
 {
@@ -198,9 +243,11 @@ bool bst_plan_shape(BstPlanShape &s, int N, int A, int pad)
     s.Lh = s.L / 2;
     s.S = s.Np;
     s.off = (pad * N) / 2;
-    int radix[24], nr = 0;
     s.threads = fft_threads(s.Np);
-    return N >= 2 && A >= 1 && factorize(s.Np, radix, nr) && 3 * (size_t)s.Np * sizeof(float2) <= kBstSmemMax;
+    BstCore c;
+    c.N = N; c.A = A; c.Np = s.Np; c.L = s.L; c.Lh = s.Lh; c.S = s.S; c.off = s.off; c.M = s.Np;
+    c.filtered = true;
+    return bst_core_ok(c);
 }
 
 size_t bst_workspace_bytes(const BstPlanShape &s, int nslices)
@@ -210,59 +257,50 @@ size_t bst_workspace_bytes(const BstPlanShape &s, int nslices)
     return ((polar + 255) & ~(size_t)255) + T;
 }
 
-void launch_bst(int device, const FbpConfig &cfg, const float *d_tomo, float *d_obj, int nslices, void *workspace,
-                cudaStream_t st)
+size_t bst_core_workspace_bytes(const BstCore &c, int nslices)
 {
-    BstPlanShape shape;
-    RAFT_CHECK(bst_plan_shape(shape, cfg.nrays, cfg.nangles, cfg.pad),
-               "BST: the padded length N*(1+pad) must have only the prime factors 2, 3, 5, 7 and be at most 9472");
-    const int c = (int)cfg.offset;   // the reference passes the axis offset to an int (filters.cu:345-390)
-    BstPlanDev *plan;
-    {
-        std::lock_guard<std::mutex> lk(g_bst_mtx);
-        const BstKey key(device, shape.Np, cfg.filter, c, cfg.paganin, cfg.reg, 0);
-        auto &slot = g_bst_plans[key];
-        if (!slot) {
-            auto pl = std::make_unique<BstPlanDev>();
-            pl->shape = shape;
-            factorize(shape.Np, pl->rl.r, pl->rl.n);
-            const std::vector<float2> tw = fft_twiddles(shape.Np);
-            RAFT_CUDA(cudaMalloc(&pl->tw, sizeof(float2) * shape.Np));
-            RAFT_CUDA(cudaMemcpy(pl->tw, tw.data(), sizeof(float2) * shape.Np, cudaMemcpyHostToDevice));
-            if (cfg.filter != FILTER_NONE) {
-                std::vector<float2> G(shape.Np);
-                for (int k = 0; k < shape.Np; k++) {
-                    const double w = filter_apply_ref(cfg.filter, (double)std::min(k, shape.Np - k) / shape.Np,
-                                                      cfg.paganin, cfg.reg);
-                    const double ph = -2.0 * M_PI * (double)c * (double)k / (double)shape.Np;
-                    G[k] = make_float2((float)(w * std::cos(ph)), (float)(w * std::sin(ph)));
-                }
-                RAFT_CUDA(cudaMalloc(&pl->G, sizeof(float2) * shape.Np));
-                RAFT_CUDA(cudaMemcpy(pl->G, G.data(), sizeof(float2) * shape.Np, cudaMemcpyHostToDevice));
-            }
-            slot = std::move(pl);
-        }
-        plan = slot.get();
-    }
+    const size_t polar = (size_t)nslices * 2 * c.A * c.Lh * sizeof(float2);
+    const size_t T = (size_t)nslices * c.S * c.N * sizeof(float2);
+    return ((polar + 255) & ~(size_t)255) + T;
+}
+
+void bst_run(int device, const BstCore &c, const float *d_tomo, float *d_obj, int nslices, void *workspace,
+             cudaStream_t st)
+{
+    RAFT_CHECK(bst_core_ok(c), "BST: unsupported transform lengths");
     if (nslices <= 0) return;
+    const FftTable &tS = fft_table(device, c.S), &tL = fft_table(device, c.L);
     BstArgs a;
     a.tomo = d_tomo;
     a.polar = (float2 *)workspace;
-    const size_t polar = (size_t)nslices * 2 * shape.A * shape.Lh * sizeof(float2);
+    const size_t polar = (size_t)nslices * 2 * c.A * c.Lh * sizeof(float2);
     a.T = (float2 *)((char *)workspace + ((polar + 255) & ~(size_t)255));
     a.obj = d_obj;
-    a.tw = plan->tw;
-    a.G = plan->G;
-    a.rl = plan->rl;
-    a.N = shape.N;
-    a.A = shape.A;
-    a.Np = shape.Np;
-    a.L = shape.L;
-    a.Lh = shape.Lh;
-    a.S = shape.S;
-    a.off = shape.off;
-    a.scale = (float)shape.Np * cfg.pixel_x * 4.0f;
-    const size_t sm3 = 3 * (size_t)shape.Np * sizeof(float2), sm2 = 2 * (size_t)shape.Np * sizeof(float2);
+    a.G = c.G;
+    if (c.G) {
+        const FftTable &tN = fft_table(device, c.Np);
+        a.tw = tN.tw;
+        a.rl = tN.rl;
+    } else {
+        a.tw = nullptr;
+        a.rl = RadixList{};
+    }
+    a.twL = tL.tw;
+    a.rlL = tL.rl;
+    a.twS = tS.tw;
+    a.rlS = tS.rl;
+    a.N = c.N;
+    a.A = c.A;
+    a.Np = c.Np;
+    a.L = c.L;
+    a.Lh = c.Lh;
+    a.S = c.S;
+    a.off = c.off;
+    a.M = c.M;
+    a.w_half = c.w_half;
+    a.scale = c.scale;
+    const int threads = fft_threads(std::max(c.M, c.S));
+    const size_t sm3 = 3 * (size_t)c.M * sizeof(float2), sm2 = 2 * (size_t)c.S * sizeof(float2);
     static thread_local int configured = -1;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -273,14 +311,38 @@ void launch_bst(int device, const FbpConfig &cfg, const float *d_tomo, float *d_
         configured = dev;
     }
     ProfScope ps(PROF_OTHER, st);   // counts the first of the three launches
-    bst_rows_kernel<<<dim3((shape.A + 1) / 2, nslices), shape.threads, sm3, st>>>(a);
+    bst_rows_kernel<<<dim3((c.A + 1) / 2, nslices), threads, sm3, st>>>(a);
     RAFT_CUDA(cudaGetLastError());
     count_launch();
-    bst_regrid_kernel<<<dim3(shape.S, nslices), shape.threads, sm2, st>>>(a);
+    bst_regrid_kernel<<<dim3(c.S, nslices), threads, sm2, st>>>(a);
     RAFT_CUDA(cudaGetLastError());
     count_launch();
-    bst_cols_kernel<<<dim3(shape.N, nslices), shape.threads, sm2, st>>>(a);
+    bst_cols_kernel<<<dim3(c.N, nslices), threads, sm2, st>>>(a);
     RAFT_CUDA(cudaGetLastError());
+}
+
+void launch_bst(int device, const FbpConfig &cfg, const float *d_tomo, float *d_obj, int nslices, void *workspace,
+                cudaStream_t st)
+{
+    BstPlanShape shape;
+    RAFT_CHECK(bst_plan_shape(shape, cfg.nrays, cfg.nangles, cfg.pad),
+               "BST: the padded length N*(1+pad) must have only the prime factors 2, 3, 5, 7 and be at most 9472");
+    BstCore c;
+    c.N = shape.N;
+    c.A = shape.A;
+    c.Np = shape.Np;
+    c.L = shape.L;
+    c.Lh = shape.Lh;
+    c.S = shape.S;
+    c.off = shape.off;
+    c.M = shape.Np;
+    c.filtered = cfg.filter != FILTER_NONE;
+    // the reference passes the axis offset to an int (filters.cu:345-390)
+    c.G = c.filtered ? bst_filter_weights(device, shape.Np, cfg.filter, (int)cfg.offset, cfg.paganin, cfg.reg)
+                     : nullptr;
+    c.w_half = 4.0f;   // pad0^2 with the reference's fixed pad0 = 2 (bst.cu:22-48, 561)
+    c.scale = (float)shape.Np * cfg.pixel_x * 4.0f;
+    bst_run(device, c, d_tomo, d_obj, nslices, workspace, st);
 }
 
 }  // namespace raft

@@ -401,6 +401,48 @@ template double centersino_host<float>(int, const float *, const float *, const 
 template double centersino_host<uint16_t>(int, const uint16_t *, const uint16_t *, const uint16_t *,
                                           const uint16_t *, int, int, int);
 
+// ---------------------------------------------------------------- tEMFQ --
+// _get_tEM_FQ_GPU (em_frequency.cu:301-331): slices in chunks; per chunk the
+// counts, flat and initial guess go to the device, the EM runs there, the
+// result comes back.
+void temfq_host_slab(const TemfqConfig &cfg, int device, float *obj, const float *counts, const float *flat,
+                     const float *angles, int nslices)
+{
+    if (nslices <= 0) return;
+    const int N = cfg.nrays, A = cfg.nangles;
+    RAFT_CHECK(temfq_shape_ok(N, A, cfg.zpad), "tEMFQ: unsupported sizes (N even; N(1+zpad) and N(1+zpad)/2 "
+                                               "with prime factors 2, 3, 5, 7 only; N(1+zpad) <= 14528)");
+    DeviceState &ds = device_state(device);
+    std::lock_guard<std::mutex> lk(ds.mtx);
+    RAFT_CUDA(cudaSetDevice(device));
+    ds.ensure();
+    cudaStream_t st = ds.s_comp;
+    const size_t per = temfq_workspace_bytes(N, A, cfg.zpad, 1);
+    int chunk = (int)std::max<size_t>(1, ((size_t)8 << 30) / per);
+    chunk = std::min(chunk, cfg.blocksize > 0 ? cfg.blocksize : 64);
+    chunk = std::max(1, std::min(chunk, nslices));
+    const size_t cps = (size_t)A * N, ops = (size_t)N * N;
+    float *d_counts = (float *)ds.sino[0].get(cps * chunk * sizeof(float));
+    float *d_obj = (float *)ds.img[0].get(ops * chunk * sizeof(float));
+    float *d_flat = (float *)ds.flat.get((size_t)N * chunk * sizeof(float) + 16);
+    float *d_ang = (float *)ds.angles.get(sizeof(float) * A);
+    char *tb = (char *)ds.tabs.get(sizeof(float) * 3 * A + 64);
+    float *cs = (float *)tb, *sn = cs + A, *wt = sn + A;
+    void *ws = ds.rows.get(temfq_workspace_bytes(N, A, cfg.zpad, chunk));
+    RAFT_CUDA(cudaMemcpyAsync(d_ang, angles, sizeof(float) * A, cudaMemcpyHostToDevice, st));
+    launch_angle_tables(d_ang, A, cs, sn, wt, 0, st);   // __cosf / __sinf, as the reference's fast-math cosf/sinf
+    for (int s0 = 0; s0 < nslices; s0 += chunk) {
+        const int ns = std::min(chunk, nslices - s0);
+        RAFT_CUDA(cudaMemcpyAsync(d_counts, counts + cps * s0, cps * ns * sizeof(float), cudaMemcpyHostToDevice, st));
+        RAFT_CUDA(cudaMemcpyAsync(d_obj, obj + ops * s0, ops * ns * sizeof(float), cudaMemcpyHostToDevice, st));
+        RAFT_CUDA(cudaMemcpyAsync(d_flat, flat + (size_t)N * s0, (size_t)N * ns * sizeof(float), cudaMemcpyHostToDevice,
+                                  st));
+        temfq_run(device, cfg, d_obj, d_counts, d_flat, cs, sn, ns, ws, st);
+        RAFT_CUDA(cudaMemcpyAsync(obj + ops * s0, d_obj, ops * ns * sizeof(float), cudaMemcpyDeviceToHost, st));
+        RAFT_CUDA(cudaStreamSynchronize(st));
+    }
+}
+
 // ------------------------------------------------------------------ BST --
 // getBSTGPU (bst.cu:534-642): slices stream through the two-slot pipeline;
 // each chunk runs the three BST kernels (bst.cu in this library).

@@ -94,6 +94,8 @@ void rotaxis_host_slab(int device, float *tomo, float axis_offset, int nrays, in
 template <typename T>
 double centersino_host(int device, const T *frame0, const T *frame1, const T *dark, const T *flat, int sizex,
                        int sizey, int subpixel);
+void temfq_host_slab(const TemfqConfig &cfg, int device, float *obj, const float *counts, const float *flat,
+                     const float *angles, int nslices);
 void lowpass_host_slab(const FbpConfig &cfg, int device, float *tomo, int nslices);
 void background_host_slab(int device, float *frames, const float *flat, const float *dark, int nrays, int nangles,
                           int nslices, int numflats, int is_log, int blocksize);

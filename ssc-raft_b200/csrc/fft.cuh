@@ -210,4 +210,13 @@ __device__ __forceinline__ float2 *fft_forward(float2 *a, float2 *b, int Np, con
 }
 
 
+// Device twiddles and radix list of one length, cached per (device, n) for
+// the life of the process (defined in bst.cu).
+struct FftTable {
+    RadixList rl;
+    float2 *tw = nullptr;
+    ~FftTable();
+};
+const FftTable &fft_table(int device, int n);
+
 }  // namespace raft

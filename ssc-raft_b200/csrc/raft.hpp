@@ -266,6 +266,35 @@ struct BstPlanShape {
 bool bst_plan_shape(BstPlanShape &s, int N, int A, int pad);
 // Device workspace bytes for nslices slices at once.
 size_t bst_workspace_bytes(const BstPlanShape &s, int nslices);
+// General form of the BST operator (both the FBP method and the EM back-
+// projector of tEMFQ): rows of N samples edge-padded to Np (offset off) and
+// optionally filtered, half-rays of Np/2 samples weighted by w_half (half of it
+// at the centre) and zero-padded to L, an S x S grid, crop offset off, image
+// divided by scale.
+struct BstCore {
+    int N = 0, A = 0, Np = 0, L = 0, Lh = 0, S = 0, off = 0, M = 0;
+    bool filtered = false;
+    const float2 *G = nullptr;      // filter weights [Np] when filtered
+    float w_half = 4.0f, scale = 1.0f;
+};
+bool bst_core_ok(const BstCore &c);
+size_t bst_core_workspace_bytes(const BstCore &c, int nslices);
+void bst_run(int device, const BstCore &c, const float *d_tomo, float *d_obj, int nslices, void *workspace,
+             cudaStream_t st);
+
+// --- tEMFQ (transmission EM, Fourier-slice projector + BST back-projector) ----
+struct TemfqConfig {
+    int nrays = 0, nangles = 0, nslices = 0, zpad = 0, niter = 0, interpolation = 1, blocksize = 0;
+    float dx = 0.f;
+};
+bool temfq_shape_ok(int N, int A, int zpad);
+BstCore temfq_bst_core(int N, int A, int zpad);
+size_t temfq_workspace_bytes(int N, int A, int zpad, int nslices);
+// niter iterations on nslices slices: d_obj [nslices][N][N] (initial guess in,
+// result out), d_counts [nslices][A][N] (read only), d_flat [nslices][N],
+// d_cs / d_sn [A] = __cosf / __sinf of the angles.
+void temfq_run(int device, const TemfqConfig &cfg, float *d_obj, const float *d_counts, const float *d_flat,
+               const float *d_cs, const float *d_sn, int nslices, void *workspace, cudaStream_t st);
 // BST reconstruction of nslices slices (d_tomo [nslices][A][N] -> d_obj
 // [nslices][N][N]) on st; cfg gives N, A, pad, filter, paganin, reg, axis
 // offset, pixel.

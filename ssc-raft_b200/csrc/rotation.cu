@@ -160,36 +160,9 @@ __global__ void peak_subpixel_kernel(const float2 *f, int sizex, int sizey, unsi
     warp_max_commit(key, best);
 }
 
-struct Twiddles {
-    RadixList rl;
-    float2 *tw = nullptr;
-    ~Twiddles()
-    {
-        if (tw) cudaFree(tw);
-    }
-};
-
-std::mutex g_tw_mtx;
-std::map<std::pair<int, int>, std::unique_ptr<Twiddles>> g_tw;
-
-const Twiddles &twiddles_for(int device, int n)
-{
-    std::lock_guard<std::mutex> lk(g_tw_mtx);
-    auto &slot = g_tw[{device, n}];
-    if (!slot) {
-        auto t = std::make_unique<Twiddles>();
-        factorize(n, t->rl.r, t->rl.n);
-        const std::vector<float2> h = fft_twiddles(n);
-        RAFT_CUDA(cudaMalloc(&t->tw, sizeof(float2) * n));
-        RAFT_CUDA(cudaMemcpy(t->tw, h.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
-        slot = std::move(t);
-    }
-    return *slot;
-}
-
 void fft2(int device, float2 *data, int sizex, int sizey, int inverse, cudaStream_t st)
 {
-    const Twiddles &tx = twiddles_for(device, sizex), &ty = twiddles_for(device, sizey);
+    const FftTable &tx = fft_table(device, sizex), &ty = fft_table(device, sizey);
     const size_t smx = 2 * (size_t)sizex * sizeof(float2), smy = 2 * (size_t)sizey * sizeof(float2);
     RAFT_CUDA(cudaFuncSetAttribute(fft_strided_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)std::max(smx, smy)));

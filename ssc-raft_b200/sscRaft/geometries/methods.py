@@ -33,7 +33,7 @@ def fbp(tomogram, angles=None, obj=None, dic=None, nstreams=0, **kwargs):
 
 
 def em(data, flat=None, angles=None, obj=None, dic=None, **kwargs):
-    """Expectation maximisation, methods 'eEMRT' and 'tEMRT' (methods.py:83-186)."""
+    """Expectation maximisation, methods 'eEMRT', 'tEMRT' and 'tEMFQ' (methods.py:83-186)."""
     required = ('gpu',)
     optional = ('iterations', 'detectorPixel[m]', 'padding', 'beamgeometry', 'interpolation', 'blocksize')
     default = (10, 0.0, 2, 'parallel', 'bilinear', 0)
@@ -60,6 +60,12 @@ def em(data, flat=None, angles=None, obj=None, dic=None, **kwargs):
     elif method == 'tEMRT':
         return tEMRT_GPU_(data, flat, angles, iterations, gpus, blocksize, obj=obj)
     elif method == 'tEMFQ':
-        return tEMFQ_GPU_()
+        # methods.py:140-181: padding and detector pixel from the dictionary,
+        # total variation off, the interpolation name mapped to 0/1
+        from ..rafttypes import setInterpolation
+        det_pixel = (dic['detectorPixel[m]'], dic['detectorPixel[m]'])
+        pad = (dic['padding'], 0, 0)
+        return tEMFQ_GPU_(data, flat, angles, pad, setInterpolation(dic['interpolation']), det_pixel, 0.0,
+                          iterations, gpus, blocksize, obj=obj)
     logger.error(f'Invalid EM method:{method}')
     raise ValueError(f'Invalid EM method:{method}')

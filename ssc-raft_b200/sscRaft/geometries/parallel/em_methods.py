@@ -71,5 +71,41 @@ def em_with_metrics(kind, data, angles, iterations, gpu=0, flat=None, obj=None, 
     return obj, metrics
 
 
-def tEMFQ_GPU_(*args, **kwargs):
-    raise NotImplementedError("tEMFQ is outside this library's scope; use method='tEMRT'")
+def tEMFQ_GPU_(count, flat, angles, pad, interpolation, det_pixel, tv_reg, iterations, gpus, blocksize,
+               obj=None):
+    """Transmission EM with the Fourier-slice projector and the BST
+    back-projector (em_methods.py:153-237 of the reference).  count: photon
+    counts [slices, angles, rays] (not -log); flat [slices, rays]; angles
+    uniform over [0, pi); pad = (padx, 0, 0): the Fourier-slice zero padding;
+    interpolation 0 nearest / 1 bilinear; det_pixel = (x, y), the projection
+    scale is det_pixel x / (rays (1 + padx)) (1 / that length when <= 0);
+    tv_reg unused (as in the reference).  obj: initial guess [slices, N, N] (default ones),
+    updated in place when float32 C-contiguous; returned."""
+    nslices = 1 if len(count.shape) == 2 else count.shape[0]
+    nflats = 1 if len(flat.shape) == 2 else flat.shape[0]
+    nangles, nrays = count.shape[-2], count.shape[-1]
+    objsize = nrays
+    # the library reads one flat row per slice; a single row serves every slice
+    flat = numpy.asarray(flat)
+    if flat.size == nrays and nslices > 1:
+        flat = numpy.broadcast_to(flat.reshape(1, nrays), (nslices, nrays))
+    elif flat.size != nslices * nrays:
+        raise ValueError(f'flat must hold one row of {nrays} rays per slice (or one row for all), '
+                         f'got shape {flat.shape}')
+    gpus_arr, ngpus = _gpus(gpus)
+    if obj is not None:
+        obj = CNICE(obj)
+    else:
+        obj = CNICE(numpy.ones([nslices, objsize, objsize], dtype=numpy.float32))
+    count = CNICE(count)
+    flat = CNICE(flat)
+    angles = CNICE(numpy.array(angles))
+    padx, pady, padz = pad
+    det_pixelx, det_pixely = det_pixel
+    param_int = CNICE(numpy.array([nrays, nangles, nslices, objsize, padx, pady, padz, nflats, iterations,
+                                   interpolation, blocksize]), numpy.int32)
+    param_float = CNICE(numpy.array([det_pixelx, det_pixely, tv_reg]), numpy.float32)
+    libraft.get_tEM_FQ_MultiGPU(_ptr(gpus_arr), ngpus, _ptr(count), _ptr(obj), _ptr(angles), _ptr(flat),
+                                _ptr(param_float), _ptr(param_int))
+    check_error("tEMFQ_GPU_")
+    return obj

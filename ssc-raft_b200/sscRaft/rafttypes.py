@@ -74,6 +74,8 @@ libraft.raft_radon_device.restype = _I
 libraft.raft_background_device.argtypes = [_I, _P, _P, _P, _I, _I, _I, _I, _I, _P]
 libraft.raft_bst_device.argtypes = [_I, _P, _P, _P, _P, _P]
 libraft.raft_bst_device.restype = _I
+libraft.raft_temfq_device.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P]
+libraft.raft_temfq_device.restype = _I
 libraft.raft_background_device.restype = _I
 libraft.raft_em_device.restype = _I
 

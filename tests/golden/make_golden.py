@@ -3,7 +3,8 @@
 Runs on a GPU box: loads oracle/_ref/libraft_ref.so (built from the
 reference sources by oracle/build_ref.sh) and calls its own C ABI
 (getFBPMultiGPU, getFilterLowPassMultiGPU, getRadonRTMultiGPU,
-get_tEM_RT_MultiGPU, get_eEM_RT_MultiGPU, getBackgroundCorrectionMultiGPU)
+get_tEM_RT_MultiGPU, get_eEM_RT_MultiGPU, getBackgroundCorrectionMultiGPU, getBSTMultiGPU,
+the rotation-axis finders and correction, get_tEM_FQ_MultiGPU)
 with the packing of the reference Python wrappers, on small seeded inputs.
 Inputs and outputs are saved together in tests/golden/ref_<case>.npz (or
 under --out); --only PREFIX writes only the cases whose names start with it.
@@ -23,7 +24,7 @@ sys.path.insert(0, os.path.join(REPO, "ssc-raft_b200"))
 sys.path.insert(0, os.path.join(REPO, "tests"))
 sys.path.insert(0, os.path.join(REPO, "oracle"))
 
-from helpers import fbp_params, phantom_case, sino_case  # noqa: E402
+from helpers import fbp_params, phantom_case, sino_case, temfq_counts  # noqa: E402
 
 
 def ptr(a):
@@ -47,6 +48,7 @@ def load_ref():
     lib.findcentersino_subpixel.argtypes = [P, P, P, P, I, I]
     lib.findcentersino_subpixel.restype = F
     lib.getRotAxisCorrectionMultiGPU.argtypes = [P, I, P, F, I, I, I, I]
+    lib.get_tEM_FQ_MultiGPU.argtypes = [P, I, P, P, P, P, P, P]
     return lib
 
 
@@ -183,12 +185,55 @@ def rotaxis_case(lib, seed):
                 out_a=out["out_+1.7"], out_b=out["out_-2.3"])
 
 
+# (name, N, A, nslices, zpad, interpolation, iterations, dx).  Sizes keep N^2 B,
+# N A B, N (1+zpad) A and N (1+zpad) A B / 2 multiples of 1024 (the reference's
+# element-wise grids are size/1024 blocks and skip a tail otherwise), zpad with
+# a convBST grid that covers every sampled frequency, angles k pi / A in [0, pi)
+# with A not a multiple of 3 (no cos/sin of exactly 1/2, so nearest-neighbour
+# rounding never meets a tie that the GPU's fast cosine could break otherwise).
+TEMFQ_CASES = [
+    ("temfq_n64_z1_bilinear", 64, 64, 2, 1, 1, 4, 0.02),
+    ("temfq_n64_z1_nearest", 64, 64, 1, 1, 0, 3, 0.02),
+    ("temfq_n64_z2_bilinear", 64, 64, 2, 2, 1, 3, 0.02),
+    ("temfq_n128_z3_nearest", 128, 80, 1, 3, 0, 2, 0.01),
+]
+
+
+def temfq_case(lib, name, N, A, B, zpad, interp, niter, dx, seed):
+    """One tEMFQ case through the reference's get_tEM_FQ_MultiGPU, packed as
+    tEMFQ_GPU_ (em_methods.py:154-232) packs it, initial guess ones.  Run in a
+    fresh process, like the BST cases (the half-ray padding is never-cleared
+    device memory)."""
+    counts, flat, ang = temfq_counts(N, A, B, dx, seed)
+    obj = np.ones((B, N, N), np.float32)
+    pi = np.array([N, A, B, N, zpad, 0, 0, B, niter, interp, 0], np.int32)
+    pf = np.array([dx, dx, 0.0], np.float32)
+    c, f = counts.copy(), flat.copy()
+    lib.get_tEM_FQ_MultiGPU(ptr(GPUS), 1, ptr(c), ptr(obj), ptr(ang), ptr(f), ptr(pf), ptr(pi))
+    return dict(kind="temfq", counts=counts, flat=flat, angles=ang, zpad=np.int32(zpad), interpolation=np.int32(interp),
+                iterations=np.int32(niter), dx=np.float32(dx), out=obj)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--only", default="")
     ap.add_argument("--bst-case", default="", help=argparse.SUPPRESS)
+    ap.add_argument("--temfq-case", default="", help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.temfq_case:
+        i = [c[0] for c in TEMFQ_CASES].index(args.temfq_case)
+        d = temfq_case(load_ref(), *TEMFQ_CASES[i], seed=1100 + i)
+        np.savez_compressed(os.path.join(args.out, f"ref_{args.temfq_case}.npz"), **d)
+        return
+    if args.only.startswith("temfq"):
+        import subprocess
+        for c in TEMFQ_CASES:
+            if c[0].startswith(args.only):
+                subprocess.run([sys.executable, os.path.abspath(__file__), "--out", args.out, "--temfq-case", c[0]],
+                               check=True)
+        print("wrote", len([c for c in TEMFQ_CASES if c[0].startswith(args.only)]), "tEMFQ fixtures to", args.out)
+        return
     if args.bst_case:
         i = [c[0] for c in BST_CASES].index(args.bst_case)
         d = bst_case(load_ref(), *BST_CASES[i], seed=800 + i)

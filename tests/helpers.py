@@ -35,3 +35,18 @@ def fbp_params(N, A, nslices, pad=2, ftype=7, pixel=1.0, offset=0.0, reg=0.0, be
 
 def ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def temfq_counts(N, A, B, dx, seed):
+    """Seeded transmission counts [B][A][N] of a phantom (attenuation in units
+    of 1/dx per pixel, projections of about 1) with Poisson noise, a flat
+    [B][N] of about 1e4 varying along the rays, and angles k pi / A."""
+    import oracle as O  # only to make the transmission data from a forward projection
+    rng = np.random.default_rng(seed)
+    ang = (np.arange(A) * (np.pi / A)).astype(np.float32)
+    img = phantom_case(N, B, seed=seed)
+    p = O.em_forward(img.astype(np.float64), ang, N) * (N / 2) * dx
+    x = np.arange(N)
+    flat = np.stack([1e4 * (1 + 0.05 * np.cos(2 * np.pi * (x / N + rng.uniform()))) for _ in range(B)])
+    counts = rng.poisson(flat[:, None, :] * np.exp(-p)).astype(np.float32)
+    return counts, flat.astype(np.float32), ang

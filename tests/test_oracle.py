@@ -126,6 +126,9 @@ def _run_oracle(d, oracle, use_tables):
         pi, pf = d["parami"], d["paramf"]
         return oracle.bst(d["sino"], int(pi[7]), int(pi[4]), reg=float(pf[1]), offset=int(pf[6]),
                           pixel=float(pf[4]))
+    if kind == "temfq":
+        return oracle.temfq(d["counts"], d["flat"], d["angles"], int(d["zpad"]), int(d["interpolation"]),
+                            int(d["iterations"]), dx=float(d["dx"]))
     return None
 
 
@@ -135,8 +138,10 @@ def _run_oracle(d, oracle, use_tables):
 # one step dt, so (x+1)/dt lands exactly on a pixel boundary for many
 # samples and the reference's approximate division decides the bin; the
 # oracle divides exactly and does not restate NVIDIA's division.
-LOOSE = {"fbp": 2e-2, "lowpass": 1e-5, "radon": 2e-2, "tem": 2e-3, "eem": 2e-2, "background": 1e-6, "bst": 2e-6}
-TIGHT = {"fbp": 5e-6, "lowpass": 1e-5, "radon": 1e-5, "tem": 1e-3, "eem": 2e-2, "background": 1e-6, "bst": 2e-6}
+LOOSE = {"fbp": 2e-2, "lowpass": 1e-5, "radon": 2e-2, "tem": 2e-3, "eem": 2e-2, "background": 1e-6, "bst": 2e-6,
+         "temfq": 2e-6}
+TIGHT = {"fbp": 5e-6, "lowpass": 1e-5, "radon": 1e-5, "tem": 1e-3, "eem": 2e-2, "background": 1e-6, "bst": 2e-6,
+         "temfq": 2e-6}
 
 
 @pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(f) for f in FIXTURES])

@@ -112,6 +112,30 @@ def test_tem_packing_and_inplace_counts(fake):
     assert np.all(flat == 1)
 
 
+def test_temfq_packing(fake):
+    # tEMFQ_GPU_ packing (em_methods.py:154-232 of the reference): parami of 11,
+    # paramf [pixel x, pixel y, 0 (total variation off)], padding from the dictionary
+    import sscRaft
+    data = np.full((2, 6, 8), 100.0, np.float32)
+    obj = sscRaft.em(data, angles=np.linspace(0, np.pi, 6, endpoint=False),
+                     dic={"gpu": [0], "method": "tEMFQ", "iterations": 5, "padding": 1,
+                          "interpolation": "nearest", "detectorPixel[m]": 2e-6})
+    name, a = fake.calls[-1]
+    assert name == "get_tEM_FQ_MultiGPU"
+    assert list(arr(a[7], 11, ctypes.c_int32)) == [8, 6, 2, 8, 1, 0, 0, 1, 5, 0, 0]   # nflats 1 for a 2-D flat
+    np.testing.assert_allclose(arr(a[6], 3, ctypes.c_float), [2e-6, 2e-6, 0.0])
+    assert np.all(arr(a[5], 16, ctypes.c_float) == 1)                 # default flat: ones per slice
+    assert np.all(arr(a[2], 96, ctypes.c_float) == 100)                # counts as given (no -log)
+    assert obj.shape == (2, 8, 8) and np.all(obj == 1)                 # default initial guess: ones
+    sscRaft.em(data, flat=np.full(8, 7.0), angles=np.zeros(6), dic={"gpu": [0], "method": "tEMFQ"})
+    name, a = fake.calls[-1]
+    assert np.all(arr(a[5], 16, ctypes.c_float) == 7)                 # one flat row serves both slices
+    assert list(arr(a[7], 11, ctypes.c_int32))[4] == 2                 # default padding 2, bilinear
+    assert list(arr(a[7], 11, ctypes.c_int32))[9] == 1
+    with pytest.raises(ValueError):
+        sscRaft.em(data, flat=np.ones((3, 8)), angles=np.zeros(6), dic={"gpu": [0], "method": "tEMFQ"})
+
+
 def test_eem_packing(fake):
     import sscRaft
     data = np.ones((6, 8), np.float32)
