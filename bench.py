@@ -180,6 +180,71 @@ def run_tem(local, dev, nslices=EM_SLICES, iters=EM_ITERS, warm_iters=3):
             "metrics": "FP64 data residual ||flat*exp(-Ax)-y||/||y|| and Poisson NLL per iteration"}
 
 
+# ---------------------------------------------------------------- tEMFQ --
+TEMFQ_ZPAD, TEMFQ_ITERS = 2, 10
+
+
+def temfq_inputs(nslices, dev):
+    """tEMFQ inputs on the tEM workload (nslices x 1024^2, 900 angles over
+    [0, pi), flat I0 = 1e4): counts, flat, a uniform start at the phantoms'
+    mean attenuation, and the pixel size 2/(N-1) that puts the Fourier-slice
+    projection in the units of the tEM data."""
+    import torch
+    trans, ang, x_true = make_tem_data(nslices, 3_000_000, dev)
+    counts = (trans * EM_I0).contiguous()
+    flat = torch.full((nslices, EM_N), EM_I0, dtype=torch.float32, device=dev)
+    x0 = float(np.mean(x_true))
+    return counts, flat, np.ascontiguousarray(ang), x0, 2.0 / (EM_N - 1)
+
+
+def run_temfq(dev, nslices=EM_SLICES, iters=TEMFQ_ITERS, warm_iters=1):
+    """tEMFQ (Fourier-slice projector + BST back-projector) on the tEM
+    workload, padding 2 (3072-point transforms) and bilinear sampling, the
+    reference's defaults: device-resident (raft_temfq_device) and through the
+    drop-in API with pinned host buffers (sscRaft.em -> get_tEM_FQ_MultiGPU)."""
+    import torch
+    import sscRaft
+    from sscRaft.rafttypes import libraft, check_error, _ptr
+    counts, flat, ang, x0, dx = temfq_inputs(nslices, dev)
+    obj = torch.full((nslices, EM_N, EM_N), x0, dtype=torch.float32, device=dev)
+    st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    pf = np.array([dx, dx, 0.0], np.float32)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+
+    def em(n):
+        pi = np.array([EM_N, EM_A, nslices, EM_N, TEMFQ_ZPAD, 0, 0, nslices, n, 1, 0], np.int32)
+        if libraft.raft_temfq_device(dev.index or 0, p(obj), p(counts), p(flat), _ptr(ang), _ptr(pf), _ptr(pi), st):
+            check_error("raft_temfq_device")
+
+    em(warm_iters)
+    torch.cuda.synchronize(dev)
+    obj.fill_(x0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    em(iters)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    dev_obj = obj.cpu().numpy()
+    h_counts = torch.empty(counts.shape, dtype=torch.float32, pin_memory=True)
+    h_counts.copy_(counts)
+    h_flat = flat.cpu().numpy()
+    h_obj = torch.empty(obj.shape, dtype=torch.float32, pin_memory=True)
+    dic = {"gpu": [dev.index or 0], "method": "tEMFQ", "iterations": iters, "padding": TEMFQ_ZPAD,
+           "interpolation": "bilinear", "detectorPixel[m]": dx}
+    h_obj.fill_(x0)
+    t0 = time.perf_counter()
+    sscRaft.em(h_counts.numpy(), flat=h_flat, angles=ang, obj=h_obj.numpy(), dic=dict(dic))
+    ms_e2e = (time.perf_counter() - t0) * 1e3
+    return {"workload": f"tEMFQ {nslices} x {EM_N}^2, {EM_A} angles over [0,pi) x {EM_N} bins, flat I0=1e4, "
+                        f"padding {TEMFQ_ZPAD} ({EM_N * (1 + TEMFQ_ZPAD)}-point transforms), bilinear, "
+                        f"{iters} iterations from a uniform start",
+            "ms_total": ms, "ms_per_iteration": ms / iters,
+            "slice_iterations_per_s": nslices * iters / (ms / 1e3),
+            "e2e_ms": ms_e2e, "e2e_api": "sscRaft.em(method='tEMFQ') -> get_tEM_FQ_MultiGPU, pinned host buffers",
+            "e2e_max_abs_diff_vs_device_path": float(np.abs(h_obj.numpy() - dev_obj).max())}
+
+
 # ---------------------------------------------------------- flat / dark --
 def run_flat_dark(dev, sino, reps=3, hbm_peak=None):
     """Flat/dark correction + -log of a raw-count volume of the FBP workload's
@@ -501,6 +566,11 @@ def run_ours(args):
         if rank == 0:
             print(json.dumps({"quick": True, "op": "flat_dark", **r}), flush=True)
         return
+    if args.quick and args.op == "temfq":
+        r = run_temfq(dev, nslices=args.slices, iters=args.steps, warm_iters=args.warmup)
+        if rank == 0:
+            print(json.dumps({"quick": True, "op": "temfq", **r}), flush=True)
+        return
     if args.quick and args.op == "tem":
         # profiling mode: a short tEM run (args.slices x 1024^2, 900 angles)
         r = run_tem(local, dev, nslices=args.slices, iters=args.steps, warm_iters=args.warmup)
@@ -571,6 +641,7 @@ def run_ours(args):
     ragged_result = None if args.no_ragged else run_ragged(dev)
     warm_result = None if args.no_warm else run_warm(dev)
     flat_dark_result = None if args.no_flat_dark else run_flat_dark(dev, sino, hbm_peak=hbm_peak)
+    temfq_result = None if args.no_temfq else run_temfq(dev)
 
     if rank == 0:
         value = ws * nsl / (ms_dev / 1e3)
@@ -616,6 +687,7 @@ def run_ours(args):
             "ragged": ragged_result,
             "warm_start": warm_result,
             "flat_dark": flat_dark_result,
+            "temfq": temfq_result,
             "clocks": clocks,
             "gpu_launches": int(launches),
         }
@@ -640,6 +712,9 @@ def run_reference(args):
     import torch
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.ref_op == "temfq":
+        run_reference_temfq(args, lib_path, dev, local)
+        return
     S = args.ref_slices
     sino, ang = make_sinograms_gpu(S, 2_000_000, dev)
     h_sino = sino.cpu().numpy()
@@ -684,6 +759,37 @@ def run_reference(args):
     }), flush=True)
 
 
+def run_reference_temfq(args, lib_path, dev, local):
+    """The reference's get_tEM_FQ_MultiGPU on `--ref-slices` slices of the
+    tEMFQ workload (host buffers), for comparison with the ours arm's temfq
+    section; prints its own line."""
+    S = args.ref_slices
+    counts, flat, ang, x0, dx = temfq_inputs(S, dev)
+    h_counts, h_flat = counts.cpu().numpy(), flat.cpu().numpy()
+    lib = ctypes.CDLL(lib_path)
+    P, I = ctypes.c_void_p, ctypes.c_int
+    lib.get_tEM_FQ_MultiGPU.argtypes = [P, I, P, P, P, P, P, P]
+    g = np.array([local], np.intc)
+    pi = np.array([EM_N, EM_A, S, EM_N, TEMFQ_ZPAD, 0, 0, S, TEMFQ_ITERS, 1, S], np.int32)
+    pf = np.array([dx, dx, 0.0], np.float32)
+    obj = np.empty((S, EM_N, EM_N), np.float32)
+
+    def p(a):
+        return a.ctypes.data_as(ctypes.c_void_p)
+
+    ts = []
+    for k in range(args.warmup + args.steps):
+        obj.fill(x0)
+        t0 = time.perf_counter()
+        lib.get_tEM_FQ_MultiGPU(p(g), 1, p(h_counts), p(obj), p(ang), p(h_flat), p(pf), p(pi))
+        if k >= args.warmup:
+            ts.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(ts) / len(ts)
+    print(json.dumps({"impl": "reference", "op": "temfq", "slices": S, "iterations": TEMFQ_ITERS,
+                      "ms_per_call": ms, "ms_per_slice_iteration": ms / (S * TEMFQ_ITERS),
+                      "slice_iterations_per_s": S * TEMFQ_ITERS / (ms / 1e3)}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -697,8 +803,12 @@ def main():
     ap.add_argument("--no-ragged", action="store_true")
     ap.add_argument("--no-warm", action="store_true")
     ap.add_argument("--no-flat-dark", action="store_true")
+    ap.add_argument("--no-temfq", action="store_true")
+    ap.add_argument("--ref-op", default="fbp", choices=["fbp", "temfq"],
+                    help="reference arm: the headline FBP, or tEMFQ on the tEM workload (comparison only)")
     ap.add_argument("--quick", action="store_true", help="device timing of one operator only (profiling)")
-    ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "tem", "ragged", "flat_dark", "bst"])
+    ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "tem", "ragged", "flat_dark", "bst",
+                                                        "temfq"])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

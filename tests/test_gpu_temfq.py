@@ -1,8 +1,9 @@
 """GPU tests of transmission EM with the Fourier-slice projector (tEMFQ):
 get_tEM_FQ_MultiGPU, raft_temfq_device, sscRaft.em(method='tEMFQ').
 
-Tolerances (rel-L2 of the object after a few iterations): <= 1e-4 against
-the reference library's own outputs and against the FP64 oracle.  All three
+Tolerances (rel-L2 of the object after two to four iterations): <= 5e-6
+against the reference library's own outputs (measured <= 7.8e-7) and against
+the FP64 oracle (measured <= 5.2e-7).  All three
 regrid in float with the same geometry and fast sine/cosine; the transforms
 are float here (own FFT) and in the reference (cuFFT), FP64 in the oracle,
 and the EM update multiplies their rounding into the object each iteration.
@@ -47,7 +48,7 @@ def test_temfq_vs_reference_fixtures():
         out = _temfq(counts, d["flat"], d["angles"], int(d["zpad"]), int(d["interpolation"]),
                      int(d["iterations"]), float(d["dx"]))
         assert np.array_equal(counts, d["counts"])                 # counts are not modified
-        assert rel_l2(out, d["out"]) <= 1e-4, (os.path.basename(f), rel_l2(out, d["out"]))
+        assert rel_l2(out, d["out"]) <= 5e-6, (os.path.basename(f), rel_l2(out, d["out"]))
 
 
 @pytest.mark.parametrize("N,A,B,zpad,interp,niter", [(64, 64, 2, 1, 1, 4), (100, 100, 1, 1, 1, 3),
@@ -56,7 +57,7 @@ def test_temfq_vs_oracle(oracle, N, A, B, zpad, interp, niter):
     counts, flat, ang = temfq_counts(N, A, B, 0.02, seed=N + A + zpad)
     out = _temfq(counts, flat, ang, zpad, interp, niter, 0.02)
     ref = oracle.temfq(counts, flat, ang, zpad, interp, niter, dx=0.02)
-    assert rel_l2(out, ref) <= 1e-4, rel_l2(out, ref)
+    assert rel_l2(out, ref) <= 5e-6, rel_l2(out, ref)
 
 
 def test_temfq_zero_pixel_size_and_initial_guess(oracle):
@@ -65,7 +66,7 @@ def test_temfq_zero_pixel_size_and_initial_guess(oracle):
     guess = np.full((1, 64, 64), 0.5, np.float32)
     out = _temfq(counts, flat, ang, 1, 1, 3, 0.0, obj=guess)
     ref = oracle.temfq(counts, flat, ang, 1, 1, 3, obj=guess, dx=0.0)
-    assert rel_l2(out, ref) <= 1e-4, rel_l2(out, ref)
+    assert rel_l2(out, ref) <= 5e-6, rel_l2(out, ref)
 
 
 def test_temfq_chunking_python_and_device_entry():
