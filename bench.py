@@ -322,6 +322,50 @@ def run_warm(dev, samples=256):
     return r
 
 
+def unet_flops_per_image(net, H=512, W=512):
+    """2 * 9 * Cin * Cout * pixels summed over the 3x3 convolutions."""
+    level = {"0": 1, "1": 2, "2": 4, "3": 8}
+    return sum(2.0 * 9 * (c0 + c1) * co * (H // level[name[1]]) * (W // level[name[1]])
+               for name, c0, c1, co in net.LAYERS)
+
+
+def run_unet(dev, samples=256, reps=3):
+    """U-Net inference (the warm start's network) on `samples` 512^2 images in
+    batches of 16: device time per image on the tcgen05 convolution and on the
+    mma.sync convolution, the convolutions' TFLOP/s, and the largest output
+    difference between the two."""
+    import torch
+    from sscRaft import warmstart as W
+    from sscRaft.rafttypes import libraft
+    net = W.UNet.from_file(W.default_weights(), dev)
+    g = torch.Generator(device=dev).manual_seed(12)
+    img = torch.rand((samples, 512, 512), generator=g, device=dev) * 0.01
+    out, ms = {}, {}
+    for name, path in (("tcgen05", 0), ("mma_sync", 1)):
+        libraft.raft_unet_set_conv_path(path)
+        try:
+            net.predict(img[:16])
+            ts = []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                o = net.predict(img)
+                e1.record()
+                torch.cuda.synchronize(dev)
+                ts.append(e0.elapsed_time(e1))
+            ms[name] = statistics.median(ts)
+            out[name] = o
+        finally:
+            libraft.raft_unet_set_conv_path(0)
+    fl = unet_flops_per_image(net)
+    return {"workload": f"U-Net inference, {samples} x 512^2, batches of 16 (4 levels, 32 base channels)",
+            "ms_per_image": {k: v / samples for k, v in ms.items()},
+            "tflops_network": {k: fl * samples / (v / 1e3) / 1e12 for k, v in ms.items()},
+            "speedup_tcgen05_vs_mma_sync": ms["mma_sync"] / ms["tcgen05"],
+            "max_abs_diff": float((out["tcgen05"] - out["mma_sync"]).abs().max()),
+            "max_abs_output": float(out["mma_sync"].abs().max())}
+
+
 # ----------------------------------------------------------- ragged batch --
 def run_ragged(dev, nreq=96, seed=5_000_000, em_iters=30):
     """96 requests, side log-uniform in [256, 2048], angles U[180, 1800], bins =
@@ -566,6 +610,16 @@ def run_ours(args):
         if rank == 0:
             print(json.dumps({"quick": True, "op": "flat_dark", **r}), flush=True)
         return
+    if args.quick and args.op == "unet":
+        r = run_unet(dev, samples=args.slices, reps=max(1, args.steps))
+        if rank == 0:
+            print(json.dumps({"quick": True, "op": "unet", **r}), flush=True)
+        return
+    if args.quick and args.op == "warm":
+        r = run_warm(dev, samples=args.slices)
+        if rank == 0:
+            print(json.dumps({"quick": True, "op": "warm", **r}), flush=True)
+        return
     if args.quick and args.op == "temfq":
         r = run_temfq(dev, nslices=args.slices, iters=args.steps, warm_iters=args.warmup)
         if rank == 0:
@@ -808,7 +862,7 @@ def main():
                     help="reference arm: the headline FBP, or tEMFQ on the tEM workload (comparison only)")
     ap.add_argument("--quick", action="store_true", help="device timing of one operator only (profiling)")
     ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "tem", "ragged", "flat_dark", "bst",
-                                                        "temfq"])
+                                                        "temfq", "unet", "warm"])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

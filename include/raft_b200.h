@@ -255,6 +255,13 @@ int raft_profile_read(double *ms, long long *counts, int nclasses);
  * [Cout][3][3][Cin], FP32 biases / gradients / master weights.  Return 0 on success. */
 int raft_unet_conv_fwd(const void *x0, int C0, const void *x1, int C1, const void *w, const float *bias,
                        void *y, void *y1, int Cy0, int N, int H, int W, int Cout, int relu, void *stream);
+/* Convolution kernel choice: 0 = tcgen05/TMA kernel where its 128-pixel tile fits (W >= 128
+ * or W dividing 128), mma.sync kernel otherwise (default); 1 = mma.sync kernel only;
+ * 2 = tcgen05 kernel only (other shapes fail). */
+int raft_unet_set_conv_path(int path);
+/* 1 if a bounded pipeline wait of the tcgen05 convolution ran out since the last call
+ * (the flag is then cleared); synchronises the current device. */
+int raft_unet_conv_error(void);
 int raft_unet_conv_wgrad(const void *dy, const void *x0, int C0, const void *x1, int C1, float *dw,
                          float *dbias, int N, int H, int W, int Cout, void *stream);
 int raft_unet_flip_weights(const void *w, void *wt, int Cout, int Cin, void *stream);

@@ -308,4 +308,11 @@ struct EmConfig {
     int nflats = 1;
 };
 
+// U-Net 3x3 convolution on tcgen05 (unet_tc.cu): 0 launched, 1 launch error,
+// 2 shape not handled (W must be >= 128 or divide 128; channels multiples of 32).
+bool conv3x3_tc_supported(int C0, int C1, int W);
+int conv3x3_tc(const void *x0, int C0, const void *x1, int C1, const void *w, const float *bias, void *y, void *y1,
+               int Cy0, int N, int H, int W, int Cout, int relu, cudaStream_t st);
+int conv3x3_tc_error();
+
 }  // namespace raft

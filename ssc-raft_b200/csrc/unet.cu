@@ -6,7 +6,9 @@
 // channel counts that are multiples of 32; weights are BF16 [Cout][3][3][Cin]
 // with FP32 master copies; every accumulation is FP32.
 //
-// Kernels (all implicit GEMM on mma.sync.m16n8k16 BF16 -> FP32):
+// The forward / data-gradient convolution runs on the tcgen05 tensor cores
+// (unet_tc.cu) wherever its 128-pixel tile fits; the kernels here are
+// implicit GEMMs on mma.sync.m16n8k16 BF16 -> FP32:
 //   conv3x3_fwd    y = act(conv(x) + b); x may be the channel concatenation
 //                  of two tensors (the decoder's skip connection), read
 //                  in place -- no concatenated copy is materialised
@@ -349,6 +351,140 @@ __global__ void up_bwd_kernel(const bf16 *dy, bf16 *dx, int N, int H, int W, int
     }
 }
 
+// Vectorised forms of the pooling / upsampling passes: one thread per (pixel,
+// group of 8 channels), 16-byte loads and stores, 32-bit index arithmetic
+// (used when every element index fits in 31 bits; C a multiple of 8).
+__device__ __forceinline__ void bf8_to_f(const uint4 v, float *f)
+{
+    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&v);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const float2 t = __bfloat1622float2(h[i]);
+        f[2 * i] = t.x;
+        f[2 * i + 1] = t.y;
+    }
+}
+
+__device__ __forceinline__ uint4 f_to_bf8(const float *f)
+{
+    uint4 v;
+    __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&v);
+#pragma unroll
+    for (int i = 0; i < 4; i++) h[i] = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+    return v;
+}
+
+__global__ void pool_fwd_v8_kernel(const bf16 *x, bf16 *y, int N, int H, int W, int C)
+{
+    const int Ho = H / 2, Wo = W / 2, G = C / 8;
+    const unsigned n = (unsigned)N * Ho * Wo * G;
+    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const unsigned g = e % G, pix = e / G;
+        const unsigned xo = pix % Wo, r = pix / Wo, yo = r % Ho, b = r / Ho;
+        const bf16 *p = x + ((size_t)(b * H + 2 * yo) * W + 2 * xo) * C + 8 * g;
+        float a[8], t[8];
+        bf8_to_f(*reinterpret_cast<const uint4 *>(p), a);
+        bf8_to_f(*reinterpret_cast<const uint4 *>(p + C), t);
+#pragma unroll
+        for (int i = 0; i < 8; i++) a[i] += t[i];
+        bf8_to_f(*reinterpret_cast<const uint4 *>(p + (size_t)W * C), t);
+#pragma unroll
+        for (int i = 0; i < 8; i++) a[i] += t[i];
+        bf8_to_f(*reinterpret_cast<const uint4 *>(p + (size_t)W * C + C), t);
+#pragma unroll
+        for (int i = 0; i < 8; i++) a[i] = 0.25f * (a[i] + t[i]);
+        *reinterpret_cast<uint4 *>(y + (size_t)pix * C + 8 * g) = f_to_bf8(a);
+    }
+}
+
+__global__ void pool_bwd_v8_kernel(const bf16 *dy, bf16 *dx, int N, int H, int W, int C)
+{
+    const int G = C / 8;
+    const unsigned n = (unsigned)N * H * W * G;
+    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const unsigned g = e % G, pix = e / G;
+        const unsigned xx = pix % W, r = pix / W, yy = r % H, b = r / H;
+        float a[8];
+        bf8_to_f(*reinterpret_cast<const uint4 *>(dy + ((size_t)(b * (H / 2) + yy / 2) * (W / 2) + xx / 2) * C + 8 * g),
+                 a);
+#pragma unroll
+        for (int i = 0; i < 8; i++) a[i] *= 0.25f;
+        *reinterpret_cast<uint4 *>(dx + (size_t)pix * C + 8 * g) = f_to_bf8(a);
+    }
+}
+
+__global__ void up_fwd_v8_kernel(const bf16 *x, bf16 *y, int N, int H, int W, int C)
+{
+    const int G = C / 8;
+    const unsigned n = (unsigned)N * 4 * H * W * G;
+    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const unsigned g = e % G, pix = e / G;
+        const unsigned X = pix % (2 * W), r = pix / (2 * W), Y = r % (2 * H), b = r / (2 * H);
+        *reinterpret_cast<uint4 *>(y + (size_t)pix * C + 8 * g) =
+            *reinterpret_cast<const uint4 *>(x + ((size_t)(b * H + Y / 2) * W + X / 2) * C + 8 * g);
+    }
+}
+
+__global__ void up_bwd_v8_kernel(const bf16 *dy, bf16 *dx, int N, int H, int W, int C)
+{
+    const int G = C / 8;
+    const unsigned n = (unsigned)N * H * W * G;
+    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const unsigned g = e % G, pix = e / G;
+        const unsigned xx = pix % W, r = pix / W, yy = r % H, b = r / H;
+        const bf16 *p = dy + ((size_t)(b * 2 * H + 2 * yy) * 2 * W + 2 * xx) * C + 8 * g;
+        const size_t rs = (size_t)2 * W * C;
+        float a[8], t[8];
+        bf8_to_f(*reinterpret_cast<const uint4 *>(p), a);
+        bf8_to_f(*reinterpret_cast<const uint4 *>(p + C), t);
+#pragma unroll
+        for (int i = 0; i < 8; i++) a[i] += t[i];
+        bf8_to_f(*reinterpret_cast<const uint4 *>(p + rs), t);
+#pragma unroll
+        for (int i = 0; i < 8; i++) a[i] += t[i];
+        bf8_to_f(*reinterpret_cast<const uint4 *>(p + rs + C), t);
+#pragma unroll
+        for (int i = 0; i < 8; i++) a[i] += t[i];
+        *reinterpret_cast<uint4 *>(dx + (size_t)pix * C + 8 * g) = f_to_bf8(a);
+    }
+}
+
+// input packing, one thread per pixel: channel 0 = scaled image, the rest zero
+__global__ void input_pack_v8_kernel(const float *img, const float *scale, bf16 *x, int N, int HW, int C)
+{
+    const unsigned n = (unsigned)N * HW;
+    for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        float f[8] = {img[p] * scale[p / HW], 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        uint4 *dst = reinterpret_cast<uint4 *>(x + (size_t)p * C);
+        dst[0] = f_to_bf8(f);
+        for (int g = 1; g < C / 8; g++) dst[g] = make_uint4(0, 0, 0, 0);
+    }
+}
+
+// head, one thread per pixel with 16-byte channel loads (C <= 64, weights in shared memory)
+__global__ void head_fwd_v8_kernel(const bf16 *h, const float *w, const float *b, const float *img,
+                                   const float *scale, float *out, int N, int HW, int C)
+{
+    __shared__ float ws[64];
+    for (int c = threadIdx.x; c < C; c += blockDim.x) ws[c] = w[c];
+    __syncthreads();
+    const unsigned n = (unsigned)N * HW;
+    const float b0 = b[0];
+    for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        float s = b0;
+        const uint4 *src = reinterpret_cast<const uint4 *>(h + (size_t)p * C);
+        for (int g = 0; g < C / 8; g++) {
+            float f[8];
+            bf8_to_f(src[g], f);
+#pragma unroll
+            for (int i = 0; i < 8; i++) s += f[i] * ws[8 * g + i];
+        }
+        out[p] = img[p] * scale[p / HW] + s;
+    }
+}
+
+static bool fits31(size_t n) { return n < ((size_t)1 << 31); }
+
 // input image (FP32 [N][H][W], scaled) -> BF16 NHWC with C channels, channel 0 = image
 __global__ void input_pack_kernel(const float *img, const float *scale, bf16 *x, int N, int H, int W, int C)
 {
@@ -457,6 +593,23 @@ using namespace raft;
 // ------------------------------------------------------------------ C ABI
 extern "C" {
 
+// Which kernel runs the 3x3 convolution: 0 = the tcgen05/TMA kernel (unet_tc.cu)
+// wherever its tile fits (W >= 128 or W dividing 128), else the mma.sync kernel;
+// 1 = the mma.sync kernel only (kept for other widths and for comparison);
+// 2 = the tcgen05 kernel only (a shape it does not take is an error).
+static int g_conv_path = 0;
+
+int raft_unet_set_conv_path(int path)
+{
+    if (path < 0 || path > 2) return 1;
+    g_conv_path = path;
+    return 0;
+}
+
+// 1 if a bounded wait of the tcgen05 convolution ran out since the last call
+// (the flag is cleared); synchronises the current device.
+int raft_unet_conv_error(void) { return conv3x3_tc_error(); }
+
 // y = act(conv3x3(concat(x0, x1)) + bias); C0, C1, Cout multiples of 32 (C1 may be 0).
 // With y1 != NULL the output channels are split: [0, Cy0) -> y, [Cy0, Cout) -> y1
 // (the data gradient of a concatenated input, back into its two parts).
@@ -465,6 +618,11 @@ int raft_unet_conv_fwd(const void *x0, int C0, const void *x1, int C1, const voi
 {
     if (C0 % 32 || C1 % 32 || Cout % 32 || N < 1 || H < 1 || W < 1) return 1;
     if (y1 && (Cy0 % 32 || Cy0 <= 0 || Cy0 >= Cout)) return 1;
+    if (g_conv_path != 1) {
+        const int rc = conv3x3_tc(x0, C0, x1, C1, w, bias, y, y1, Cy0, N, H, W, Cout, relu, (cudaStream_t)stream);
+        if (rc != 2) return rc;
+        if (g_conv_path == 2) return 1;
+    }
     ConvArgs a{(const bf16 *)x0, (const bf16 *)x1, C0, C1, (const bf16 *)w, bias, (bf16 *)y, (bf16 *)y1, Cy0,
                N, H, W, Cout, relu};
     dim3 grid((unsigned)((size_t)N * H * ((W + CV_PIX - 1) / CV_PIX)), Cout / CV_CO);
@@ -506,6 +664,15 @@ int raft_unet_relu_bwd(const void *y, const void *dy, void *dpre, size_t n, void
 int raft_unet_pool(int backward, const void *src, void *dst, int N, int H, int W, int C, void *stream)
 {
     count_launch();
+    if (C % 8 == 0 && fits31((size_t)N * H * W * C)) {
+        if (!backward)
+            pool_fwd_v8_kernel<<<grid_for((size_t)N * H * W * C / 32), 256, 0, (cudaStream_t)stream>>>(
+                (const bf16 *)src, (bf16 *)dst, N, H, W, C);
+        else
+            pool_bwd_v8_kernel<<<grid_for((size_t)N * H * W * C / 8), 256, 0, (cudaStream_t)stream>>>(
+                (const bf16 *)src, (bf16 *)dst, N, H, W, C);
+        return cudaGetLastError() == cudaSuccess ? 0 : 1;
+    }
     if (!backward)
         pool_fwd_kernel<<<grid_for((size_t)N * H * W * C / 4), 256, 0, (cudaStream_t)stream>>>((const bf16 *)src,
                                                                                                 (bf16 *)dst, N, H, W, C);
@@ -519,6 +686,15 @@ int raft_unet_pool(int backward, const void *src, void *dst, int N, int H, int W
 int raft_unet_upsample(int backward, const void *src, void *dst, int N, int H, int W, int C, void *stream)
 {
     count_launch();
+    if (C % 8 == 0 && fits31((size_t)N * 4 * H * W * C)) {
+        if (!backward)
+            up_fwd_v8_kernel<<<grid_for((size_t)N * 4 * H * W * C / 8), 256, 0, (cudaStream_t)stream>>>(
+                (const bf16 *)src, (bf16 *)dst, N, H, W, C);
+        else
+            up_bwd_v8_kernel<<<grid_for((size_t)N * H * W * C / 8), 256, 0, (cudaStream_t)stream>>>(
+                (const bf16 *)src, (bf16 *)dst, N, H, W, C);
+        return cudaGetLastError() == cudaSuccess ? 0 : 1;
+    }
     if (!backward)
         up_fwd_kernel<<<grid_for((size_t)N * 4 * H * W * C), 256, 0, (cudaStream_t)stream>>>(
             (const bf16 *)src, (bf16 *)dst, N, H, W, C);
@@ -531,6 +707,11 @@ int raft_unet_upsample(int backward, const void *src, void *dst, int N, int H, i
 int raft_unet_input(const float *img, const float *scale, void *x, int N, int H, int W, int C, void *stream)
 {
     count_launch();
+    if (C % 8 == 0 && fits31((size_t)N * H * W * C)) {
+        input_pack_v8_kernel<<<grid_for((size_t)N * H * W), 256, 0, (cudaStream_t)stream>>>(img, scale, (bf16 *)x, N,
+                                                                                             H * W, C);
+        return cudaGetLastError() == cudaSuccess ? 0 : 1;
+    }
     input_pack_kernel<<<grid_for((size_t)N * H * W * C), 256, 0, (cudaStream_t)stream>>>(img, scale, (bf16 *)x, N, H,
                                                                                         W, C);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
@@ -542,6 +723,11 @@ int raft_unet_head(int backward, const void *h, const float *w, const float *b, 
 {
     if (C > 64) return 1;
     count_launch();
+    if (!backward && C % 8 == 0 && fits31((size_t)N * HW * C)) {
+        head_fwd_v8_kernel<<<grid_for((size_t)N * HW), 256, 0, (cudaStream_t)stream>>>((const bf16 *)h, w, b, img, scale,
+                                                                                       out_or_grad, N, HW, C);
+        return cudaGetLastError() == cudaSuccess ? 0 : 1;
+    }
     if (!backward)
         head_fwd_kernel<<<grid_for((size_t)N * HW), 256, 0, (cudaStream_t)stream>>>((const bf16 *)h, w, b, img, scale,
                                                                                     out_or_grad, N, HW, C);

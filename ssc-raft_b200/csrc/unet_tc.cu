@@ -1,0 +1,539 @@
+// unet_tc.cu -- the U-Net's 3x3 convolution on the 5th-generation tensor
+// cores (tcgen05.mma, accumulators in tensor memory), operands staged by TMA.
+//
+// Implicit GEMM: D[pixel][co] = sum over (tap, ci) of X[pixel + tap][ci] * W[co][tap][ci].
+// One tile = MT x 128 output pixels (BW consecutive pixels of BH image rows,
+// BW = 256 / 128 / W) x BN output channels.  Per k-block (one tap, KC input
+// channels) the producer issues two TMA loads into a pipeline stage:
+//   A: box (KC channels, BW pixels, BH rows) of the NHWC input at
+//      (c0, x0 + kx, y0 + ky, n) -- the 3x3 halo outside the image arrives as
+//      zeros from the TMA unit's out-of-bounds fill, no padded copy exists;
+//   B: box (KC, BN) of the weights viewed as [Cout][9 Cin].
+// Both land 128-byte (KC = 64) or 64-byte (KC = 32) swizzled, the K-major
+// layout the MMA's shared-memory descriptors describe.  One thread issues
+// MT x KC/16 tcgen05.mma (M = 128, N = BN, K = 16, BF16 x BF16 -> FP32) per
+// k-block into MT TMEM accumulators and commits the stage back to the producer
+// (MT > 1 spreads the fixed cost of a pipeline step -- the barrier handoffs
+// and issue of one k-block, about 0.3 us -- over more tensor-core work);
+// the accumulator is double-buffered in TMEM so the epilogue of one tile
+// (tcgen05.ld, bias, ReLU, BF16, NHWC store, optional split of the output
+// channels into two tensors) overlaps the MMAs of the next.  CTAs are
+// persistent over the tiles.
+//
+// Warp roles (192 threads): warp 0 = TMA producer, warp 1 = TMEM owner and
+// MMA issuer, warps 2-5 = epilogue (warp w reads TMEM lanes 32 (w mod 4) ..).
+// Every mbarrier wait is bounded; a wait that runs out sets the CTA's abort
+// flag and the library's error flag, every role then leaves its loop, the
+// MMA issuer drains its outstanding MMAs (bounded) and TMEM is released.
+// No cluster launch and no multicast: every TMA load reads this GPU's memory
+// into this CTA's shared memory.
+#include "raft.hpp"
+#include "profile.hpp"
+#include "ptx.hpp"
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <mutex>
+
+namespace raft {
+
+namespace {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int TC_M = 128;                 // output pixels per tile (MMA M)
+constexpr int TC_THREADS = 192;
+constexpr uint32_t TC_WAIT_LIMIT = 1u << 20;   // polls of try_wait (at least ~0.1 s)
+
+struct TcArgs {
+    bf16 *y, *y1;          // outputs (see raft_unet_conv_fwd)
+    int Cy0;
+    const float *bias;     // [Cout] or null
+    int N, H, W, Cout, C0, C1;
+    int BW, BH, n_xb, n_yb, n_co, tiles;
+    int relu;
+    int *err;              // library error flag (set on a wait that runs out)
+};
+
+// --------------------------------------------------------------- tcgen05
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                 "r"(ncols)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_relinquish()
+{
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// arrive on `bar` once every tcgen05.mma issued so far by this thread has completed
+__device__ __forceinline__ void tc_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// D[tmem] (+)= A[smem desc] * B[smem desc]^T, kind::f16 (BF16 in, FP32 accumulate)
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+// 32 consecutive 32-bit TMEM columns of this thread's lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor, K-major, swizzled rows: start address,
+// leading offset 16 B (unused for swizzled K-major), stride offset = one
+// 8-row swizzle atom, descriptor version 1, layout (2 = 128 B, 4 = 64 B swizzle).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t sbo_bytes, uint32_t layout)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)layout << 61);
+}
+
+// ------------------------------------------------------------------- TMA
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int c0, int c1, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait that also gives up when another role has aborted.
+__device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err)
+{
+    for (uint32_t it = 0; it < TC_WAIT_LIMIT; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 255) == 255 && *abort_flag) return false;
+    }
+    *abort_flag = 1;
+    if (err) atomicExch(err, 1);
+    return false;
+}
+
+struct TileCoord {
+    int n, y0, x0, co0;
+};
+
+__device__ __forceinline__ TileCoord tile_coord(const TcArgs &a, int t, int BN)
+{
+    TileCoord c;
+    const int cot = t % a.n_co;
+    int r = t / a.n_co;
+    const int xb = r % a.n_xb;
+    r /= a.n_xb;
+    const int yb = r % a.n_yb;
+    c.n = r / a.n_yb;
+    c.y0 = yb * a.BH;
+    c.x0 = xb * a.BW;
+    c.co0 = cot * BN;
+    return c;
+}
+
+template <int BN, int KC, int MT, int ST>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    conv3x3_tc_kernel(const __grid_constant__ CUtensorMap mx0, const __grid_constant__ CUtensorMap mx1,
+                      const __grid_constant__ CUtensorMap mw, const TcArgs a)
+{
+    constexpr int A_PART = TC_M * KC * 2;                  // one 128-row MMA operand
+    constexpr int A_BYTES = MT * A_PART, B_BYTES = BN * KC * 2, STAGE = A_BYTES + B_BYTES;
+    constexpr uint32_t SBO = 8 * KC * 2;                   // one 8-row swizzle atom
+    constexpr uint32_t LAYOUT = KC == 64 ? 2u : 4u;        // 128-byte / 64-byte swizzle
+    constexpr uint32_t ACC = MT * BN;                      // TMEM columns of one accumulator buffer
+    constexpr uint32_t TMEM_COLS = 2 * ACC < 32 ? 32 : 2 * ACC;
+    static_assert(2 * ACC <= 512, "two accumulator buffers must fit in TMEM");
+    static_assert(STAGE % 1024 == 0, "stages must keep 1024-byte alignment");
+    static_assert(BN % 32 == 0 && BN <= 256 && (KC == 32 || KC == 64), "tile shape");
+    // instruction descriptor: D F32, A/B BF16, both K-major, N = BN, M = 128
+    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(TC_M >> 4) << 24);
+
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + ST * STAGE);
+    uint64_t *empty = full + ST;
+    uint64_t *accf = empty + ST;
+    uint64_t *acce = accf + 2;
+    uint64_t *drain = acce + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < ST; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&accf[b], 1);
+            mbar_init(&acce[b], 128);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const int Cin = a.C0 + a.C1;
+    const int kb_per_tile = 9 * (Cin / KC);
+
+    if (warp == 0) {
+        // ---------------------------------------------------------- producer
+        if (lane == 0) {
+            uint32_t g = 0;                      // k-blocks issued so far
+            bool ok = true;
+            for (int t = blockIdx.x; t < a.tiles && ok; t += gridDim.x) {
+                const TileCoord c = tile_coord(a, t, BN);
+                for (int kb = 0; kb < kb_per_tile && ok; ++kb, ++g) {
+                    const int tap = kb / (Cin / KC), cc = (kb % (Cin / KC)) * KC;
+                    const int ky = tap / 3 - 1, kx = tap % 3 - 1;
+                    const int s = (int)(g % ST);
+                    const uint32_t u = g / ST;
+                    if (u >= 1 && !(ok = tc_wait(&empty[s], (u - 1) & 1, abort_flag, a.err))) break;
+                    uint8_t *st = base + s * STAGE;
+                    mbar_arrive_expect_tx(&full[s], STAGE);
+                    if (cc < a.C0) tma_load_4d(st, &mx0, cc, c.x0 + kx, c.y0 + ky, c.n, &full[s]);
+                    else tma_load_4d(st, &mx1, cc - a.C0, c.x0 + kx, c.y0 + ky, c.n, &full[s]);
+                    tma_load_2d(st + A_BYTES, &mw, tap * Cin + cc, c.co0, &full[s]);
+                }
+            }
+            // every issued load lands before the CTA may exit: the last use of
+            // stage s was k-block s + ST * ((g - 1 - s) / ST)
+            for (uint32_t s = 0; s < (uint32_t)ST && s < g; ++s)
+                mbar_wait_bounded(&full[s], ((g - 1 - s) / ST) & 1, TC_WAIT_LIMIT);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ------------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            uint32_t g = 0;
+            bool ok = true;
+            int i = 0;
+            for (int t = blockIdx.x; t < a.tiles && ok; t += gridDim.x, ++i) {
+                const int buf = i & 1, v = i >> 1;
+                if (v >= 1 && !(ok = tc_wait(&acce[buf], (v - 1) & 1, abort_flag, a.err))) break;
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)buf * ACC;
+                for (int kb = 0; kb < kb_per_tile; ++kb, ++g) {
+                    const int s = (int)(g % ST);
+                    const uint32_t u = g / ST;
+                    if (!(ok = tc_wait(&full[s], u & 1, abort_flag, a.err))) break;
+                    tc_fence_after();
+                    const uint32_t sa = smem_u32(base + s * STAGE);
+                    const uint64_t bd = umma_desc(sa + A_BYTES, SBO, LAYOUT);
+#pragma unroll
+                    for (int mt = 0; mt < MT; ++mt) {
+                        const uint64_t ad = umma_desc(sa + mt * A_PART, SBO, LAYOUT);
+#pragma unroll
+                        for (int j = 0; j < KC / 16; ++j)   // K = 16 per MMA: 32 bytes further along the swizzled row
+                            tc_mma(d + mt * BN, ad + (uint64_t)(2 * j), bd + (uint64_t)(2 * j), IDESC, (kb | j) != 0);
+                    }
+                    tc_commit(&empty[s]);
+                }
+                if (ok) tc_commit(&accf[buf]);
+            }
+            // all MMAs issued by this thread complete before TMEM is released
+            tc_commit(drain);
+            mbar_wait_bounded(drain, 0, TC_WAIT_LIMIT);
+        }
+        __syncwarp();
+    } else {
+        // --------------------------------------------------------- epilogue
+        const int q = warp & 3;                 // TMEM lane quarter of this warp
+        int i = 0;
+        for (int t = blockIdx.x; t < a.tiles; t += gridDim.x, ++i) {
+            const int buf = i & 1, v = i >> 1;
+            if (!tc_wait(&accf[buf], v & 1, abort_flag, a.err)) break;
+            tc_fence_after();
+            const TileCoord c = tile_coord(a, t, BN);
+#pragma unroll 1
+            for (int part = 0; part < MT * (BN / 32); ++part) {
+                const int mt = part / (BN / 32), ch = part % (BN / 32);
+                const int m = TC_M * mt + 32 * q + lane;        // tile pixel of this thread
+                const int yy = c.y0 + m / a.BW, xx = c.x0 + m % a.BW;
+                const bool valid = yy < a.H && xx < a.W;
+                const size_t pix = ((size_t)c.n * a.H + yy) * a.W + xx;
+                uint32_t r[32];
+                tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)buf * ACC + (uint32_t)(mt * BN + 32 * ch), r);
+                const int co = c.co0 + 32 * ch;
+                if (!valid) continue;
+                float f[32];
+#pragma unroll
+                for (int e = 0; e < 32; ++e) f[e] = __uint_as_float(r[e]);
+                if (a.bias) {
+#pragma unroll
+                    for (int e = 0; e < 32; ++e) f[e] += __ldg(a.bias + co + e);
+                }
+                if (a.relu) {
+#pragma unroll
+                    for (int e = 0; e < 32; ++e) f[e] = fmaxf(f[e], 0.f);
+                }
+                bf16 *dst;
+                if (a.y1 && co >= a.Cy0) dst = a.y1 + pix * (a.Cout - a.Cy0) + (co - a.Cy0);
+                else if (a.y1) dst = a.y + pix * a.Cy0 + co;
+                else dst = a.y + pix * a.Cout + co;
+#pragma unroll
+                for (int e = 0; e < 32; e += 8) {
+                    __nv_bfloat162 h0 = __floats2bfloat162_rn(f[e], f[e + 1]);
+                    __nv_bfloat162 h1 = __floats2bfloat162_rn(f[e + 2], f[e + 3]);
+                    __nv_bfloat162 h2 = __floats2bfloat162_rn(f[e + 4], f[e + 5]);
+                    __nv_bfloat162 h3 = __floats2bfloat162_rn(f[e + 6], f[e + 7]);
+                    uint4 pk;
+                    pk.x = *reinterpret_cast<uint32_t *>(&h0);
+                    pk.y = *reinterpret_cast<uint32_t *>(&h1);
+                    pk.z = *reinterpret_cast<uint32_t *>(&h2);
+                    pk.w = *reinterpret_cast<uint32_t *>(&h3);
+                    *reinterpret_cast<uint4 *>(dst + e) = pk;
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&acce[buf]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+// ------------------------------------------------------------------ host
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+int *tc_err_flag(int device)
+{
+    static std::mutex mu;
+    static int *flags[64] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    if (device < 0 || device >= 64) return nullptr;
+    if (!flags[device]) {
+        if (cudaMalloc(&flags[device], sizeof(int)) != cudaSuccess) return nullptr;
+        cudaMemset(flags[device], 0, sizeof(int));
+    }
+    return flags[device];
+}
+
+// pipeline depth: as many stages as fit in 196 KB, at most 16 (the loads in
+// flight are what hides the L2 latency of the per-tap operand tiles)
+// 128-pixel MMA blocks per tile: two accumulator buffers of MT x BN columns
+// within TMEM's 512, an A operand of at most 32 KB
+template <int BN, int KC>
+constexpr int tc_mt()
+{
+    return (256 / BN < 4 ? 256 / BN : 4) < 32768 / (TC_M * KC * 2) ? (256 / BN < 4 ? 256 / BN : 4)
+                                                                   : 32768 / (TC_M * KC * 2);
+}
+
+template <int BN, int KC>
+constexpr int tc_stage_bytes()
+{
+    return tc_mt<BN, KC>() * TC_M * KC * 2 + BN * KC * 2;
+}
+
+template <int BN, int KC>
+constexpr int tc_stages()
+{
+    return (196 * 1024) / tc_stage_bytes<BN, KC>() > 16 ? 16 : (196 * 1024) / tc_stage_bytes<BN, KC>();
+}
+
+template <int BN, int KC>
+int launch_tc(const CUtensorMap &m0, const CUtensorMap &m1, const CUtensorMap &mw, const TcArgs &a,
+              cudaStream_t st)
+{
+    constexpr int MT = tc_mt<BN, KC>(), ST = tc_stages<BN, KC>();
+    constexpr size_t SMEM = (size_t)ST * tc_stage_bytes<BN, KC>() + 1024 + 256;
+    auto kern = conv3x3_tc_kernel<BN, KC, MT, ST>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM) != cudaSuccess) return 1;
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    int dev = 0, sms = 148, occ = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TC_THREADS, SMEM) != cudaSuccess || occ < 1)
+        occ = 1;
+    const int grid = std::max(1, std::min(a.tiles, sms * occ));
+    count_launch();
+    kern<<<grid, TC_THREADS, SMEM, st>>>(m0, m1, mw, a);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+bool encode_act(CUtensorMap *m, const void *ptr, int C, int N, int H, int W, int KC, int BW, int BH)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return false;
+    cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+    cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+    cuuint32_t box[4] = {(cuuint32_t)KC, (cuuint32_t)BW, (cuuint32_t)BH, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(ptr), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, KC == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool encode_w(CUtensorMap *m, const void *ptr, int Cout, int Cin, int KC, int BN)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)9 * Cin, (cuuint64_t)Cout};
+    cuuint64_t strides[1] = {(cuuint64_t)9 * Cin * 2};
+    cuuint32_t box[2] = {(cuuint32_t)KC, (cuuint32_t)BN};
+    cuuint32_t es[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, KC == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+bool conv3x3_tc_supported(int C0, int C1, int W)
+{
+    if (C0 % 32 || C1 % 32 || C0 <= 0) return false;
+    if (W >= TC_M) return true;
+    return W > 0 && TC_M % W == 0;
+}
+
+// 0 = launched, 1 = launch error, 2 = shape not handled here (caller uses the mma.sync kernel)
+int conv3x3_tc(const void *x0, int C0, const void *x1, int C1, const void *w, const float *bias, void *y, void *y1,
+               int Cy0, int N, int H, int W, int Cout, int relu, cudaStream_t st)
+{
+    if (!conv3x3_tc_supported(C0, C1, W) || Cout % 32 || Cout <= 0) return 2;
+    const int KC = (C0 % 64 == 0 && C1 % 64 == 0) ? 64 : 32;
+    const int BN = Cout % 256 == 0 ? 256 : Cout % 128 == 0 ? 128 : Cout % 64 == 0 ? 64 : 32;
+    int MT = 1;
+    switch (BN * 100 + KC) {
+    case 25664: MT = tc_mt<256, 64>(); break;
+    case 25632: MT = tc_mt<256, 32>(); break;
+    case 12864: MT = tc_mt<128, 64>(); break;
+    case 12832: MT = tc_mt<128, 32>(); break;
+    case 6464: MT = tc_mt<64, 64>(); break;
+    case 6432: MT = tc_mt<64, 32>(); break;
+    case 3264: MT = tc_mt<32, 64>(); break;
+    default: MT = tc_mt<32, 32>(); break;
+    }
+    TcArgs a;
+    a.y = (bf16 *)y;
+    a.y1 = (bf16 *)y1;
+    a.Cy0 = Cy0;
+    a.bias = bias;
+    a.N = N;
+    a.H = H;
+    a.W = W;
+    a.Cout = Cout;
+    a.C0 = C0;
+    a.C1 = C1;
+    // box of MT x 128 pixels: 256-pixel row segments where the image is that
+    // wide, else 128-pixel segments, else whole rows
+    a.BW = (W >= 2 * TC_M && MT >= 2) ? 2 * TC_M : (W >= TC_M ? TC_M : W);
+    a.BH = MT * TC_M / a.BW;
+    a.n_xb = (W + a.BW - 1) / a.BW;
+    a.n_yb = (H + a.BH - 1) / a.BH;
+    a.n_co = Cout / BN;
+    const long long tiles = (long long)N * a.n_yb * a.n_xb * a.n_co;
+    if (tiles <= 0 || tiles > (1LL << 30)) return 2;
+    a.tiles = (int)tiles;
+    a.relu = relu;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    a.err = tc_err_flag(dev);
+    CUtensorMap m0, m1, mw;
+    if (!encode_act(&m0, x0, C0, N, H, W, KC, a.BW, a.BH)) return 2;
+    if (C1 > 0) {
+        if (!encode_act(&m1, x1, C1, N, H, W, KC, a.BW, a.BH)) return 2;
+    } else {
+        m1 = m0;
+    }
+    if (!encode_w(&mw, w, Cout, C0 + C1, KC, BN)) return 2;
+    switch (BN * 100 + KC) {
+    case 25664: return launch_tc<256, 64>(m0, m1, mw, a, st);
+    case 25632: return launch_tc<256, 32>(m0, m1, mw, a, st);
+    case 12864: return launch_tc<128, 64>(m0, m1, mw, a, st);
+    case 12832: return launch_tc<128, 32>(m0, m1, mw, a, st);
+    case 6464: return launch_tc<64, 64>(m0, m1, mw, a, st);
+    case 6432: return launch_tc<64, 32>(m0, m1, mw, a, st);
+    case 3264: return launch_tc<32, 64>(m0, m1, mw, a, st);
+    default: return launch_tc<32, 32>(m0, m1, mw, a, st);
+    }
+}
+
+// Reads and clears the tensor-core convolution's error flag of the current device
+// (1 = a bounded wait ran out).  Synchronises the device.
+int conv3x3_tc_error()
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int *f = tc_err_flag(dev);
+    if (!f) return 0;
+    int h = 0;
+    if (cudaMemcpy(&h, f, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+    if (h) cudaMemset(f, 0, sizeof(int));
+    return h;
+}
+
+}  // namespace raft

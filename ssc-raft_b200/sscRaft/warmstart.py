@@ -34,7 +34,9 @@ libraft.raft_unet_mse.argtypes = [_P, _P, _P, _P, _P, _I, _I, _P]
 libraft.raft_unet_adam.argtypes = [_P, _P, _P, _P, _P, _Z, _F, _F, _F, _F, _I, _P]
 libraft.raft_unet_add.argtypes = [_P, _P, _Z, _P]
 libraft.raft_unet_to_bf16.argtypes = [_P, _P, _Z, _P]
-for _f in ("raft_unet_conv_fwd", "raft_unet_conv_wgrad", "raft_unet_flip_weights", "raft_unet_relu_bwd",
+libraft.raft_unet_set_conv_path.argtypes = [_I]
+libraft.raft_unet_conv_error.argtypes = []
+for _f in ("raft_unet_set_conv_path", "raft_unet_conv_error", "raft_unet_conv_fwd", "raft_unet_conv_wgrad", "raft_unet_flip_weights", "raft_unet_relu_bwd",
            "raft_unet_pool", "raft_unet_upsample", "raft_unet_input", "raft_unet_head", "raft_unet_mse",
            "raft_unet_adam", "raft_unet_add", "raft_unet_to_bf16"):
     getattr(libraft, _f).restype = _I
@@ -250,7 +252,13 @@ class UNet:
             o = self.forward(x, sc) / sc[:, None, None]
             floor = 1e-3 * torch.clamp(x.abs().mean(dim=(1, 2)), min=1e-12)
             res[i:i + batch] = torch.maximum(o, floor[:, None, None])
+        self.check()
         return res
+
+    def check(self):
+        """Raises if a bounded wait of the tensor-core convolution ran out since
+        the last check (synchronises the device)."""
+        _ok(libraft.raft_unet_conv_error(), "tensor-core convolution: a pipeline wait timed out")
 
     def state(self):
         return {k: v.detach().cpu().numpy() for k, v in list(self.w.items())} | \
