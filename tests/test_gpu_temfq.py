@@ -61,9 +61,10 @@ def test_temfq_vs_oracle(oracle, N, A, B, zpad, interp, niter):
 
 
 def test_temfq_zero_pixel_size_and_initial_guess(oracle):
-    # dx <= 0: scale 1 / (N (1 + zpad)); a non-trivial initial guess
+    # dx <= 0: scale 1 / (N (1 + zpad)), i.e. attenuation per pixel; counts whose
+    # attenuation is about 0.01 per pixel and a uniform initial guess near it
     counts, flat, ang = temfq_counts(64, 64, 1, 1.0 / 128, seed=3)
-    guess = np.full((1, 64, 64), 0.5, np.float32)
+    guess = np.full((1, 64, 64), 0.01, np.float32)
     out = _temfq(counts, flat, ang, 1, 1, 3, 0.0, obj=guess)
     ref = oracle.temfq(counts, flat, ang, 1, 1, 3, obj=guess, dx=0.0)
     assert rel_l2(out, ref) <= 5e-6, rel_l2(out, ref)
