@@ -319,9 +319,10 @@ int raft_fbp_device(int gpu, float *d_obj, const float *d_tomogram, const float 
         const size_t tomo_ps = (size_t)cfg.nangles * cfg.nrays;
         const int chunk = std::max(1, std::min(cfg.nslices, cfg.blocksize > 0 ? cfg.blocksize : 32));
         void *rows = ds.rows.get(fbp_rows_bytes(fp, chunk));
+        void *il = fbp_il_bytes(fp, chunk) ? ds.il.get(fbp_il_bytes(fp, chunk)) : nullptr;
         for (int s0 = 0; s0 < cfg.nslices; s0 += chunk) {
             const int ns = std::min(chunk, cfg.nslices - s0);
-            fbp_chunk(ds, fp, tb, d_tomogram + tomo_ps * s0, d_obj + (size_t)fp.No * fp.No * s0, ns, rows, st);
+            fbp_chunk(ds, fp, tb, d_tomogram + tomo_ps * s0, d_obj + (size_t)fp.No * fp.No * s0, ns, rows, st, il);
         }
         if (!stream) RAFT_CUDA(cudaStreamSynchronize(st));
     } catch (const CudaFail &) {

@@ -62,6 +62,7 @@ struct BpArgs {
     const double *csd, *snd;     // FP64 tables
     int *err;
     int update;                  // 0: store, 1: img = img * acc / den
+    int il;                      // 1: filt holds groups of 4 slices interleaved, [group][angle][Wg][4]
 };
 
 constexpr uint32_t kWaitLimit = 1u << 24;
@@ -148,18 +149,22 @@ __device__ __forceinline__ float lerp_fetch(const unsigned char *w, int k, float
 //
 // S slices share one CTA: the per-pixel position, rounding and window index
 // are computed once per (pixel, angle) and reused for every slice, whose
-// windows sit side by side in shared memory ([angle][slice][W]), so the
-// per-slice address is the shared one plus an immediate offset.  AB (angles
-// per pipeline stage) is a launch parameter; S and AB are chosen by the
-// autotuner below.
+// windows sit side by side in shared memory ([angle][slice][W]).  With IL
+// (S = 4, 4-byte elements) the rows arrive interleaved by slice
+// ([group][angle][Wg][4], see interleave4_kernel), the staged windows are
+// [angle][W][4] and one 16-byte load fetches the sample of all four slices:
+// one bulk copy per angle instead of four, one shared-memory instruction per
+// (pixel, angle) instead of four.  AB (angles per pipeline stage) is a launch
+// parameter; S and AB are chosen by the autotuner below.
 // ------------------------------------------------------------------------
 // One 64 x 32 tile of S slices.  `gstage` counts the pipeline stages this
 // CTA has consumed so far (a persistent CTA runs many tiles through the same
 // two buffers and mbarriers); returns false if a staging wait timed out.
-template <int GEOM, int STORE, int S>
+template <int GEOM, int STORE, int S, bool IL = false>
 __device__ __forceinline__ bool bp_tile(const BpArgs &p, const int AB, const int x0, const int y0,
                                         const int slice0, unsigned char *smem, uint32_t &gstage)
 {
+    static_assert(!IL || (S == 4 && STORE != STORE_PAIR_F32 && GEOM != GEOM_FBP_LIN), "interleaved: 4 x f32");
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     AngleParam *prm = reinterpret_cast<AngleParam *>(smem + 128);
     unsigned char *win = smem + kWinOffset;
@@ -182,7 +187,8 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &p, const int AB, const int
 #pragma unroll
     for (int j = 0; j < 2; j++) lj[j] = wy * 8 + ly + 4 * j;
 
-    const unsigned char *rows = p.filt + (size_t)slice0 * A * p.Wg * esize;
+    const unsigned char *rows = IL ? p.filt + (size_t)(slice0 / 4) * A * p.Wg * 16
+                                   : p.filt + (size_t)slice0 * A * p.Wg * esize;
     const size_t slice_stride = (size_t)A * p.Wg * esize;
 
     auto issue = [&](int s, int b) {
@@ -197,16 +203,24 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &p, const int AB, const int
         }
         if (lane == 0) {
             fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&bars[b], (uint32_t)(na * nsl * wbytes));
+            mbar_arrive_expect_tx(&bars[b], (uint32_t)(na * (IL ? S : nsl) * wbytes));
         }
         __syncwarp();
         unsigned char *dst = win + (size_t)b * stage_bytes;
-        for (int c = lane; c < na * nsl; c += 32) {
-            const int al = c / nsl, sl = c - al * nsl;
-            const int base = prm[b * 32 + al].d - (GEOM == GEOM_FBP_LIN ? 0 : p.wlo);
-            bulk_g2s(dst + (size_t)(al * S + sl) * wbytes,
-                     rows + sl * slice_stride + ((size_t)(a0 + al) * p.Wg + base) * esize, (uint32_t)wbytes,
-                     &bars[b]);
+        if constexpr (IL) {
+            // one copy of the four interleaved windows per angle
+            for (int al = lane; al < na; al += 32)
+                bulk_g2s(dst + (size_t)al * S * wbytes,
+                         rows + ((size_t)(a0 + al) * p.Wg + prm[b * 32 + al].d - p.wlo) * 16, (uint32_t)(S * wbytes),
+                         &bars[b]);
+        } else {
+            for (int c = lane; c < na * nsl; c += 32) {
+                const int al = c / nsl, sl = c - al * nsl;
+                const int base = prm[b * 32 + al].d - (GEOM == GEOM_FBP_LIN ? 0 : p.wlo);
+                bulk_g2s(dst + (size_t)(al * S + sl) * wbytes,
+                         rows + sl * slice_stride + ((size_t)(a0 + al) * p.Wg + base) * esize, (uint32_t)wbytes,
+                         &bars[b]);
+            }
         }
     };
 
@@ -283,9 +297,17 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &p, const int AB, const int
                         const float t = __fmaf_rn(xr[i], c, ys);
                         int ti = (int)((t - p.tmin) / p.dt);
                         const unsigned k = min((unsigned)(ti - wbase), (unsigned)(W - 1));
-                        const float *wk = reinterpret_cast<const float *>(w) + k;
+                        if constexpr (IL) {
+                            const float4 v = reinterpret_cast<const float4 *>(w)[k];
+                            acc[0][j][i] += v.x;
+                            acc[1][j][i] += v.y;
+                            acc[2][j][i] += v.z;
+                            acc[3][j][i] += v.w;
+                        } else {
+                            const float *wk = reinterpret_cast<const float *>(w) + k;
 #pragma unroll
-                        for (int q = 0; q < S; q++) acc[q][j][i] += wk[q * W];
+                            for (int q = 0; q < S; q++) acc[q][j][i] += wk[q * W];
+                        }
                     }
                 }
             }
@@ -321,7 +343,7 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &p, const int AB, const int
 }
 
 
-template <int GEOM, int STORE, int S>
+template <int GEOM, int STORE, int S, bool IL = false>
 __device__ __forceinline__ void bp_body(const BpArgs &p, const int AB)
 {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -333,7 +355,7 @@ __device__ __forceinline__ void bp_body(const BpArgs &p, const int AB)
     }
     __syncthreads();
     uint32_t gstage = 0;
-    bp_tile<GEOM, STORE, S>(p, AB, blockIdx.x * BP_TX, blockIdx.y * BP_TY, blockIdx.z * S, smem, gstage);
+    bp_tile<GEOM, STORE, S, IL>(p, AB, blockIdx.x * BP_TX, blockIdx.y * BP_TY, blockIdx.z * S, smem, gstage);
 }
 
 template <int GEOM, int STORE, int S>
@@ -344,10 +366,25 @@ __global__ void __launch_bounds__(BP_THREADS) bp_kernel(const BpArgs p, const in
 
 // The S = 4 instance, held to 80 registers so that three CTAs fit an SM
 // (its shared memory allows three).
-template <int GEOM, int STORE>
+template <int GEOM, int STORE, bool IL>
 __global__ void __launch_bounds__(BP_THREADS, 3) bp_kernel_s4(const BpArgs p, const int AB)
 {
-    bp_body<GEOM, STORE, 4>(p, AB);
+    bp_body<GEOM, STORE, 4, IL>(p, AB);
+}
+
+// Window rows [nslices][nangles][Wg] (f32) -> [ceil(nslices/4)][nangles][Wg][4],
+// slices beyond nslices zero; one CTA per (group, angle) row.
+__global__ void interleave4_kernel(const float *__restrict__ rows, float4 *__restrict__ out, int nslices, int A,
+                                   int Wg)
+{
+    const int r = blockIdx.x, g = r / A, a = r - g * A;
+    const float *src[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) src[q] = 4 * g + q < nslices ? rows + ((size_t)(4 * g + q) * A + a) * Wg : nullptr;
+    float4 *dst = out + (size_t)r * Wg;
+    for (int e = threadIdx.x; e < Wg; e += blockDim.x)
+        dst[e] = make_float4(src[0] ? __ldcs(src[0] + e) : 0.f, src[1] ? __ldcs(src[1] + e) : 0.f,
+                             src[2] ? __ldcs(src[2] + e) : 0.f, src[3] ? __ldcs(src[3] + e) : 0.f);
 }
 
 // ------------------------------------------------------------------------
@@ -498,7 +535,7 @@ static size_t bp_smem(int S, int AB, int W, int esize)
     return kWinOffset + 2 * (size_t)AB * S * W * esize;
 }
 
-template <int GEOM, int STORE, int S>
+template <int GEOM, int STORE, int S, bool IL = false>
 static void launch_bp_s(const BpArgs &a, int AB, cudaStream_t st)
 {
     const int esize = (STORE == STORE_PAIR_F32) ? 8 : 4;
@@ -508,7 +545,7 @@ static void launch_bp_s(const BpArgs &a, int AB, cudaStream_t st)
     int dev = 0;
     cudaGetDevice(&dev);
     void (*kern)(const BpArgs, const int);
-    if constexpr (S == 4) kern = bp_kernel_s4<GEOM, STORE>;
+    if constexpr (S == 4) kern = bp_kernel_s4<GEOM, STORE, IL>;
     else kern = bp_kernel<GEOM, STORE, S>;
     if (configured != dev) {
         RAFT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBpSmemMax));
@@ -526,7 +563,15 @@ static void launch_bp_cfg(const BpArgs &a, BpTune t, cudaStream_t st)
     switch (t.S) {
     case 1: launch_bp_s<GEOM, STORE, 1>(a, t.AB, st); break;
     case 2: launch_bp_s<GEOM, STORE, 2>(a, t.AB, st); break;
-    default: launch_bp_s<GEOM, STORE, 4>(a, t.AB, st); break;
+    default:
+        if constexpr (GEOM != GEOM_FBP_LIN && STORE == STORE_F32) {
+            if (a.il) {
+                launch_bp_s<GEOM, STORE, 4, true>(a, t.AB, st);
+                break;
+            }
+        }
+        launch_bp_s<GEOM, STORE, 4>(a, t.AB, st);
+        break;
     }
 }
 
@@ -572,12 +617,16 @@ static bool forced_tune(BpTune &t)
 
 // Pick (S, AB) for this configuration: the cached choice, else time every
 // candidate that fits shared memory on up to 8 slices of the real data
-// (store launches only -- they are idempotent), else a default.
-static BpTune choose_tune(const BpArgs &a, int geometry, int store, cudaStream_t st)
+// (store launches only -- they are idempotent), else a default.  With
+// a_il (the same launch on slice-interleaved rows) the S = 4 candidates are
+// timed on it; prep_il makes those rows and is called at most once.
+template <class Prep>
+static BpTune choose_tune(const BpArgs &a, const BpArgs *a_il, Prep &&prep_il, int geometry, int store,
+                          cudaStream_t st)
 {
     int dev = 0;
     cudaGetDevice(&dev);
-    const TuneKey key(dev, geometry, store, a.No, a.W, a.nangles);
+    const TuneKey key(dev, geometry, store + (a_il ? 16 : 0), a.No, a.W, a.nangles);
     const int esize = store_bytes(store);
     BpTune forced;
     if (forced_tune(forced) && bp_smem(forced.S, forced.AB, a.W, esize) <= kBpSmemMax) return forced;
@@ -592,14 +641,20 @@ static BpTune choose_tune(const BpArgs &a, int geometry, int store, cudaStream_t
     cudaStreamIsCapturing(st, &cap);
     const bool can_tune = tuning_enabled() && a.update == 0 && cap == cudaStreamCaptureStatusNone;
     if (can_tune) {
-        BpArgs t = a;
-        t.nslices = std::min(a.nslices, 8);
+        BpArgs t0 = a;
+        t0.nslices = std::min(a.nslices, 8);
         cudaEvent_t e0, e1;
         RAFT_CUDA(cudaEventCreate(&e0));
         RAFT_CUDA(cudaEventCreate(&e1));
         float best_ms = 1e30f;
         for (const BpTune &c : kTuneCandidates) {
             if (bp_smem(c.S, c.AB, a.W, esize) > kBpSmemMax) continue;
+            BpArgs t = t0;
+            if (c.S == 4 && a_il) {
+                prep_il();
+                t = *a_il;
+                t.nslices = t0.nslices;
+            }
             launch_bp_any(t, geometry, store, c, st);   // warm
             RAFT_CUDA(cudaEventRecord(e0, st));
             launch_bp_any(t, geometry, store, c, st);
@@ -668,7 +723,13 @@ static BpArgs to_args(const BpLaunch &bl)
     a.snd = bl.snd;
     a.err = bl.err;
     a.update = bl.den ? 1 : 0;
+    a.il = 0;
     return a;
+}
+
+size_t bp_il_bytes(int nslices, int nangles, int Wg)
+{
+    return (size_t)((nslices + 3) / 4) * nangles * Wg * 16;
 }
 
 void launch_backproject(const BpLaunch &bl, cudaStream_t st)
@@ -676,8 +737,28 @@ void launch_backproject(const BpLaunch &bl, cudaStream_t st)
     if (bl.nslices <= 0 || bl.nangles <= 0) return;
     const BpArgs a = to_args(bl);
     const int store = bl.geometry == GEOM_FBP_LIN ? bl.store : STORE_F32;
-    const BpTune t = choose_tune(a, bl.geometry, store, st);
-    launch_bp_any(a, bl.geometry, store, t, st);
+    // four slices per CTA on slice-interleaved rows, when the caller provides the workspace
+    const bool il_ok = bl.il_ws && bl.geometry != GEOM_FBP_LIN;
+    BpArgs a_il = a;
+    a_il.filt = reinterpret_cast<const unsigned char *>(bl.il_ws);
+    a_il.il = 1;
+    bool il_done = false;
+    auto prep_il = [&]() {
+        if (il_done) return;
+        count_launch();
+        interleave4_kernel<<<(unsigned)(((bl.nslices + 3) / 4) * bl.nangles), 256, 0, st>>>(
+            reinterpret_cast<const float *>(bl.filt), reinterpret_cast<float4 *>(bl.il_ws), bl.nslices, bl.nangles,
+            bl.win.Wg);
+        RAFT_CUDA(cudaGetLastError());
+        il_done = true;
+    };
+    const BpTune t = choose_tune(a, il_ok ? &a_il : nullptr, prep_il, bl.geometry, store, st);
+    if (il_ok && t.S == 4) {
+        prep_il();
+        launch_bp_any(a_il, bl.geometry, store, t, st);
+    } else {
+        launch_bp_any(a, bl.geometry, store, t, st);
+    }
 }
 
 // ------------------------------------------------------------------------

@@ -289,7 +289,7 @@ size_t fbp_rows_bytes(const FbpPrepared &fp, int nslices)
 }
 
 void fbp_chunk(DeviceState &ds, const FbpPrepared &fp, const FbpTables &tb, const float *d_sino, float *d_img,
-               int nslices, void *d_rows, cudaStream_t st)
+               int nslices, void *d_rows, cudaStream_t st, void *d_il)
 {
     (void)ds;
     if (nslices <= 0) return;
@@ -318,7 +318,13 @@ void fbp_chunk(DeviceState &ds, const FbpPrepared &fp, const FbpTables &tb, cons
     bl.csd = tb.csd;
     bl.snd = tb.snd;
     bl.err = tb.err;
+    bl.il_ws = fp.cfg.geometry == GEOM_FBP_REF ? d_il : nullptr;
     launch_backproject(bl, st);
+}
+
+size_t fbp_il_bytes(const FbpPrepared &fp, int nslices)
+{
+    return fp.cfg.geometry == GEOM_FBP_REF ? bp_il_bytes(nslices, fp.cfg.nangles, fp.win.Wg) : 0;
 }
 
 static void check_device_flag(const int *d_err, const char *what)
@@ -342,8 +348,9 @@ void fbp_host_slab(const FbpConfig &cfg, int device, float *obj, const float *to
     const size_t out_ps = (size_t)fp.No * fp.No * sizeof(float);
     const int chunk = auto_chunk(nslices, in_ps, cfg.blocksize);
     void *rows = ds.rows.get(fbp_rows_bytes(fp, chunk));
+    void *il = fbp_il_bytes(fp, chunk) ? ds.il.get(fbp_il_bytes(fp, chunk)) : nullptr;
     run_pipeline(ds, nslices, chunk, in_ps, out_ps, tomo, obj, [&](void *din, void *dout, int ns, cudaStream_t st) {
-        fbp_chunk(ds, fp, tb, (const float *)din, (float *)dout, ns, rows, st);
+        fbp_chunk(ds, fp, tb, (const float *)din, (float *)dout, ns, rows, st, il);
     });
     check_device_flag(tb.err, "FBP");
 }

@@ -31,7 +31,7 @@ struct DeviceState {
     std::mutex mtx;
     cudaStream_t s_comp = nullptr, s_h2d = nullptr, s_d2h = nullptr;
     cudaStream_t s_hi = nullptr, s_lo = nullptr;   // ragged batches: FBP (high) and EM (low) priority
-    DevBuf sino[2], img[2], rows, den, flat, data, angles, tabs, metrics, err, imgT;
+    DevBuf sino[2], img[2], rows, den, flat, data, angles, tabs, metrics, err, imgT, il;
     PinBuf pin_in[2], pin_out[2];
     cudaEvent_t ev_h2d[2] = {}, ev_comp[2] = {}, ev_d2h[2] = {};
     cudaEvent_t ev_join = nullptr;
@@ -77,9 +77,12 @@ struct FbpTables {
     int *err = nullptr;
 };
 FbpTables fbp_tables(DeviceState &ds, const FbpPrepared &fp, const float *h_angles, cudaStream_t st);
+// d_il (optional, fbp_il_bytes): workspace for the slice-interleaved rows the
+// nearest backprojector reads with four slices per CTA; null keeps the planar rows.
 void fbp_chunk(DeviceState &ds, const FbpPrepared &fp, const FbpTables &tb, const float *d_sino, float *d_img,
-               int nslices, void *d_rows, cudaStream_t st);
+               int nslices, void *d_rows, cudaStream_t st, void *d_il = nullptr);
 size_t fbp_rows_bytes(const FbpPrepared &fp, int nslices);
+size_t fbp_il_bytes(const FbpPrepared &fp, int nslices);
 
 // Host-buffer FBP of one slab on one device (the body of getFBPMultiGPU).
 void fbp_host_slab(const FbpConfig &cfg, int device, float *obj, const float *tomo, const float *angles,
