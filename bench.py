@@ -37,8 +37,9 @@ N_RAYS, N_ANGLES, N_SLICES = 2048, 1800, 512
 OFFSET, PAD, FILTER_ID = 3.5, 2, 5          # Hann
 I0 = 1.0e4
 # DRAM bytes (read + write) of one 32-slice nearest backprojector launch at
-# 2048^2 x 1800 angles, measured with ncu (1.18x the algorithmic bytes).
-BP_TRAFFIC_PER_LAUNCH = 896_157_440 + 520_072_704
+# 2048^2 x 1800 angles (four slices per CTA on slice-interleaved rows),
+# measured with ncu (1.08x the algorithmic bytes).
+BP_TRAFFIC_PER_LAUNCH = 783_763_456 + 518_802_944
 WORKLOAD = ("batched FBP: 512 slices x 2048^2, 1800 angles over [0,pi), 2048 bins, "
             "axis offset +3.5 px, Hann, padding 2")
 
@@ -727,9 +728,9 @@ def run_ours(args):
                          "unit": "GB/s", "frac": alg_bytes / bp_avg_s / 1e9 / hbm_peak,
                          "traffic": BP_TRAFFIC_PER_LAUNCH if chunk == 32 else None,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 32-slice "
-                                           "launch (S4, AB16), --set full capture",
+                                           "launch (S4 interleaved, AB16), --set full capture",
                          "algorithmic_bytes_per_launch": alg_bytes,
-                         "kernel": "bp_kernel<nearest,f32>", "peak_kind": peak_kind,
+                         "kernel": "bp_kernel_s4<nearest,f32,interleaved>", "peak_kind": peak_kind,
                          "note": "the backprojector is bounded by its shared-memory gather, see gather_roofline"},
             "gather_roofline": {"achieved_gups": gups_bp, "peak_gups": peak_gups, "frac": gups_bp / peak_gups,
                                 "bytes_per_update": 4, "fp32_ops_per_update": 4, "sm_mhz": sm_mhz},

@@ -636,6 +636,7 @@ void em_chunk(DeviceState &ds, const EmPrepared &ep, int kind, const float *d_da
     bl.cs = cs;
     bl.sn = sn;
     bl.err = err;
+    bl.il_ws = ds.il.get(bp_il_bytes(nslices, A, win.Wg));
 
     // sensitivity image: BP of the counts (tEM, em_rt.cu:178) or of ones (eEM, :343)
     launch_to_window(kind == 0 ? d_data : nullptr, rows, wt, nslices * A, A, n, win.wlo, win.Wg, st);
