@@ -39,6 +39,7 @@
 #include "profile.hpp"
 #include "fft.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <memory>
@@ -154,7 +155,7 @@ __global__ void __launch_bounds__(512) bst_regrid_kernel(const BstArgs p)
         sm_bst[X] = make_float2(v.x * sgn, -v.y * sgn);   // conjugated: see bst_cols_kernel
     }
     __syncthreads();
-    const float2 *r = fft_forward(sm_bst, sm_bst + S, S, p.rlS, p.twS);
+    const float2 *r = fft_forward(sm_bst, sm_bst + fft_span(S), S, p.rlS, p.twS);
     float2 *trow = p.T + ((size_t)slice * S + Y) * p.N;
     for (int i = threadIdx.x; i < p.N; i += blockDim.x) trow[i] = r[p.off + i];
 }
@@ -168,7 +169,7 @@ __global__ void __launch_bounds__(512) bst_cols_kernel(const BstArgs p)
     const float2 *tcol = p.T + (size_t)slice * p.S * p.N + i;
     for (int Y = threadIdx.x; Y < p.S; Y += blockDim.x) sm_bst[Y] = tcol[(size_t)Y * p.N];
     __syncthreads();
-    const float2 *r = fft_forward(sm_bst, sm_bst + p.S, p.S, p.rlS, p.twS);
+    const float2 *r = fft_forward(sm_bst, sm_bst + fft_span(p.S), p.S, p.rlS, p.twS);
     float *o = p.obj + (size_t)slice * p.N * p.N + i;
     for (int j = threadIdx.x; j < p.N; j += blockDim.x) o[(size_t)j * p.N] = r[p.off + j].x / p.scale;
 }
@@ -227,11 +228,15 @@ static bool fft_len_ok(int n)
     return n >= 1 && factorize(n, r, nr);
 }
 
+// Shared-memory buffer length of the row kernel: the padded row and both
+// transforms' ping-pong buffers (fft_span is not monotonic at its padding limit).
+static int bst_row_span(const BstCore &c) { return std::max({c.Np, fft_span(c.Np), fft_span(c.L)}); }
+
 bool bst_core_ok(const BstCore &c)
 {
     return c.N >= 2 && c.A >= 1 && c.L >= 2 && c.S >= 2 && fft_len_ok(c.L) && fft_len_ok(c.S) &&
-           (!c.filtered || fft_len_ok(c.Np)) && 3 * (size_t)c.M * sizeof(float2) <= kBstSmemMax &&
-           2 * (size_t)c.S * sizeof(float2) <= kBstSmemMax;
+           (!c.filtered || fft_len_ok(c.Np)) && 3 * (size_t)bst_row_span(c) * sizeof(float2) <= kBstSmemMax &&
+           2 * (size_t)fft_span(c.S) * sizeof(float2) <= kBstSmemMax;
 }
 
 bool bst_plan_shape(BstPlanShape &s, int N, int A, int pad)
@@ -296,11 +301,11 @@ void bst_run(int device, const BstCore &c, const float *d_tomo, float *d_obj, in
     a.Lh = c.Lh;
     a.S = c.S;
     a.off = c.off;
-    a.M = c.M;
+    a.M = bst_row_span(c);
     a.w_half = c.w_half;
     a.scale = c.scale;
     const int threads = fft_threads(std::max(c.M, c.S));
-    const size_t sm3 = 3 * (size_t)c.M * sizeof(float2), sm2 = 2 * (size_t)c.S * sizeof(float2);
+    const size_t sm3 = 3 * (size_t)a.M * sizeof(float2), sm2 = 2 * (size_t)fft_span(c.S) * sizeof(float2);
     static thread_local int configured = -1;
     int dev = 0;
     cudaGetDevice(&dev);

@@ -211,12 +211,16 @@ static void run_pipeline(DeviceState &ds, int nslices, int chunk, size_t in_ps, 
     RAFT_CUDA(cudaStreamSynchronize(ds.s_d2h));
 }
 
+// Slices per pipeline chunk: about 512 MB of input, at most 32, a multiple of
+// four where possible (the backprojector's CTAs take four slices each).
 static int auto_chunk(int nslices, size_t bytes_per_slice, int blocksize)
 {
     if (blocksize > 0) return std::max(1, std::min(blocksize, nslices));
-    const size_t target = 256u << 20;
+    const size_t target = (size_t)512 << 20;
     int c = (int)std::max<size_t>(1, target / std::max<size_t>(1, bytes_per_slice));
-    return std::max(1, std::min({c, 32, nslices}));
+    c = std::min(c, 32);
+    if (c >= 4) c -= c % 4;
+    return std::max(1, std::min(c, nslices));
 }
 
 // ------------------------------------------------------------------ FBP --

@@ -2,10 +2,15 @@
 // filter, BST and rotation-axis kernels.
 //
 // A CTA transforms one length-n sequence held in shared memory, ping-ponging
-// between two buffers; radices 2, 3, 4, 5, 7, 8 (lengths whose other prime
-// factors are rejected on the host).  Twiddles exp(-2 pi i k / n) come from a
-// table built in FP64 on the host.  Only the forward transform exists: an
-// inverse is the forward transform of the conjugate, conjugated.
+// between two buffers of fft_span(n) elements each; radices 2, 3, 4, 5, 7, 8
+// (lengths whose other prime factors are rejected on the host).  The input is
+// read from, and the result left in, plain order; intermediate passes store
+// one pad element after every 16 (n <= 12288) so that the strided writes of
+// the early passes spread over the shared-memory banks.  Twiddles: one value
+// exp(-2 pi i k / n) per butterfly from a table built in FP64 on the host, its
+// powers by repeated complex products.  Only the
+// forward transform exists: an inverse is the forward transform of the
+// conjugate, conjugated.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -41,6 +46,13 @@ static inline std::vector<float2> fft_twiddles(int n)
     }
     return tw;
 }
+
+// Intermediate passes are stored padded up to this length (above it the two
+// padded buffers would not fit beside each other in shared memory).
+constexpr int kFftPadMax = 12288;
+__host__ __device__ constexpr bool fft_padded(int n) { return n <= kFftPadMax; }
+// Elements one ping-pong buffer of an n-point transform occupies.
+__host__ __device__ constexpr int fft_span(int n) { return fft_padded(n) ? n + n / 16 + 1 : n; }
 
 // Threads per CTA for one length-n transform: about 8 butterflies of the
 // smallest radix per thread, 128..512 threads.
@@ -159,27 +171,51 @@ template <> struct Dft<3> { static __device__ __forceinline__ void run(float2 *v
 template <> struct Dft<5> { static __device__ __forceinline__ void run(float2 *v) { DftOdd<5>::run(v); } };
 template <> struct Dft<7> { static __device__ __forceinline__ void run(float2 *v) { DftOdd<7>::run(v); } };
 
-// One Stockham pass of radix R from src to dst (both Np complex values in
-// shared memory).  Only one butterfly's R values are live per thread.
+__device__ __forceinline__ int fft_pad(int i) { return i + (i >> 4); }
+
+// One Stockham pass of radix R from src to dst (Np complex values in shared
+// memory; pin / pout: src / dst stored padded).  Butterfly j = q Ns + k; the
+// thread's (q, k) advance by blockDim.x without a division per butterfly.
 template <int R>
 __device__ __noinline__ void fft_pass(const float2 *__restrict__ src, float2 *__restrict__ dst, int Np,
-                                      int Ns, const float2 *__restrict__ tw)
+                                      int Ns, const float2 *__restrict__ tw, int pin, int pout)
 {
     const int nb = Np / R;
     const int twstep = Np / (Ns * R);
-    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
-        const int k = j % Ns;
+    const int T = blockDim.x;
+    int q = threadIdx.x / Ns, k = threadIdx.x - q * Ns;
+    const int dq = T / Ns, dk = T - dq * Ns;
+    for (int j = threadIdx.x; j < nb; j += T) {
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; r++) {
-            float2 x = src[j + r * nb];
-            if (r > 0 && k > 0) x = cmul(x, __ldg(&tw[r * k * twstep]));
-            v[r] = x;
+            const int si = j + r * nb;
+            v[r] = src[pin ? fft_pad(si) : si];
+        }
+        if (k > 0) {
+            // w^r, r < R, from w = exp(-2 pi i k twstep / Np) by repeated products
+            // (two complex registers live; relative error of w^7 a few 1e-7)
+            const float2 w1 = __ldg(&tw[k * twstep]);
+            float2 w = w1;
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                v[r] = cmul(v[r], w);
+                if (r + 1 < R) w = cmul(w, w1);
+            }
         }
         Dft<R>::run(v);
-        const int base = (j / Ns) * Ns * R + k;
+        const int base = q * Ns * R + k;
 #pragma unroll
-        for (int r = 0; r < R; r++) dst[base + r * Ns] = v[r];
+        for (int r = 0; r < R; r++) {
+            const int di = base + r * Ns;
+            dst[pout ? fft_pad(di) : di] = v[r];
+        }
+        q += dq;
+        k += dk;
+        if (k >= Ns) {
+            k -= Ns;
+            q++;
+        }
     }
     __syncthreads();
 }
@@ -189,19 +225,22 @@ struct RadixList {
     int r[24];
 };
 
-// Forward FFT of a[0..Np); the result ends in a or b, which is returned.
+// Forward FFT of a[0..Np) (plain order); a and b each hold fft_span(Np)
+// elements; the result ends in a or b (plain order), which is returned.
 __device__ __forceinline__ float2 *fft_forward(float2 *a, float2 *b, int Np, const RadixList &rl,
                                                const float2 *tw)
 {
     int Ns = 1;
+    const int pad = fft_padded(Np);
     for (int p = 0; p < rl.n; p++) {
+        const int pin = pad && p > 0, pout = pad && p + 1 < rl.n;
         switch (rl.r[p]) {
-        case 2: fft_pass<2>(a, b, Np, Ns, tw); break;
-        case 3: fft_pass<3>(a, b, Np, Ns, tw); break;
-        case 4: fft_pass<4>(a, b, Np, Ns, tw); break;
-        case 5: fft_pass<5>(a, b, Np, Ns, tw); break;
-        case 7: fft_pass<7>(a, b, Np, Ns, tw); break;
-        default: fft_pass<8>(a, b, Np, Ns, tw); break;
+        case 2: fft_pass<2>(a, b, Np, Ns, tw, pin, pout); break;
+        case 3: fft_pass<3>(a, b, Np, Ns, tw, pin, pout); break;
+        case 4: fft_pass<4>(a, b, Np, Ns, tw, pin, pout); break;
+        case 5: fft_pass<5>(a, b, Np, Ns, tw, pin, pout); break;
+        case 7: fft_pass<7>(a, b, Np, Ns, tw, pin, pout); break;
+        default: fft_pass<8>(a, b, Np, Ns, tw, pin, pout); break;
         }
         Ns *= rl.r[p];
         float2 *t = a; a = b; b = t;

@@ -129,7 +129,7 @@ bool build_filter_plan(FilterPlan &plan, int geometry, int ftype, int N, int pad
     plan.skip = (ftype == FILTER_NONE);
     if (plan.skip) return true;
 
-    const size_t smem = 2 * (size_t)Np * sizeof(float2);   // ping-pong buffers
+    const size_t smem = 2 * (size_t)fft_span(Np) * sizeof(float2);   // ping-pong buffers
     plan.fft = factorize(Np, plan.radix, plan.nradix) && smem <= kFilterSmemMax;
     plan.threads = fft_threads(Np);
     std::vector<double> hre(Np), him(Np);
@@ -208,14 +208,15 @@ __device__ __forceinline__ void pack_row(const float2 *z, int row, int part, con
 }
 
 // ================================================== kernel: FFT filter
-__global__ void __launch_bounds__(512)
+// two CTAs per SM (registers capped at 64: two 512-thread CTAs, or 384 + 384)
+__global__ void __launch_bounds__(512, 2)
 filter_fft_kernel(const float *__restrict__ sino, int N, int Np, int off, int nrows,
                   const float2 *__restrict__ H, const float2 *__restrict__ tw, RadixList rl,
                   PackArgs pk, int skip, float *lowpass_out)
 {
     extern __shared__ float2 smem_fft[];
     float2 *z = smem_fft;
-    float2 *zb = smem_fft + Np;
+    float2 *zb = smem_fft + fft_span(Np);
     const int r0 = 2 * blockIdx.x, r1 = r0 + 1;
     const bool has1 = r1 < nrows;
     const float *s0 = sino + (size_t)r0 * N;
@@ -236,7 +237,7 @@ filter_fft_kernel(const float *__restrict__ sino, int N, int Np, int off, int nr
             z[k] = make_float2(g.x, -g.y);
         }
         __syncthreads();
-        zb = (z == smem_fft) ? smem_fft + Np : smem_fft;
+        zb = (z == smem_fft) ? smem_fft + fft_span(Np) : smem_fft;
         z = fft_forward(z, zb, Np, rl, tw);
     } else {
         // no transform: match the conjugation convention of pack_row
@@ -311,13 +312,14 @@ void launch_filter(const FilterPlan &plan, const FilterLaunch &fl, cudaStream_t 
         rl.n = plan.skip ? 0 : plan.nradix;
         for (int i = 0; i < rl.n; i++) rl.r[i] = plan.radix[i];
         const int T = plan.skip ? 256 : plan.threads;
-        const size_t smem = 2 * (size_t)plan.Np * sizeof(float2);
+        const size_t smem = 2 * (size_t)fft_span(plan.Np) * sizeof(float2);
         static thread_local int configured_dev = -1;
         int dev = 0;
         cudaGetDevice(&dev);
         if (configured_dev != dev) {
             RAFT_CUDA(cudaFuncSetAttribute(filter_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)kFilterSmemMax));
+            RAFT_CUDA(cudaFuncSetAttribute(filter_fft_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
             configured_dev = dev;
         }
         ProfScope ps(PROF_FILTER, st);
@@ -352,7 +354,7 @@ bool filter_plan_shape(FilterPlan &plan, int ftype, int N, int pad)
     plan.skip = (ftype == FILTER_NONE);
     plan.threads = fft_threads(plan.Np);
     plan.fft = factorize(plan.Np, plan.radix, plan.nradix) &&
-               2 * (size_t)plan.Np * sizeof(float2) <= kFilterSmemMax;
+               2 * (size_t)fft_span(plan.Np) * sizeof(float2) <= kFilterSmemMax;
     return plan.skip || plan.fft;
 }
 

@@ -68,7 +68,7 @@ fft_strided_kernel(float2 *data, int n, size_t seq_stride, size_t elem_stride, R
         sm_rot[k] = inverse ? make_float2(v.x, -v.y) : v;
     }
     __syncthreads();
-    const float2 *r = fft_forward(sm_rot, sm_rot + n, n, rl, tw);
+    const float2 *r = fft_forward(sm_rot, sm_rot + fft_span(n), n, rl, tw);
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const float2 v = r[k];
         base[(size_t)k * elem_stride] = inverse ? make_float2(v.x, -v.y) : v;
@@ -163,7 +163,7 @@ __global__ void peak_subpixel_kernel(const float2 *f, int sizex, int sizey, unsi
 void fft2(int device, float2 *data, int sizex, int sizey, int inverse, cudaStream_t st)
 {
     const FftTable &tx = fft_table(device, sizex), &ty = fft_table(device, sizey);
-    const size_t smx = 2 * (size_t)sizex * sizeof(float2), smy = 2 * (size_t)sizey * sizeof(float2);
+    const size_t smx = 2 * (size_t)fft_span(sizex) * sizeof(float2), smy = 2 * (size_t)fft_span(sizey) * sizeof(float2);
     RAFT_CUDA(cudaFuncSetAttribute(fft_strided_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)std::max(smx, smy)));
     count_launch();
@@ -181,7 +181,7 @@ bool centersino_shape_ok(int sizex, int sizey)
     int r[24], n = 0;
     const size_t lim = 227 * 1024;
     return sizex >= 1 && sizey >= 1 && factorize(sizex, r, n) && factorize(sizey, r, n) &&
-           2 * (size_t)sizex * sizeof(float2) <= lim && 2 * (size_t)sizey * sizeof(float2) <= lim &&
+           2 * (size_t)fft_span(sizex) * sizeof(float2) <= lim && 2 * (size_t)fft_span(sizey) * sizeof(float2) <= lim &&
            (unsigned long long)sizex * sizey < 0xffffffffull;
 }
 

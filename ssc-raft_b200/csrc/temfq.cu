@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(512) fst_rows_kernel(const FstArgs p)
         sm_fst[c] = make_float2(v, 0.f);
     }
     __syncthreads();
-    const float2 *r = fft_forward(sm_fst, sm_fst + L, L, p.rl, p.tw);
+    const float2 *r = fft_forward(sm_fst, sm_fst + fft_span(L), L, p.rl, p.tw);
     float2 *dst = p.rows + ((size_t)b * N + q) * L;
     for (int c = threadIdx.x; c < L; c += blockDim.x) dst[c] = r[c];
 }
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(512) fst_cols_kernel(const FstArgs p)
     const float2 *col = p.rows + (size_t)b * N * L + c;
     for (int q = threadIdx.x; q < N; q += blockDim.x) sm_fst[q < h ? q : q + L - N] = col[(size_t)q * L];
     __syncthreads();
-    const float2 *r = fft_forward(sm_fst, sm_fst + L, L, p.rl, p.tw);
+    const float2 *r = fft_forward(sm_fst, sm_fst + fft_span(L), L, p.rl, p.tw);
     float2 *dst = p.spec + ((size_t)b * L + c) * L;
     for (int y = threadIdx.x; y < L; y += blockDim.x) dst[y] = r[y];
 }
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(512) fst_sino_kernel(const FstArgs p)
         sm_fst[qq] = make_float2(v.x, -v.y);               // conjugate: inverse = conj(forward(conj))
     }
     __syncthreads();
-    const float2 *H = fft_forward(sm_fst, sm_fst + L, L, p.rl, p.tw);
+    const float2 *H = fft_forward(sm_fst, sm_fst + fft_span(L), L, p.rl, p.tw);
     const float *fl = p.flat + (size_t)b * N;
     float *out = p.model + ((size_t)b * p.A + a) * N;
     for (int i = threadIdx.x; i < N; i += blockDim.x) {
@@ -177,7 +177,7 @@ bool temfq_shape_ok(int N, int A, int zpad)
     if ((N * (zpad + 1)) % 2) return false;
     BstCore c = temfq_bst_core(N, A, zpad);
     int r[24], n = 0;
-    return factorize(L, r, n) && 2 * (size_t)L * sizeof(float2) <= 227 * 1024 && bst_core_ok(c);
+    return factorize(L, r, n) && 2 * (size_t)fft_span(L) * sizeof(float2) <= 227 * 1024 && bst_core_ok(c);
 }
 
 BstCore temfq_bst_core(int N, int A, int zpad)
@@ -261,7 +261,7 @@ void temfq_run(int device, const TemfqConfig &cfg, float *d_obj, const float *d_
     f.interp = cfg.interpolation;
     // em_frequency.cu:166: dx / L, or 1 / L when dx <= 0 (the latter in double)
     f.scale = cfg.dx > 0.f ? cfg.dx / (float)L : (float)(1.0 / (float)L);
-    const size_t sm = 2 * (size_t)L * sizeof(float2);
+    const size_t sm = 2 * (size_t)fft_span(L) * sizeof(float2);
     const int threads = fft_threads(L);
     RAFT_CUDA(cudaFuncSetAttribute(fst_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     RAFT_CUDA(cudaFuncSetAttribute(fst_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
