@@ -62,7 +62,7 @@ struct BpArgs {
     const double *csd, *snd;     // FP64 tables
     int *err;
     int update;                  // 0: store, 1: img = img * acc / den
-    int il;                      // 1: filt holds groups of 4 slices interleaved, [group][angle][Wg][4]
+    int il;                      // 1: filt holds groups of 4 slices interleaved, [group][angle][Wg][4 elements]
 };
 
 constexpr uint32_t kWaitLimit = 1u << 24;
@@ -150,11 +150,11 @@ __device__ __forceinline__ float lerp_fetch(const unsigned char *w, int k, float
 // S slices share one CTA: the per-pixel position, rounding and window index
 // are computed once per (pixel, angle) and reused for every slice, whose
 // windows sit side by side in shared memory ([angle][slice][W]).  With IL
-// (S = 4, 4-byte elements) the rows arrive interleaved by slice
-// ([group][angle][Wg][4], see interleave4_kernel), the staged windows are
-// [angle][W][4] and one 16-byte load fetches the sample of all four slices:
-// one bulk copy per angle instead of four, one shared-memory instruction per
-// (pixel, angle) instead of four.  AB (angles per pipeline stage) is a launch
+// (S = 4) the rows arrive interleaved by slice ([group][angle][Wg][4
+// elements], see interleave4_kernel), the staged windows are [angle][W][4]
+// and one 16-byte load (two for f32 pairs) fetches the sample of all four
+// slices: one bulk copy per angle instead of four, one or two shared-memory
+// instructions per (pixel, angle) instead of four.  AB (angles per pipeline stage) is a launch
 // parameter; S and AB are chosen by the autotuner below.
 // ------------------------------------------------------------------------
 // One 64 x 32 tile of S slices.  `gstage` counts the pipeline stages this
@@ -164,7 +164,7 @@ template <int GEOM, int STORE, int S, bool IL = false>
 __device__ __forceinline__ bool bp_tile(const BpArgs &p, const int AB, const int x0, const int y0,
                                         const int slice0, unsigned char *smem, uint32_t &gstage)
 {
-    static_assert(!IL || (S == 4 && STORE != STORE_PAIR_F32 && GEOM != GEOM_FBP_LIN), "interleaved: 4 x f32");
+    static_assert(!IL || S == 4, "interleaved rows: four slices per CTA");
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     AngleParam *prm = reinterpret_cast<AngleParam *>(smem + 128);
     unsigned char *win = smem + kWinOffset;
@@ -187,7 +187,7 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &p, const int AB, const int
 #pragma unroll
     for (int j = 0; j < 2; j++) lj[j] = wy * 8 + ly + 4 * j;
 
-    const unsigned char *rows = IL ? p.filt + (size_t)(slice0 / 4) * A * p.Wg * 16
+    const unsigned char *rows = IL ? p.filt + (size_t)(slice0 / 4) * A * p.Wg * (4 * esize)
                                    : p.filt + (size_t)slice0 * A * p.Wg * esize;
     const size_t slice_stride = (size_t)A * p.Wg * esize;
 
@@ -209,10 +209,11 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &p, const int AB, const int
         unsigned char *dst = win + (size_t)b * stage_bytes;
         if constexpr (IL) {
             // one copy of the four interleaved windows per angle
-            for (int al = lane; al < na; al += 32)
-                bulk_g2s(dst + (size_t)al * S * wbytes,
-                         rows + ((size_t)(a0 + al) * p.Wg + prm[b * 32 + al].d - p.wlo) * 16, (uint32_t)(S * wbytes),
-                         &bars[b]);
+            for (int al = lane; al < na; al += 32) {
+                const int base = prm[b * 32 + al].d - (GEOM == GEOM_FBP_LIN ? 0 : p.wlo);
+                bulk_g2s(dst + (size_t)al * S * wbytes, rows + ((size_t)(a0 + al) * p.Wg + base) * (4 * esize),
+                         (uint32_t)(S * wbytes), &bars[b]);
+            }
         } else {
             for (int c = lane; c < na * nsl; c += 32) {
                 const int al = c / nsl, sl = c - al * nsl;
@@ -278,10 +279,28 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &p, const int AB, const int
                         const float m = __fadd_rn(v, MAGIC);
                         const unsigned k = min((unsigned)(__float_as_int(m) - 0x4B400000), (unsigned)(W - 1));
                         const float f = __fsub_rn(v, __fsub_rn(m, MAGIC));
-                        const unsigned char *wk = w + (size_t)k * esize;
+                        if constexpr (IL && STORE == STORE_PAIR_F32) {
+                            // bin k: (mid, dif) of slices 0..3 in 32 bytes
+                            const float4 u0 = reinterpret_cast<const float4 *>(w)[2 * k];
+                            const float4 u1 = reinterpret_cast<const float4 *>(w)[2 * k + 1];
+                            acc[0][j][i] += fmaf(f, u0.y, u0.x);
+                            acc[1][j][i] += fmaf(f, u0.w, u0.z);
+                            acc[2][j][i] += fmaf(f, u1.y, u1.x);
+                            acc[3][j][i] += fmaf(f, u1.w, u1.z);
+                        } else if constexpr (IL) {
+                            // bin k: bf16 (mid, dif) pairs of slices 0..3 in 16 bytes
+                            const uint4 u = reinterpret_cast<const uint4 *>(w)[k];
+                            const uint32_t bits[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
-                        for (int q = 0; q < S; q++)
-                            acc[q][j][i] += lerp_fetch<STORE>(wk + q * wbytes, 0, f);
+                            for (int q = 0; q < 4; q++)
+                                acc[q][j][i] += fmaf(f, __uint_as_float(bits[q] & 0xffff0000u),
+                                                     __uint_as_float(bits[q] << 16));
+                        } else {
+                            const unsigned char *wk = w + (size_t)k * esize;
+#pragma unroll
+                            for (int q = 0; q < S; q++)
+                                acc[q][j][i] += lerp_fetch<STORE>(wk + q * wbytes, 0, f);
+                        }
                     }
                 }
             } else {
@@ -372,19 +391,23 @@ __global__ void __launch_bounds__(BP_THREADS, 3) bp_kernel_s4(const BpArgs p, co
     bp_body<GEOM, STORE, 4, IL>(p, AB);
 }
 
-// Window rows [nslices][nangles][Wg] (f32) -> [ceil(nslices/4)][nangles][Wg][4],
-// slices beyond nslices zero; one CTA per (group, angle) row.
-__global__ void interleave4_kernel(const float *__restrict__ rows, float4 *__restrict__ out, int nslices, int A,
-                                   int Wg)
+// Window rows [nslices][nangles][Wg] of 4-byte (E = uint32_t: f32, bf16 pair) or
+// 8-byte (E = uint2: f32 pair) elements -> [ceil(nslices/4)][nangles][Wg][4],
+// slices beyond nslices zero; a bit copy, one CTA per (group, angle) row.
+template <typename E>
+__global__ void interleave4_kernel(const E *__restrict__ rows, E *__restrict__ out, int nslices, int A, int Wg)
 {
     const int r = blockIdx.x, g = r / A, a = r - g * A;
-    const float *src[4];
+    const E *src[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) src[q] = 4 * g + q < nslices ? rows + ((size_t)(4 * g + q) * A + a) * Wg : nullptr;
-    float4 *dst = out + (size_t)r * Wg;
-    for (int e = threadIdx.x; e < Wg; e += blockDim.x)
-        dst[e] = make_float4(src[0] ? __ldcs(src[0] + e) : 0.f, src[1] ? __ldcs(src[1] + e) : 0.f,
-                             src[2] ? __ldcs(src[2] + e) : 0.f, src[3] ? __ldcs(src[3] + e) : 0.f);
+    E *dst = out + (size_t)r * Wg * 4;
+    E zero;
+    memset(&zero, 0, sizeof(E));
+    for (int e = threadIdx.x; e < Wg; e += blockDim.x) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) dst[4 * e + q] = src[q] ? __ldcs(src[q] + e) : zero;
+    }
 }
 
 // ------------------------------------------------------------------------
@@ -564,13 +587,8 @@ static void launch_bp_cfg(const BpArgs &a, BpTune t, cudaStream_t st)
     case 1: launch_bp_s<GEOM, STORE, 1>(a, t.AB, st); break;
     case 2: launch_bp_s<GEOM, STORE, 2>(a, t.AB, st); break;
     default:
-        if constexpr (GEOM != GEOM_FBP_LIN && STORE == STORE_F32) {
-            if (a.il) {
-                launch_bp_s<GEOM, STORE, 4, true>(a, t.AB, st);
-                break;
-            }
-        }
-        launch_bp_s<GEOM, STORE, 4>(a, t.AB, st);
+        if (a.il) launch_bp_s<GEOM, STORE, 4, true>(a, t.AB, st);
+        else launch_bp_s<GEOM, STORE, 4>(a, t.AB, st);
         break;
     }
 }
@@ -727,9 +745,9 @@ static BpArgs to_args(const BpLaunch &bl)
     return a;
 }
 
-size_t bp_il_bytes(int nslices, int nangles, int Wg)
+size_t bp_il_bytes(int nslices, int nangles, int Wg, int esize)
 {
-    return (size_t)((nslices + 3) / 4) * nangles * Wg * 16;
+    return (size_t)((nslices + 3) / 4) * nangles * Wg * 4 * esize;
 }
 
 void launch_backproject(const BpLaunch &bl, cudaStream_t st)
@@ -738,7 +756,9 @@ void launch_backproject(const BpLaunch &bl, cudaStream_t st)
     const BpArgs a = to_args(bl);
     const int store = bl.geometry == GEOM_FBP_LIN ? bl.store : STORE_F32;
     // four slices per CTA on slice-interleaved rows, when the caller provides the workspace
-    const bool il_ok = bl.il_ws && bl.geometry != GEOM_FBP_LIN;
+    // (4-byte elements: f32 samples and bf16 pairs; the 8-byte f32 pairs keep
+    // their planar rows, whose S = 4 shape measured faster)
+    const bool il_ok = bl.il_ws != nullptr && a.esize == 4;
     BpArgs a_il = a;
     a_il.filt = reinterpret_cast<const unsigned char *>(bl.il_ws);
     a_il.il = 1;
@@ -746,9 +766,15 @@ void launch_backproject(const BpLaunch &bl, cudaStream_t st)
     auto prep_il = [&]() {
         if (il_done) return;
         count_launch();
-        interleave4_kernel<<<(unsigned)(((bl.nslices + 3) / 4) * bl.nangles), 256, 0, st>>>(
-            reinterpret_cast<const float *>(bl.filt), reinterpret_cast<float4 *>(bl.il_ws), bl.nslices, bl.nangles,
-            bl.win.Wg);
+        const unsigned grid = (unsigned)(((bl.nslices + 3) / 4) * bl.nangles);
+        if (a.esize == 8)
+            interleave4_kernel<uint2><<<grid, 256, 0, st>>>(reinterpret_cast<const uint2 *>(bl.filt),
+                                                          reinterpret_cast<uint2 *>(bl.il_ws), bl.nslices,
+                                                          bl.nangles, bl.win.Wg);
+        else
+            interleave4_kernel<uint32_t><<<grid, 256, 0, st>>>(reinterpret_cast<const uint32_t *>(bl.filt),
+                                                             reinterpret_cast<uint32_t *>(bl.il_ws), bl.nslices,
+                                                             bl.nangles, bl.win.Wg);
         RAFT_CUDA(cudaGetLastError());
         il_done = true;
     };

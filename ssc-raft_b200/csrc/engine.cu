@@ -322,13 +322,13 @@ void fbp_chunk(DeviceState &ds, const FbpPrepared &fp, const FbpTables &tb, cons
     bl.csd = tb.csd;
     bl.snd = tb.snd;
     bl.err = tb.err;
-    bl.il_ws = fp.cfg.geometry == GEOM_FBP_REF ? d_il : nullptr;
+    bl.il_ws = d_il;
     launch_backproject(bl, st);
 }
 
 size_t fbp_il_bytes(const FbpPrepared &fp, int nslices)
 {
-    return fp.cfg.geometry == GEOM_FBP_REF ? bp_il_bytes(nslices, fp.cfg.nangles, fp.win.Wg) : 0;
+    return store_bytes(fp.cfg.store) == 4 ? bp_il_bytes(nslices, fp.cfg.nangles, fp.win.Wg, 4) : 0;
 }
 
 static void check_device_flag(const int *d_err, const char *what)
@@ -640,7 +640,7 @@ void em_chunk(DeviceState &ds, const EmPrepared &ep, int kind, const float *d_da
     bl.cs = cs;
     bl.sn = sn;
     bl.err = err;
-    bl.il_ws = ds.il.get(bp_il_bytes(nslices, A, win.Wg));
+    bl.il_ws = ds.il.get(bp_il_bytes(nslices, A, win.Wg, 4));
 
     // sensitivity image: BP of the counts (tEM, em_rt.cu:178) or of ones (eEM, :343)
     launch_to_window(kind == 0 ? d_data : nullptr, rows, wt, nslices * A, A, n, win.wlo, win.Wg, st);

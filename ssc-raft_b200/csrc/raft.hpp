@@ -154,13 +154,13 @@ struct BpLaunch {
     const float *cs = nullptr, *sn = nullptr;     // FP32 angle tables
     const double *csd = nullptr, *snd = nullptr;  // FP64 angle tables
     int *err = nullptr;                           // device error flag
-    // optional workspace of bp_il_bytes(): lets nearest (FBP / EM) launches of
-    // four slices per CTA read the rows interleaved by slice (made here)
+    // optional workspace of bp_il_bytes(): lets launches of four slices per
+    // CTA read the rows interleaved by slice (made here)
     void *il_ws = nullptr;
 };
 
 void launch_backproject(const BpLaunch &bl, cudaStream_t st);
-size_t bp_il_bytes(int nslices, int nangles, int Wg);
+size_t bp_il_bytes(int nslices, int nangles, int Wg, int esize);
 
 // Backprojector launch shape chosen by the autotuner: S slices per CTA
 // (sharing each pixel's position arithmetic) and AB angles per pipeline stage.
