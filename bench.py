@@ -685,7 +685,9 @@ def run_ours(args):
     sm_mhz = (clocks or {}).get("sm_mhz") or sm_max
     gups_bp = upd_per_launch / bp_avg_s / 1e9
     peak_gups = gather_peak_gups(4, 4, sm_mhz)
-    for name, (g, s, bytes_upd, ops) in (("linear_fp32", (1, 1, 8, 5)), ("linear_bf16", (1, 2, 4, 7))):
+    # f32 pairs: 8 B + 5 FP32 ops per update; bf16 pairs on slice-interleaved rows:
+    # 4 B + 4 ops (two FP32, two integer to unpack the pair)
+    for name, (g, s, bytes_upd, ops) in (("linear_fp32", (1, 1, 8, 5)), ("linear_bf16", (1, 2, 4, 4))):
         _, _, vms, vn = profile_bp(g, s)
         vg = upd_per_launch / (vms / vn / 1e3) / 1e9
         pk = gather_peak_gups(bytes_upd, ops, sm_mhz)
