@@ -131,6 +131,15 @@ int raft_last_error(char *buf, int len);
 void raft_clear_error(void);
 int raft_abi_version(void);
 
+/* Failure injection: the next n device-buffer requests of the library fail as
+ * an out-of-memory would (the call reports the error; the library stays
+ * usable); n = 0 clears it. */
+void raft_inject_alloc_failures(int n);
+/* Self test of the bounded device-side wait of the staging pipelines: 1 if a
+ * wait on a barrier nothing arrives on (arrive = 0) ran out after `limit` polls
+ * and was reported, 0 if it completed (arrive = 1), -1 on error. */
+int raft_selftest_bounded_wait(int gpu, int arrive, unsigned limit);
+
 /* FBP with a selectable operator and sinogram storage (host buffers).
  * geometry 0 = reference nearest-sample rule (store must be 0),
  * geometry 1 = linear interpolation with true ramp-family filters

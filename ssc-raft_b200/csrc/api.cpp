@@ -225,6 +225,25 @@ int raft_last_error(char *buf, int len)
 
 void raft_clear_error(void) { clear_error(); }
 
+// Failure injection: the next n device-buffer requests of the library fail (as
+// an out-of-memory would): the entry point reports the error and the library
+// stays usable.  n = 0 clears it.
+void raft_inject_alloc_failures(int n) { inject_alloc_failures(n); }
+
+// Self test of the bounded device-side wait the staging pipelines use: returns
+// 1 if a wait on a barrier nothing arrives on (arrive = 0) ran out after `limit`
+// polls and was reported, 0 if the wait completed (arrive = 1), -1 on error.
+int raft_selftest_bounded_wait(int gpu, int arrive, unsigned limit)
+{
+    clear_error();
+    if (!check_gpus(&gpu, 1)) return -1;
+    try {
+        return selftest_bounded_wait(gpu, arrive, limit);
+    } catch (const CudaFail &) {
+    }
+    return -1;
+}
+
 int raft_abi_version(void) { return 1; }
 
 // Host-only: the slab each of `ngpus` devices receives for `nslices` slices.

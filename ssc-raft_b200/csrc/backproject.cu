@@ -466,6 +466,40 @@ bp_ragged_kernel(const BpArgs *__restrict__ reqs, const int *__restrict__ item_s
 }
 
 // ------------------------------------------------------------------------
+// Self test of the bounded staging wait: one thread waits on an mbarrier that
+// is arrived on (arrive = 1) or that nothing ever arrives on (arrive = 0); a
+// wait that runs out after `limit` polls sets the flag, as the staging
+// pipeline does, and the kernel returns.
+// ------------------------------------------------------------------------
+__global__ void bounded_wait_selftest_kernel(int arrive, unsigned limit, int *err)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+    if (arrive) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&bar)) : "memory");
+    if (!mbar_wait_bounded(&bar, 0, limit)) atomicExch(err, 1);
+}
+
+int selftest_bounded_wait(int gpu, int arrive, unsigned limit)
+{
+    RAFT_CUDA(cudaSetDevice(gpu));
+    int *d_err = nullptr;
+    RAFT_CUDA(cudaMalloc(&d_err, sizeof(int)));
+    int h = -1;
+    cudaError_t e = cudaMemset(d_err, 0, sizeof(int));
+    if (e == cudaSuccess) {
+        count_launch();
+        bounded_wait_selftest_kernel<<<1, 32>>>(arrive, limit, d_err);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d_err);
+    RAFT_CUDA(e);
+    return h;
+}
+
+// ------------------------------------------------------------------------
 // angle tables: the reference computes sin/cos with the fast intrinsics,
 // __sinf/__cosf for FBP (opt.cu:187-194) and __sincosf for EM
 // (em_RT_kernel.cu:120); angle steps as em_RT_kernel.cu:122-126 / fbp.cu:61-64.

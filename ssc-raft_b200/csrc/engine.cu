@@ -18,6 +18,8 @@
 // loop is captured once as a CUDA graph and replayed as a single launch.
 #include "engine.hpp"
 
+#include <atomic>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -29,9 +31,22 @@
 namespace raft {
 
 // ----------------------------------------------------------- buffers ------
+// Injected allocation refusals (raft_inject_alloc_failures): the next n
+// device-buffer requests of the engine fail as an out-of-memory would
+// (whether or not the buffer would have grown).
+static std::atomic<int> g_alloc_failures{0};
+void inject_alloc_failures(int n) { g_alloc_failures.store(n > 0 ? n : 0); }
+
 void *DevBuf::get(size_t need)
 {
     if (need == 0) need = 16;
+    int left = g_alloc_failures.load();
+    while (left > 0 && !g_alloc_failures.compare_exchange_weak(left, left - 1)) {
+    }
+    if (left > 0) {
+        set_error("device allocation of " + std::to_string(need) + " bytes refused (injected failure)");
+        throw CudaFail{};
+    }
     if (need > bytes) {
         if (ptr) cudaFree(ptr);
         ptr = nullptr;

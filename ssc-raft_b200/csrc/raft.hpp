@@ -312,6 +312,10 @@ struct EmConfig {
     int nflats = 1;
 };
 
+// Failure injection and self tests (engine.cu, backproject.cu).
+void inject_alloc_failures(int n);
+int selftest_bounded_wait(int gpu, int arrive, unsigned limit);
+
 // U-Net 3x3 convolution on tcgen05 (unet_tc.cu): 0 launched, 1 launch error,
 // 2 shape not handled (W must be >= 128 or divide 128; channels multiples of 32).
 bool conv3x3_tc_supported(int C0, int C1, int W);

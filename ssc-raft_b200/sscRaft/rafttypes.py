@@ -58,6 +58,10 @@ libraft.raft_last_error.argtypes = [ctypes.c_char_p, _I]
 libraft.raft_last_error.restype = _I
 libraft.raft_clear_error.argtypes = []
 libraft.raft_clear_error.restype = None
+libraft.raft_inject_alloc_failures.argtypes = [_I]
+libraft.raft_inject_alloc_failures.restype = None
+libraft.raft_selftest_bounded_wait.argtypes = [_I, _I, ctypes.c_uint]
+libraft.raft_selftest_bounded_wait.restype = _I
 libraft.raft_abi_version.argtypes = []
 libraft.raft_abi_version.restype = _I
 libraft.raft_fbp_ext.argtypes = [_P, _I, _P, _P, _P, _P, _P, _I, _I]
