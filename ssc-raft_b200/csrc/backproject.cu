@@ -668,7 +668,7 @@ static bool forced_tune(BpTune &t)
 }
 
 // Pick (S, AB) for this configuration: the cached choice, else time every
-// candidate that fits shared memory on up to 8 slices of the real data
+// candidate that fits shared memory on 8 to 32 slices of the real data
 // (store launches only -- they are idempotent), else a default.  With
 // a_il (the same launch on slice-interleaved rows) the S = 4 candidates are
 // timed on it; prep_il makes those rows and is called at most once.
@@ -693,8 +693,12 @@ static BpTune choose_tune(const BpArgs &a, const BpArgs *a_il, Prep &&prep_il, i
     cudaStreamIsCapturing(st, &cap);
     const bool can_tune = tuning_enabled() && a.update == 0 && cap == cudaStreamCaptureStatusNone;
     if (can_tune) {
+        // enough slices that a four-slice grid is several waves deep (a shallow
+        // grid's tail would favour the smaller slice groups), 8 to 32
         BpArgs t0 = a;
-        t0.nslices = std::min(a.nslices, 8);
+        const long long tiles = (long long)((a.No + BP_TX - 1) / BP_TX) * ((a.No + BP_TY - 1) / BP_TY);
+        const int want = (int)std::min<long long>(32, std::max<long long>(8, (4LL * 3 * 148 * 8 + tiles - 1) / tiles));
+        t0.nslices = std::min(a.nslices, (want + 3) / 4 * 4);
         cudaEvent_t e0, e1;
         RAFT_CUDA(cudaEventCreate(&e0));
         RAFT_CUDA(cudaEventCreate(&e1));
