@@ -42,7 +42,15 @@ __device__ __forceinline__ double warp_sum(double v)
 // 32 rays of the warp touch consecutive addresses; the index arithmetic and
 // therefore the chosen pixels are unchanged.  IL = 1 (S = 8) reads the
 // slice-interleaved copies instead (il[g][y][x][8], ilT[g][x][y][8]): one
-// sample's eight slice values are two 16-byte loads from one 32-byte sector.
+// sample's eight slice values are one 32-byte load (one sector).
+// 256-bit read-only load of eight consecutive floats (32-byte aligned)
+__device__ __forceinline__ void ldg_v8(const float *p, float (&w)[8])
+{
+    asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(w[0]), "=f"(w[1]), "=f"(w[2]), "=f"(w[3]), "=f"(w[4]), "=f"(w[5]), "=f"(w[6]), "=f"(w[7])
+                 : "l"(p));
+}
+
 template <int EM, int EPI, int S, int IL>
 __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx, const int by, const int bz)
 {
@@ -87,12 +95,11 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
                     const bool in = (X >= 0) & (X < limx) & (Y >= 0) & (Y < limy);
                     const size_t off = (size_t)(in ? Y : 0) * sy + (size_t)(in ? X : 0) * sx;
                     if constexpr (IL) {
-                        const float4 *px = reinterpret_cast<const float4 *>(img + off * 8);
-                        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-                        const float4 lo = in ? __ldg(px) : zero;
-                        const float4 hi = in ? __ldg(px + 1) : zero;
-                        v[u][0] = lo.x; v[u][1] = lo.y; v[u][2] = lo.z; v[u][3] = lo.w;
-                        v[u][4] = hi.x; v[u][5] = hi.y; v[u][6] = hi.z; v[u][7] = hi.w;
+                        // one 32-byte load: the pixel's eight slice values (pixel 0 when outside)
+                        float w[8];
+                        ldg_v8(img + off * 8, w);
+#pragma unroll
+                        for (int q = 0; q < 8; q++) v[u][q] = in ? w[q] : 0.f;
                     } else {
                         const float *pix = img + off;
 #pragma unroll
@@ -113,9 +120,8 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
                 if ((X >= 0) & (X < limx) & (Y >= 0) & (Y < limy)) {
                     const size_t off = (size_t)Y * sy + (size_t)X * sx;
                     if constexpr (IL) {
-                        const float4 *px = reinterpret_cast<const float4 *>(img + off * 8);
-                        const float4 lo = __ldg(px), hi = __ldg(px + 1);
-                        const float w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+                        float w[8];
+                        ldg_v8(img + off * 8, w);
 #pragma unroll
                         for (int q = 0; q < S; q++) linesum[q] += w[q];
                     } else {
