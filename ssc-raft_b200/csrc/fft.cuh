@@ -195,7 +195,14 @@ __device__ __noinline__ void fft_pass(const float2 *__restrict__ src, float2 *__
         if (k > 0) {
             // w^r, r < R, from w = exp(-2 pi i k twstep / Np) by repeated products
             // (two complex registers live; relative error of w^7 a few 1e-7)
-            const float2 w1 = __ldg(&tw[k * twstep]);
+            float2 w1;
+            {
+                // exp(-2 pi i k twstep / Np) computed in place of a (latency-bound)
+                // table load; sincospif rounds to about one unit in the last place
+                float sn, cs;
+                sincospif(-2.0f * (float)(k * twstep) / (float)Np, &sn, &cs);
+                w1 = make_float2(cs, sn);
+            }
             float2 w = w1;
 #pragma unroll
             for (int r = 1; r < R; r++) {
