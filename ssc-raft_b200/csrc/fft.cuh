@@ -1,5 +1,5 @@
 // fft.cuh -- the self-sorting (Stockham) mixed-radix complex FFT shared by the
-// filter, BST and rotation-axis kernels.
+// filter, BST, tEMFQ and rotation-axis kernels.
 //
 // A CTA transforms one length-n sequence held in shared memory, ping-ponging
 // between two buffers of fft_span(n) elements each; radices 2, 3, 4, 5, 7, 8
@@ -7,10 +7,11 @@
 // read from, and the result left in, plain order; intermediate passes store
 // one pad element after every 16 (n <= 12288) so that the strided writes of
 // the early passes spread over the shared-memory banks.  Twiddles: one value
-// exp(-2 pi i k / n) per butterfly from a table built in FP64 on the host, its
-// powers by repeated complex products.  Only the
-// forward transform exists: an inverse is the forward transform of the
-// conjugate, conjugated.
+// exp(-2 pi i k / n) per butterfly from sincospif (a table load from global
+// memory was latency-bound; the host-built FP64 table stays available to the
+// callers), its powers by repeated complex products.  Only the forward
+// transform exists: an inverse is the forward transform of the conjugate,
+// conjugated.
 #pragma once
 
 #include <cuda_runtime.h>
