@@ -268,6 +268,9 @@ int raft_unet_conv_fwd(const void *x0, int C0, const void *x1, int C1, const voi
  * or W dividing 128), mma.sync kernel otherwise (default); 1 = mma.sync kernel only;
  * 2 = tcgen05 kernel only (other shapes fail). */
 int raft_unet_set_conv_path(int path);
+/* tcgen05 convolution of the 32 -> 32 channel layers (W >= 128): 1 = halo tiles (one input
+ * box per 32-channel chunk serves all nine taps; default), 0 = one input box per tap. */
+int raft_unet_set_conv_halo(int on);
 /* 1 if a bounded pipeline wait of the tcgen05 convolution ran out since the last call
  * (the flag is then cleared); synchronises the current device. */
 int raft_unet_conv_error(void);

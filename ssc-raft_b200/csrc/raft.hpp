@@ -322,5 +322,6 @@ bool conv3x3_tc_supported(int C0, int C1, int W);
 int conv3x3_tc(const void *x0, int C0, const void *x1, int C1, const void *w, const float *bias, void *y, void *y1,
                int Cy0, int N, int H, int W, int Cout, int relu, cudaStream_t st);
 int conv3x3_tc_error();
+void conv3x3_tc_set_halo(int on);
 
 }  // namespace raft

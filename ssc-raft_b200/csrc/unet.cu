@@ -606,6 +606,14 @@ int raft_unet_set_conv_path(int path)
     return 0;
 }
 
+// Halo tiles of the tcgen05 convolution for its 32 -> 32 channel layers (1, the
+// default) or the per-tap operand tiles for every layer (0).
+int raft_unet_set_conv_halo(int on)
+{
+    conv3x3_tc_set_halo(on);
+    return 0;
+}
+
 // 1 if a bounded wait of the tcgen05 convolution ran out since the last call
 // (the flag is cleared); synchronises the current device.
 int raft_unet_conv_error(void) { return conv3x3_tc_error(); }

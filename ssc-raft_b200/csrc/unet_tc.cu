@@ -119,6 +119,24 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t sbo_bytes
            ((uint64_t)1 << 46) | ((uint64_t)layout << 61);
 }
 
+// Shared-memory matrix descriptor, K-major, no swizzle: 8-row x 16-byte core
+// matrices, rows 16 bytes apart, 8-row groups `sbo` bytes apart, the two
+// 8-element K halves of an MMA `lbo` bytes apart.
+__device__ __forceinline__ uint64_t umma_desc_interleaved(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo_bytes >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+
+// Halo tiles (the level-0 layers: 32 channels in, 32 out, W >= 128): one tile =
+// 4 rows x 128 pixels (MT = 4 MMA blocks); a k-block is one 32-channel chunk
+// with all nine taps.  The input arrives once per k-block as a (4+2) x 136
+// pixel halo box, 8 channels per plane ([row][16 B], the unswizzled K-major
+// layout), so a tap's 128-row operand is the plane region starting at row
+// (mt + ky + 1) * 136 + kx + 1: a descriptor offset, no reload.
+constexpr int HB_W = 136, HB_H = 6, HB_ROWS = HB_W * HB_H;
+constexpr int HB_PLANE = HB_ROWS * 16;     // one 8-channel plane (13056 bytes)
+
 // ------------------------------------------------------------------- TMA
 __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
                                             uint64_t *bar)
@@ -175,13 +193,16 @@ __device__ __forceinline__ TileCoord tile_coord(const TcArgs &a, int t, int BN)
     return c;
 }
 
-template <int BN, int KC, int MT, int ST>
+template <int BN, int KC, int MT, int ST, bool HALO = false>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     conv3x3_tc_kernel(const __grid_constant__ CUtensorMap mx0, const __grid_constant__ CUtensorMap mx1,
                       const __grid_constant__ CUtensorMap mw, const TcArgs a)
 {
+    static_assert(!HALO || (BN == 32 && KC == 32 && MT == 4), "halo tiles: 32 -> 32 channels, 4 MMA blocks");
     constexpr int A_PART = TC_M * KC * 2;                  // one 128-row MMA operand
-    constexpr int A_BYTES = MT * A_PART, B_BYTES = BN * KC * 2, STAGE = A_BYTES + B_BYTES;
+    constexpr int B_TAP = BN * KC * 2;                     // one tap's weights
+    constexpr int A_BYTES = HALO ? (KC / 8) * HB_PLANE : MT * A_PART;
+    constexpr int B_BYTES = HALO ? 9 * B_TAP : B_TAP, STAGE = A_BYTES + B_BYTES;
     constexpr uint32_t SBO = 8 * KC * 2;                   // one 8-row swizzle atom
     constexpr uint32_t LAYOUT = KC == 64 ? 2u : 4u;        // 128-byte / 64-byte swizzle
     constexpr uint32_t ACC = MT * BN;                      // TMEM columns of one accumulator buffer
@@ -226,7 +247,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     const int Cin = a.C0 + a.C1;
-    const int kb_per_tile = 9 * (Cin / KC);
+    const int kb_per_tile = HALO ? Cin / KC : 9 * (Cin / KC);
 
     if (warp == 0) {
         // ---------------------------------------------------------- producer
@@ -236,16 +257,29 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             for (int t = blockIdx.x; t < a.tiles && ok; t += gridDim.x) {
                 const TileCoord c = tile_coord(a, t, BN);
                 for (int kb = 0; kb < kb_per_tile && ok; ++kb, ++g) {
-                    const int tap = kb / (Cin / KC), cc = (kb % (Cin / KC)) * KC;
-                    const int ky = tap / 3 - 1, kx = tap % 3 - 1;
                     const int s = (int)(g % ST);
                     const uint32_t u = g / ST;
                     if (u >= 1 && !(ok = tc_wait(&empty[s], (u - 1) & 1, abort_flag, a.err))) break;
                     uint8_t *st = base + s * STAGE;
                     mbar_arrive_expect_tx(&full[s], STAGE);
-                    if (cc < a.C0) tma_load_4d(st, &mx0, cc, c.x0 + kx, c.y0 + ky, c.n, &full[s]);
-                    else tma_load_4d(st, &mx1, cc - a.C0, c.x0 + kx, c.y0 + ky, c.n, &full[s]);
-                    tma_load_2d(st + A_BYTES, &mw, tap * Cin + cc, c.co0, &full[s]);
+                    if constexpr (HALO) {
+                        // the halo box of one 32-channel chunk, one plane per 8 channels; all nine taps' weights
+                        const int cc = kb * KC;
+                        const CUtensorMap *mx = cc < a.C0 ? &mx0 : &mx1;
+                        const int ch = cc < a.C0 ? cc : cc - a.C0;
+#pragma unroll
+                        for (int pl = 0; pl < KC / 8; ++pl)
+                            tma_load_4d(st + pl * HB_PLANE, mx, ch + 8 * pl, c.x0 - 1, c.y0 - 1, c.n, &full[s]);
+#pragma unroll 1
+                        for (int tap = 0; tap < 9; ++tap)
+                            tma_load_2d(st + A_BYTES + tap * B_TAP, &mw, tap * Cin + cc, c.co0, &full[s]);
+                    } else {
+                        const int tap = kb / (Cin / KC), cc = (kb % (Cin / KC)) * KC;
+                        const int ky = tap / 3 - 1, kx = tap % 3 - 1;
+                        if (cc < a.C0) tma_load_4d(st, &mx0, cc, c.x0 + kx, c.y0 + ky, c.n, &full[s]);
+                        else tma_load_4d(st, &mx1, cc - a.C0, c.x0 + kx, c.y0 + ky, c.n, &full[s]);
+                        tma_load_2d(st + A_BYTES, &mw, tap * Cin + cc, c.co0, &full[s]);
+                    }
                 }
             }
             // every issued load lands before the CTA may exit: the last use of
@@ -271,13 +305,31 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     if (!(ok = tc_wait(&full[s], u & 1, abort_flag, a.err))) break;
                     tc_fence_after();
                     const uint32_t sa = smem_u32(base + s * STAGE);
-                    const uint64_t bd = umma_desc(sa + A_BYTES, SBO, LAYOUT);
+                    if constexpr (HALO) {
+#pragma unroll 1
+                        for (int tap = 0; tap < 9; ++tap) {
+                            const int ky = tap / 3, kx = tap % 3;          // offsets + 1
+                            const uint64_t bd = umma_desc(sa + A_BYTES + tap * B_TAP, SBO, LAYOUT);
 #pragma unroll
-                    for (int mt = 0; mt < MT; ++mt) {
-                        const uint64_t ad = umma_desc(sa + mt * A_PART, SBO, LAYOUT);
+                            for (int mt = 0; mt < MT; ++mt) {
+                                const uint32_t row0 = (uint32_t)((mt + ky) * HB_W + kx);
 #pragma unroll
-                        for (int j = 0; j < KC / 16; ++j)   // K = 16 per MMA: 32 bytes further along the swizzled row
-                            tc_mma(d + mt * BN, ad + (uint64_t)(2 * j), bd + (uint64_t)(2 * j), IDESC, (kb | j) != 0);
+                                for (int j = 0; j < KC / 16; ++j)   // K halves in planes 2j, 2j + 1
+                                    tc_mma(d + mt * BN,
+                                           umma_desc_interleaved(sa + 2 * j * HB_PLANE + row0 * 16, HB_PLANE, 128),
+                                           bd + (uint64_t)(2 * j), IDESC, (kb | tap | j) != 0);
+                            }
+                        }
+                    } else {
+                        const uint64_t bd = umma_desc(sa + A_BYTES, SBO, LAYOUT);
+#pragma unroll
+                        for (int mt = 0; mt < MT; ++mt) {
+                            const uint64_t ad = umma_desc(sa + mt * A_PART, SBO, LAYOUT);
+#pragma unroll
+                            for (int j = 0; j < KC / 16; ++j)   // K = 16 per MMA: 32 bytes further along the swizzled row
+                                tc_mma(d + mt * BN, ad + (uint64_t)(2 * j), bd + (uint64_t)(2 * j), IDESC,
+                                       (kb | j) != 0);
+                        }
                     }
                     tc_commit(&empty[s]);
                 }
@@ -437,6 +489,41 @@ bool encode_act(CUtensorMap *m, const void *ptr, int C, int N, int H, int W, int
                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// halo boxes: 8 channels (16 bytes, unswizzled) x HB_W pixels x HB_H rows
+bool encode_act_halo(CUtensorMap *m, const void *ptr, int C, int N, int H, int W)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return false;
+    cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+    cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+    cuuint32_t box[4] = {8, (cuuint32_t)HB_W, (cuuint32_t)HB_H, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(ptr), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// halo-tile instance: 32 -> 32 channels, two stages of one halo box and nine weight boxes
+int launch_tc_halo(const CUtensorMap &m0, const CUtensorMap &m1, const CUtensorMap &mw, const TcArgs &a,
+                   cudaStream_t st)
+{
+    constexpr int STAGE = 4 * HB_PLANE + 9 * 32 * 32 * 2, ST = 2;
+    static_assert(STAGE % 1024 == 0, "stage alignment");
+    constexpr size_t SMEM = (size_t)ST * STAGE + 1024 + 256;
+    auto kern = conv3x3_tc_kernel<32, 32, 4, ST, true>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM) != cudaSuccess) return 1;
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    int dev = 0, sms = 148, occ = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TC_THREADS, SMEM) != cudaSuccess || occ < 1)
+        occ = 1;
+    const int grid = std::max(1, std::min(a.tiles, sms * occ));
+    count_launch();
+    kern<<<grid, TC_THREADS, SMEM, st>>>(m0, m1, mw, a);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
 bool encode_w(CUtensorMap *m, const void *ptr, int Cout, int Cin, int KC, int BN)
 {
     EncodeTiledFn enc = encode_fn();
@@ -450,7 +537,11 @@ bool encode_w(CUtensorMap *m, const void *ptr, int Cout, int Cin, int KC, int BN
                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+bool g_halo = true;   // halo tiles for the 32 -> 32 channel layers (raft_unet_set_conv_halo)
+
 }  // namespace
+
+void conv3x3_tc_set_halo(int on) { g_halo = on != 0; }
 
 bool conv3x3_tc_supported(int C0, int C1, int W)
 {
@@ -503,6 +594,22 @@ int conv3x3_tc(const void *x0, int C0, const void *x1, int C1, const void *w, co
     cudaGetDevice(&dev);
     a.err = tc_err_flag(dev);
     CUtensorMap m0, m1, mw;
+    if (g_halo && Cout == 32 && KC == 32 && W >= TC_M) {
+        // halo tiles: 4 rows x 128 pixels, the taps served from one box per channel chunk
+        TcArgs h = a;
+        h.BW = TC_M;
+        h.BH = 4;
+        h.n_xb = (W + TC_M - 1) / TC_M;
+        h.n_yb = (H + 3) / 4;
+        h.n_co = 1;
+        const long long ht = (long long)N * h.n_yb * h.n_xb;
+        if (ht > 0 && ht <= (1LL << 30) && encode_act_halo(&m0, x0, C0, N, H, W) &&
+            (C1 == 0 || encode_act_halo(&m1, x1, C1, N, H, W)) && encode_w(&mw, w, Cout, C0 + C1, 32, 32)) {
+            if (C1 == 0) m1 = m0;
+            h.tiles = (int)ht;
+            return launch_tc_halo(m0, m1, mw, h, st);
+        }
+    }
     if (!encode_act(&m0, x0, C0, N, H, W, KC, a.BW, a.BH)) return 2;
     if (C1 > 0) {
         if (!encode_act(&m1, x1, C1, N, H, W, KC, a.BW, a.BH)) return 2;

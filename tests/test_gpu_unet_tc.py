@@ -96,3 +96,26 @@ def test_tc_only_path_rejects_other_widths():
     # the default path takes the mma.sync kernel for this width
     assert libraft.raft_unet_conv_fwd(ws._p(x), 32, None, 0, ws._p(w), None, ws._p(y), None, 0,
                                       1, 2, 70, 32, 0, None) == 0
+
+
+@pytest.mark.parametrize("N,H,W,C0,C1", [(1, 5, 128, 32, 0), (2, 3, 130, 32, 0), (1, 6, 256, 64, 32), (1, 4, 512, 32, 0)])
+def test_tc_conv_halo_tiles(oracle, N, H, W, C0, C1):
+    # 32 -> 32 channel layers use halo tiles (one input box per 32-channel chunk serves
+    # all nine taps); same results as the per-tap tiles and the oracle
+    import torch
+    from sscRaft.rafttypes import libraft
+    torch.manual_seed(7 + H + W + C0 + C1)
+    x0 = _bf(torch.randn(N, H, W, C0, device="cuda"))
+    x1 = _bf(torch.randn(N, H, W, C1, device="cuda")) if C1 else None
+    w = _bf(torch.randn(32, 3, 3, C0 + C1, device="cuda") * 0.1)
+    b = torch.randn(32, device="cuda")
+    y_halo = _conv(x0, x1, w, b, N, H, W, C0, C1, 32)
+    libraft.raft_unet_set_conv_halo(0)
+    try:
+        y_tap = _conv(x0, x1, w, b, N, H, W, C0, C1, 32)
+    finally:
+        libraft.raft_unet_set_conv_halo(1)
+    xc = _f64(x0) if x1 is None else np.concatenate([_f64(x0), _f64(x1)], axis=-1)
+    ref = oracle.conv3x3(xc, _f64(w), _f64(b), relu=True)
+    assert rel_l2(_f64(y_halo), ref) <= 1e-2, rel_l2(_f64(y_halo), ref)
+    assert rel_l2(_f64(y_halo), _f64(y_tap)) <= 2e-3, rel_l2(_f64(y_halo), _f64(y_tap))
