@@ -119,23 +119,14 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t sbo_bytes
            ((uint64_t)1 << 46) | ((uint64_t)layout << 61);
 }
 
-// Shared-memory matrix descriptor, K-major, no swizzle: 8-row x 16-byte core
-// matrices, rows 16 bytes apart, 8-row groups `sbo` bytes apart, the two
-// 8-element K halves of an MMA `lbo` bytes apart.
-__device__ __forceinline__ uint64_t umma_desc_interleaved(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes)
-{
-    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo_bytes >> 4) & 0x3FFF) << 16) |
-           ((uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
-}
-
 // Halo tiles (the level-0 layers: 32 channels in, 32 out, W >= 128): one tile =
 // 4 rows x 128 pixels (MT = 4 MMA blocks); a k-block is one 32-channel chunk
-// with all nine taps.  The input arrives once per k-block as a (4+2) x 136
-// pixel halo box, 8 channels per plane ([row][16 B], the unswizzled K-major
-// layout), so a tap's 128-row operand is the plane region starting at row
-// (mt + ky + 1) * 136 + kx + 1: a descriptor offset, no reload.
+// with all nine taps.  The input arrives once per k-block as one (4+2) x 136
+// pixel halo box (64-byte swizzled rows), so a tap's 128-row operand starts
+// at row (mt + ky + 1) * 136 + kx + 1 of it: a descriptor offset, no reload.
+// The MMA applies the swizzle to absolute shared-memory addresses, as the TMA
+// unit does (base offset 0 at any row; checked against the oracle).
 constexpr int HB_W = 136, HB_H = 6, HB_ROWS = HB_W * HB_H;
-constexpr int HB_PLANE = HB_ROWS * 16;     // one 8-channel plane (13056 bytes)
 
 // ------------------------------------------------------------------- TMA
 __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
@@ -201,13 +192,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     static_assert(!HALO || (BN == 32 && KC == 32 && MT == 4), "halo tiles: 32 -> 32 channels, 4 MMA blocks");
     constexpr int A_PART = TC_M * KC * 2;                  // one 128-row MMA operand
     constexpr int B_TAP = BN * KC * 2;                     // one tap's weights
-    constexpr int A_BYTES = HALO ? (KC / 8) * HB_PLANE : MT * A_PART;
+    constexpr int A_BYTES = HALO ? HB_ROWS * KC * 2 : MT * A_PART;
     constexpr int B_BYTES = HALO ? 9 * B_TAP : B_TAP, STAGE = A_BYTES + B_BYTES;
     constexpr uint32_t SBO = 8 * KC * 2;                   // one 8-row swizzle atom
     constexpr uint32_t LAYOUT = KC == 64 ? 2u : 4u;        // 128-byte / 64-byte swizzle
     constexpr uint32_t ACC = MT * BN;                      // TMEM columns of one accumulator buffer
     constexpr uint32_t TMEM_COLS = 2 * ACC < 32 ? 32 : 2 * ACC;
     static_assert(2 * ACC <= 512, "two accumulator buffers must fit in TMEM");
+    // lanes of the MMA warp that issue: halo tiles issue their MT blocks from MT
+    // lanes at once (one warp instruction, MT MMAs); each issuing lane commits
+    constexpr int NISSUE = HALO ? MT : 1;
     static_assert(STAGE % 1024 == 0, "stages must keep 1024-byte alignment");
     static_assert(BN % 32 == 0 && BN <= 256 && (KC == 32 || KC == 64), "tile shape");
     // instruction descriptor: D F32, A/B BF16, both K-major, N = BN, M = 128
@@ -228,13 +222,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (threadIdx.x == 0) {
         for (int s = 0; s < ST; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 1);
+            mbar_init(&empty[s], NISSUE);
         }
         for (int b = 0; b < 2; ++b) {
-            mbar_init(&accf[b], 1);
+            mbar_init(&accf[b], NISSUE);
             mbar_init(&acce[b], 128);
         }
-        mbar_init(drain, 1);
+        mbar_init(drain, NISSUE);
         *abort_flag = 0;
         fence_mbar_init();
     }
@@ -263,13 +257,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     uint8_t *st = base + s * STAGE;
                     mbar_arrive_expect_tx(&full[s], STAGE);
                     if constexpr (HALO) {
-                        // the halo box of one 32-channel chunk, one plane per 8 channels; all nine taps' weights
+                        // the halo box of one 32-channel chunk and all nine taps' weights
                         const int cc = kb * KC;
                         const CUtensorMap *mx = cc < a.C0 ? &mx0 : &mx1;
                         const int ch = cc < a.C0 ? cc : cc - a.C0;
-#pragma unroll
-                        for (int pl = 0; pl < KC / 8; ++pl)
-                            tma_load_4d(st + pl * HB_PLANE, mx, ch + 8 * pl, c.x0 - 1, c.y0 - 1, c.n, &full[s]);
+                        tma_load_4d(st, mx, ch, c.x0 - 1, c.y0 - 1, c.n, &full[s]);
 #pragma unroll 1
                         for (int tap = 0; tap < 9; ++tap)
                             tma_load_2d(st + A_BYTES + tap * B_TAP, &mw, tap * Cin + cc, c.co0, &full[s]);
@@ -290,7 +282,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         __syncwarp();
     } else if (warp == 1) {
         // ------------------------------------------------------- MMA issuer
-        if (lane == 0) {
+        if (lane < NISSUE) {
             uint32_t g = 0;
             bool ok = true;
             int i = 0;
@@ -306,19 +298,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     tc_fence_after();
                     const uint32_t sa = smem_u32(base + s * STAGE);
                     if constexpr (HALO) {
-#pragma unroll 1
+                        // this lane's MMA block: output row mt = lane of the tile
+                        const int mt = lane;
+                        const uint64_t bd0 = umma_desc(sa + A_BYTES, SBO, LAYOUT);
+                        const uint64_t ad0 = umma_desc(sa + (uint32_t)(mt * HB_W) * (KC * 2), SBO, LAYOUT);
+#pragma unroll
                         for (int tap = 0; tap < 9; ++tap) {
                             const int ky = tap / 3, kx = tap % 3;          // offsets + 1
-                            const uint64_t bd = umma_desc(sa + A_BYTES + tap * B_TAP, SBO, LAYOUT);
+                            // descriptor start fields count 16-byte units
+                            const uint64_t bd = bd0 + (uint64_t)(tap * B_TAP / 16);
+                            const uint64_t ad = ad0 + (uint64_t)((ky * HB_W + kx) * (KC * 2) / 16);
 #pragma unroll
-                            for (int mt = 0; mt < MT; ++mt) {
-                                const uint32_t row0 = (uint32_t)((mt + ky) * HB_W + kx);
-#pragma unroll
-                                for (int j = 0; j < KC / 16; ++j)   // K halves in planes 2j, 2j + 1
-                                    tc_mma(d + mt * BN,
-                                           umma_desc_interleaved(sa + 2 * j * HB_PLANE + row0 * 16, HB_PLANE, 128),
-                                           bd + (uint64_t)(2 * j), IDESC, (kb | tap | j) != 0);
-                            }
+                            for (int j = 0; j < KC / 16; ++j)
+                                tc_mma(d + mt * BN, ad + (uint64_t)(2 * j), bd + (uint64_t)(2 * j), IDESC,
+                                       (kb | tap | j) != 0);
                         }
                     } else {
                         const uint64_t bd = umma_desc(sa + A_BYTES, SBO, LAYOUT);
@@ -335,7 +328,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 if (ok) tc_commit(&accf[buf]);
             }
-            // all MMAs issued by this thread complete before TMEM is released
+            // all MMAs issued by the issuing lanes complete before TMEM is released
             tc_commit(drain);
             mbar_wait_bounded(drain, 0, TC_WAIT_LIMIT);
         }
@@ -489,25 +482,11 @@ bool encode_act(CUtensorMap *m, const void *ptr, int C, int N, int H, int W, int
                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// halo boxes: 8 channels (16 bytes, unswizzled) x HB_W pixels x HB_H rows
-bool encode_act_halo(CUtensorMap *m, const void *ptr, int C, int N, int H, int W)
-{
-    EncodeTiledFn enc = encode_fn();
-    if (!enc) return false;
-    cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
-    cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
-    cuuint32_t box[4] = {8, (cuuint32_t)HB_W, (cuuint32_t)HB_H, 1};
-    cuuint32_t es[4] = {1, 1, 1, 1};
-    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(ptr), dims, strides, box, es,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
 // halo-tile instance: 32 -> 32 channels, two stages of one halo box and nine weight boxes
 int launch_tc_halo(const CUtensorMap &m0, const CUtensorMap &m1, const CUtensorMap &mw, const TcArgs &a,
                    cudaStream_t st)
 {
-    constexpr int STAGE = 4 * HB_PLANE + 9 * 32 * 32 * 2, ST = 2;
+    constexpr int STAGE = HB_ROWS * 32 * 2 + 9 * 32 * 32 * 2, ST = 2;
     static_assert(STAGE % 1024 == 0, "stage alignment");
     constexpr size_t SMEM = (size_t)ST * STAGE + 1024 + 256;
     auto kern = conv3x3_tc_kernel<32, 32, 4, ST, true>;
@@ -603,8 +582,9 @@ int conv3x3_tc(const void *x0, int C0, const void *x1, int C1, const void *w, co
         h.n_yb = (H + 3) / 4;
         h.n_co = 1;
         const long long ht = (long long)N * h.n_yb * h.n_xb;
-        if (ht > 0 && ht <= (1LL << 30) && encode_act_halo(&m0, x0, C0, N, H, W) &&
-            (C1 == 0 || encode_act_halo(&m1, x1, C1, N, H, W)) && encode_w(&mw, w, Cout, C0 + C1, 32, 32)) {
+        if (ht > 0 && ht <= (1LL << 30) && encode_act(&m0, x0, C0, N, H, W, 32, HB_W, HB_H) &&
+            (C1 == 0 || encode_act(&m1, x1, C1, N, H, W, 32, HB_W, HB_H)) &&
+            encode_w(&mw, w, Cout, C0 + C1, 32, 32)) {
             if (C1 == 0) m1 = m0;
             h.tiles = (int)ht;
             return launch_tc_halo(m0, m1, mw, h, st);
