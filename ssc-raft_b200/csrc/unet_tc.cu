@@ -193,7 +193,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     constexpr int A_PART = TC_M * KC * 2;                  // one 128-row MMA operand
     constexpr int B_TAP = BN * KC * 2;                     // one tap's weights
     constexpr int A_BYTES = HALO ? HB_ROWS * KC * 2 : MT * A_PART;
-    constexpr int B_BYTES = HALO ? 9 * B_TAP : B_TAP, STAGE = A_BYTES + B_BYTES;
+    // halo tiles keep every tap's weights resident (loaded once per CTA); the
+    // stages carry the input boxes only
+    constexpr int B_BYTES = HALO ? 0 : B_TAP, STAGE = A_BYTES + B_BYTES;
     constexpr uint32_t SBO = 8 * KC * 2;                   // one 8-row swizzle atom
     constexpr uint32_t LAYOUT = KC == 64 ? 2u : 4u;        // 128-byte / 64-byte swizzle
     constexpr uint32_t ACC = MT * BN;                      // TMEM columns of one accumulator buffer
@@ -210,12 +212,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
     extern __shared__ uint8_t smem_raw[];
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-    uint64_t *full = reinterpret_cast<uint64_t *>(base + ST * STAGE);
+    const int wres_bytes = HALO ? 9 * ((a.C0 + a.C1) / KC) * B_TAP : 0;   // resident weights (halo tiles)
+    uint8_t *wres = base + ST * STAGE;
+    uint64_t *full = reinterpret_cast<uint64_t *>(wres + wres_bytes);
     uint64_t *empty = full + ST;
     uint64_t *accf = empty + ST;
     uint64_t *acce = accf + 2;
     uint64_t *drain = acce + 2;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    uint64_t *wbar = drain + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(wbar + 1);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -229,6 +234,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             mbar_init(&acce[b], 128);
         }
         mbar_init(drain, NISSUE);
+        mbar_init(wbar, 1);
         *abort_flag = 0;
         fence_mbar_init();
     }
@@ -248,6 +254,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (lane == 0) {
             uint32_t g = 0;                      // k-blocks issued so far
             bool ok = true;
+            if constexpr (HALO) {
+                // every chunk's nine taps of weights, once per CTA
+                mbar_arrive_expect_tx(wbar, (uint32_t)wres_bytes);
+#pragma unroll 1
+                for (int ck = 0; ck < Cin / KC; ++ck)
+#pragma unroll 1
+                    for (int tap = 0; tap < 9; ++tap)
+                        tma_load_2d(wres + (ck * 9 + tap) * B_TAP, &mw, tap * Cin + ck * KC, 0, wbar);
+            }
             for (int t = blockIdx.x; t < a.tiles && ok; t += gridDim.x) {
                 const TileCoord c = tile_coord(a, t, BN);
                 for (int kb = 0; kb < kb_per_tile && ok; ++kb, ++g) {
@@ -257,14 +272,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     uint8_t *st = base + s * STAGE;
                     mbar_arrive_expect_tx(&full[s], STAGE);
                     if constexpr (HALO) {
-                        // the halo box of one 32-channel chunk and all nine taps' weights
+                        // the halo box of one 32-channel chunk
                         const int cc = kb * KC;
                         const CUtensorMap *mx = cc < a.C0 ? &mx0 : &mx1;
                         const int ch = cc < a.C0 ? cc : cc - a.C0;
                         tma_load_4d(st, mx, ch, c.x0 - 1, c.y0 - 1, c.n, &full[s]);
-#pragma unroll 1
-                        for (int tap = 0; tap < 9; ++tap)
-                            tma_load_2d(st + A_BYTES + tap * B_TAP, &mw, tap * Cin + cc, c.co0, &full[s]);
                     } else {
                         const int tap = kb / (Cin / KC), cc = (kb % (Cin / KC)) * KC;
                         const int ky = tap / 3 - 1, kx = tap % 3 - 1;
@@ -278,13 +290,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             // stage s was k-block s + ST * ((g - 1 - s) / ST)
             for (uint32_t s = 0; s < (uint32_t)ST && s < g; ++s)
                 mbar_wait_bounded(&full[s], ((g - 1 - s) / ST) & 1, TC_WAIT_LIMIT);
+            if (HALO) mbar_wait_bounded(wbar, 0, TC_WAIT_LIMIT);
         }
         __syncwarp();
     } else if (warp == 1) {
         // ------------------------------------------------------- MMA issuer
         if (lane < NISSUE) {
             uint32_t g = 0;
-            bool ok = true;
+            bool ok = !HALO || tc_wait(wbar, 0, abort_flag, a.err);
             int i = 0;
             for (int t = blockIdx.x; t < a.tiles && ok; t += gridDim.x, ++i) {
                 const int buf = i & 1, v = i >> 1;
@@ -300,7 +313,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     if constexpr (HALO) {
                         // this lane's MMA block: output row mt = lane of the tile
                         const int mt = lane;
-                        const uint64_t bd0 = umma_desc(sa + A_BYTES, SBO, LAYOUT);
+                        const uint64_t bd0 = umma_desc(smem_u32(wres) + (uint32_t)(kb * 9 * B_TAP), SBO, LAYOUT);
                         const uint64_t ad0 = umma_desc(sa + (uint32_t)(mt * HB_W) * (KC * 2), SBO, LAYOUT);
 #pragma unroll
                         for (int tap = 0; tap < 9; ++tap) {
@@ -486,9 +499,9 @@ bool encode_act(CUtensorMap *m, const void *ptr, int C, int N, int H, int W, int
 int launch_tc_halo(const CUtensorMap &m0, const CUtensorMap &m1, const CUtensorMap &mw, const TcArgs &a,
                    cudaStream_t st)
 {
-    constexpr int STAGE = HB_ROWS * 32 * 2 + 9 * 32 * 32 * 2, ST = 2;
+    constexpr int STAGE = HB_ROWS * 32 * 2, ST = 3;
     static_assert(STAGE % 1024 == 0, "stage alignment");
-    constexpr size_t SMEM = (size_t)ST * STAGE + 1024 + 256;
+    const size_t SMEM = (size_t)ST * STAGE + (size_t)9 * ((a.C0 + a.C1) / 32) * 32 * 32 * 2 + 1024 + 256;
     auto kern = conv3x3_tc_kernel<32, 32, 4, ST, true>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM) != cudaSuccess) return 1;
     cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
@@ -573,7 +586,7 @@ int conv3x3_tc(const void *x0, int C0, const void *x1, int C1, const void *w, co
     cudaGetDevice(&dev);
     a.err = tc_err_flag(dev);
     CUtensorMap m0, m1, mw;
-    if (g_halo && Cout == 32 && KC == 32 && W >= TC_M) {
+    if (g_halo && Cout == 32 && KC == 32 && W >= TC_M && C0 + C1 <= 96) {
         // halo tiles: 4 rows x 128 pixels, the taps served from one box per channel chunk
         TcArgs h = a;
         h.BW = TC_M;
