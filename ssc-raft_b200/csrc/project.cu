@@ -92,15 +92,18 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
                     const float y = __fmaf_rn(t, stheta, __fmul_rn(s, ctheta));
                     const int X = (int)((x + 1) / ddx);
                     const int Y = (int)((y + 1) / ddy);
-                    const bool in = (X >= 0) & (X < limx) & (Y >= 0) & (Y < limy);
-                    const size_t off = (size_t)(in ? Y : 0) * sy + (size_t)(in ? X : 0) * sx;
                     if constexpr (IL) {
-                        // one 32-byte load: the pixel's eight slice values (pixel 0 when outside)
+                        // one 32-byte load: the pixel's eight slice values, or
+                        // eight zeros (p.il_zero) for a sample outside the image
+                        const bool in = ((unsigned)X < (unsigned)limx) & ((unsigned)Y < (unsigned)limy);
+                        const unsigned pix = (unsigned)Y * (unsigned)sy + (unsigned)X * (unsigned)sx;
                         float w[8];
-                        ldg_v8(img + off * 8, w);
+                        ldg_v8(in ? img + (size_t)pix * 8 : p.il_zero, w);
 #pragma unroll
-                        for (int q = 0; q < 8; q++) v[u][q] = in ? w[q] : 0.f;
+                        for (int q = 0; q < 8; q++) v[u][q] = w[q];
                     } else {
+                        const bool in = (X >= 0) & (X < limx) & (Y >= 0) & (Y < limy);
+                        const size_t off = (size_t)(in ? Y : 0) * sy + (size_t)(in ? X : 0) * sx;
                         const float *pix = img + off;
 #pragma unroll
                         for (int q = 0; q < S; q++) v[u][q] = (in && q < nsl) ? __ldg(pix + q * plane) : 0.f;
@@ -293,14 +296,16 @@ void launch_transpose(const float *in, float *out, int nx, int ny, int nslices, 
 
 // Slice-interleaved copies of groups of 8 planes, row-major and transposed:
 // il[g][y][x][s] = ilT[g][x][y][s] = in[8g + s][y][x] (zero where 8g + s is
-// past the last plane).  One 32 x 32 pixel tile of all 8 planes per block.
+// past the last plane), plus the eight zeros that samples outside the image
+// read.  One 32 x 32 pixel tile of all 8 planes per block.
 __global__ void __launch_bounds__(256)
-interleave_kernel(const float *__restrict__ in, float *__restrict__ il, float *__restrict__ ilT, int nx, int ny,
-                  int nslices)
+interleave_kernel(const float *__restrict__ in, float *__restrict__ il, float *__restrict__ ilT,
+                  float *__restrict__ zero8, int nx, int ny, int nslices)
 {
     __shared__ float tile[8][32][33];
     const size_t plane = (size_t)nx * ny;
     const int g = blockIdx.z, tx = threadIdx.x;
+    if ((blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.y) == 0 && tx < 8) zero8[tx] = 0.f;
     const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
 #pragma unroll
     for (int s = 0; s < 8; s++) {
@@ -336,7 +341,7 @@ size_t proj_scratch_bytes(int nx, int ny, int nslices)
 {
     const size_t plane = (size_t)nx * ny * sizeof(float);
     if (nslices <= 0) return 16;
-    if (use_interleaved(nslices)) return 2 * (size_t)((nslices + 7) / 8) * 8 * plane;
+    if (use_interleaved(nslices)) return 2 * (size_t)((nslices + 7) / 8) * 8 * plane + 8 * sizeof(float);
     return (size_t)nslices * plane;
 }
 
@@ -347,18 +352,20 @@ void stage_proj_images(ProjLaunch &pl, void *scratch, cudaStream_t st)
         const int G = (pl.nslices + 7) / 8;
         float *il = (float *)scratch;
         float *ilT = il + (size_t)G * 8 * pl.nx * pl.ny;
+        float *zero8 = ilT + (size_t)G * 8 * pl.nx * pl.ny;
         count_launch();
         dim3 grid((pl.nx + 31) / 32, (pl.ny + 31) / 32, G);
-        interleave_kernel<<<grid, dim3(32, 8), 0, st>>>(pl.img, il, ilT, pl.nx, pl.ny, pl.nslices);
+        interleave_kernel<<<grid, dim3(32, 8), 0, st>>>(pl.img, il, ilT, zero8, pl.nx, pl.ny, pl.nslices);
         RAFT_CUDA(cudaGetLastError());
         pl.il = il;
         pl.ilT = ilT;
+        pl.il_zero = zero8;
         pl.imgT = nullptr;
     } else {
         float *t = (float *)scratch;
         launch_transpose(pl.img, t, pl.nx, pl.ny, pl.nslices, st);
         pl.imgT = t;
-        pl.il = pl.ilT = nullptr;
+        pl.il = pl.ilT = pl.il_zero = nullptr;
     }
 }
 
@@ -379,7 +386,8 @@ static void launch_project_s(const ProjLaunch &pl, int S, cudaStream_t st)
 void launch_project(const ProjLaunch &pl, cudaStream_t st)
 {
     if (pl.nslices <= 0 || pl.nangles <= 0 || pl.nrays <= 0) return;
-    RAFT_CHECK((pl.il == nullptr) == (pl.ilT == nullptr), "projector: interleaved copies come in pairs");
+    RAFT_CHECK((pl.il == nullptr) == (pl.ilT == nullptr) && (pl.il == nullptr) == (pl.il_zero == nullptr),
+               "projector: interleaved copies come with their transposed copy and zero pixel");
     const int S = pl.il ? 8 : (pl.nslices >= 4 ? 4 : (pl.nslices >= 2 ? 2 : 1));
     if (!pl.em) {
         launch_project_s<0, 0>(pl, S, st);

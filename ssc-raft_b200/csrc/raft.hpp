@@ -195,6 +195,7 @@ struct ProjLaunch {
     const float *imgT = nullptr;    // optional transposed copy [nslices][nx][ny] for steep angles
     const float *il = nullptr;      // optional slice-interleaved copies (groups of 8 planes):
     const float *ilT = nullptr;     //   il [G][ny][nx][8], ilT [G][nx][ny][8]; used instead of img/imgT
+    const float *il_zero = nullptr; //   with 8 zero floats (32-byte aligned) that outside samples read
     float *out = nullptr;           // plain [nslices][nangles][nrays] or window rows
     const float *angles = nullptr;
     int nx = 0, ny = 0, nrays = 0, nangles = 0, nslices = 0;
