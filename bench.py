@@ -181,6 +181,62 @@ def run_tem(local, dev, nslices=EM_SLICES, iters=EM_ITERS, warm_iters=3):
             "metrics": "FP64 data residual ||flat*exp(-Ax)-y||/||y|| and Poisson NLL per iteration"}
 
 
+def run_radon(dev, sm_mhz, nslices=EM_SLICES, reps=5, warm=3):
+    """Radon transform (the ray-driven Radon_RT projector of getRadonRTMultiGPU)
+    of nslices seeded random 1024^2 images at 900 angles x 1024 bins.
+    Device-resident through raft_radon_device (slice-interleaved re-layout +
+    projector; median of reps CUDA-event timings) and end to end through
+    getRadonRTMultiGPU with pinned host buffers.  Roofline: one sample-update
+    moves 4 B through the L1/shared-memory data pipe (a 32-byte sector serves
+    8 slices) and costs one FP32 add -- the gather roofline of the
+    backprojector."""
+    import torch
+    from sscRaft.rafttypes import libraft, check_error, _ptr
+    N, A = EM_N, EM_A
+    g = torch.Generator(device=dev).manual_seed(4242)
+    img = torch.rand((nslices, N, N), generator=g, device=dev)
+    out = torch.empty((nslices, A, N), device=dev)
+    ang = np.ascontiguousarray(np.linspace(0.0, np.pi, A, endpoint=False).astype(np.float32))
+    st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    times = []
+    for r in range(warm + reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rc = libraft.raft_radon_device(dev.index or 0, p(out), p(img), _ptr(ang), N, N, N, A, nslices, 1.0, 1.0, st)
+        e1.record()
+        if rc:
+            check_error("raft_radon_device")
+        torch.cuda.synchronize(dev)
+        if r >= warm:
+            times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times)
+    upd = float(nslices) * A * N * N
+    gups = upd / (ms / 1e3) / 1e9
+    peak = gather_peak_gups(4, 1, sm_mhz)
+    h_img = torch.empty((nslices, N, N), dtype=torch.float32, pin_memory=True)
+    h_img.copy_(img)
+    h_out = torch.empty((nslices, A, N), dtype=torch.float32, pin_memory=True)
+    hi, ho = h_img.numpy(), h_out.numpy()
+    gl = np.array([dev.index or 0], np.intc)
+    e2e = []
+    for r in range(3):
+        t0 = time.perf_counter()
+        libraft.getRadonRTMultiGPU(_ptr(gl), 1, _ptr(ho), _ptr(hi), _ptr(ang), N, N, N, A, nslices, 1.0, 1.0)
+        e2e.append(time.perf_counter() - t0)
+        check_error("getRadonRTMultiGPU")
+    spot = float((torch.from_numpy(ho[nslices // 2]).to(dev) - out[nslices // 2]).abs().max())
+    ms_e2e = 1e3 * statistics.median(e2e)
+    return {"workload": f"Radon transform {nslices} x {N}^2 -> {A} angles x {N} bins, uniform random images",
+            "ms_per_step": ms, "slices_per_s": nslices / (ms / 1e3), "gups": gups,
+            "gather_roofline": {"achieved_gups": gups, "peak_gups": peak, "frac": gups / peak,
+                                "bytes_per_update": 4, "fp32_ops_per_update": 1, "sm_mhz": sm_mhz},
+            "e2e": {"slices_per_s": nslices / (ms_e2e / 1e3), "ms_per_step": ms_e2e,
+                    "api": "getRadonRTMultiGPU, pinned host buffers",
+                    "h2d_bytes_per_step": nslices * N * N * 4, "d2h_bytes_per_step": nslices * A * N * 4,
+                    "max_abs_diff_vs_device_path": spot}}
+
+
 # ---------------------------------------------------------------- tEMFQ --
 TEMFQ_ZPAD, TEMFQ_ITERS = 2, 10
 
@@ -626,6 +682,11 @@ def run_ours(args):
         if rank == 0:
             print(json.dumps({"quick": True, "op": "temfq", **r}), flush=True)
         return
+    if args.quick and args.op == "radon":
+        r = run_radon(dev, sm_max, nslices=args.slices, reps=max(1, args.steps), warm=max(1, args.warmup))
+        if rank == 0:
+            print(json.dumps({"quick": True, "op": "radon", **r}), flush=True)
+        return
     if args.quick and args.op == "tem":
         # profiling mode: a short tEM run (args.slices x 1024^2, 900 angles)
         r = run_tem(local, dev, nslices=args.slices, iters=args.steps, warm_iters=args.warmup)
@@ -694,6 +755,7 @@ def run_ours(args):
         variants[name].update({"bp_gups": vg, "gather_roofline": {"achieved_gups": vg, "peak_gups": pk,
                                                                    "frac": vg / pk}})
 
+    radon_result = None if args.no_radon else run_radon(dev, sm_mhz)
     em_result = None if args.no_em else run_tem(local, dev)
     ragged_result = None if args.no_ragged else run_ragged(dev)
     warm_result = None if args.no_warm else run_warm(dev)
@@ -740,6 +802,7 @@ def run_ours(args):
                           "launches_per_step": {"filter": f_n, "bp": bp_n}},
             "variants": variants,
             "autotune": autotune_table(),
+            "radon": radon_result,
             "em": em_result,
             "ragged": ragged_result,
             "warm_start": warm_result,
@@ -856,6 +919,7 @@ def main():
     ap.add_argument("--slices", type=int, default=N_SLICES)
     ap.add_argument("--ref-slices", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-radon", action="store_true")
     ap.add_argument("--no-em", action="store_true")
     ap.add_argument("--no-ragged", action="store_true")
     ap.add_argument("--no-warm", action="store_true")
@@ -864,7 +928,7 @@ def main():
     ap.add_argument("--ref-op", default="fbp", choices=["fbp", "temfq"],
                     help="reference arm: the headline FBP, or tEMFQ on the tEM workload (comparison only)")
     ap.add_argument("--quick", action="store_true", help="device timing of one operator only (profiling)")
-    ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "tem", "ragged", "flat_dark", "bst",
+    ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "radon", "tem", "ragged", "flat_dark", "bst",
                                                         "temfq", "unet", "warm"])
     args = ap.parse_args()
     if args.impl == "reference":
