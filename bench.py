@@ -237,6 +237,92 @@ def run_radon(dev, sm_mhz, nslices=EM_SLICES, reps=5, warm=3):
                     "max_abs_diff_vs_device_path": spot}}
 
 
+def run_aux(dev, sino, reps=3):
+    """Timings of the remaining drop-in operators through their Python entry
+    points with pinned host arrays, on the FBP workload's shapes: lowpass
+    (getFilterLowPassMultiGPU: Hann, padding 2, in place) and the sub-pixel
+    rotation-axis correction (getRotAxisCorrectionMultiGPU, 1.5 rays) of 64 x
+    1800 x 2048 sinograms (host -> device -> host inside the timed call), and
+    the rotation-axis search (findcentersino, findcentersino_subpixel) on one
+    2048 x 2048 frame pair of a smooth object mirrored about ray 1061 --
+    through the host entries and on device frames (raft_centersino_device)."""
+    import torch
+    import sscRaft
+    from sscRaft.processing import Centersino, Centersino_subpixel, correct_rotation_axis
+    from sscRaft.rafttypes import libraft, check_error
+    gpu = dev.index or 0
+    n = min(64, sino.shape[0])
+    A, N = sino.shape[1], sino.shape[2]
+    h_base = torch.empty((n, A, N), dtype=torch.float32, pin_memory=True)
+    h_base.copy_(sino[:n])
+    h_work = torch.empty_like(h_base).pin_memory()
+    base, work = h_base.numpy(), h_work.numpy()
+
+    def timed(fn):
+        ts = []
+        for r in range(reps + 1):
+            np.copyto(work, base)
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+        return 1e3 * statistics.median(ts[1:])
+
+    ms_lp = timed(lambda: sscRaft.lowpass(work, dic={"gpu": [gpu], "filter": "hann", "padding": 2}))
+    ms_ax = timed(lambda: correct_rotation_axis(work, 1.5, gpus=[gpu]))
+    io = {"h2d_bytes_per_step": n * A * N * 4, "d2h_bytes_per_step": n * A * N * 4}
+
+    sx = sy = 2048
+    axis = sx // 2 + 37
+    rng = np.random.default_rng(2024)
+    x = np.arange(sx, dtype=np.float64)
+    p0 = np.zeros((sy, sx))
+    for _ in range(6):
+        c, w, a = rng.uniform(0.3, 0.7) * sx, rng.uniform(8, 40), rng.uniform(0.2, 1.0)
+        p0 += a * rng.uniform(0.5, 1.5, sy)[:, None] * np.exp(-((x[None, :] - c) ** 2) / (2 * w * w))
+    src = (2 * axis - np.arange(sx))
+    ok = (src >= 0) & (src < sx)
+    p180 = np.zeros_like(p0)
+    p180[:, ok] = p0[:, src[ok]]
+    dark = np.full((sy, sx), 100.0, np.float32)
+    flat = dark + 1e4
+    f0 = (dark + 1e4 * np.exp(-p0)).astype(np.float32)
+    f1 = (dark + 1e4 * np.exp(-p180)).astype(np.float32)
+    ts, tsp = [], []
+    for r in range(reps + 1):
+        t0 = time.perf_counter()
+        off = Centersino(f0, f1, flat, dark)
+        t1 = time.perf_counter()
+        off_sp = Centersino_subpixel(f0, f1, flat, dark)
+        t2 = time.perf_counter()
+        if r:
+            ts.append(t1 - t0)
+            tsp.append(t2 - t1)
+    d = [torch.from_numpy(a).to(dev) for a in (f0, f1, dark, flat)]
+    res = ctypes.c_double(0)
+    st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    td = []
+    for r in range(reps + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        rc = libraft.raft_centersino_device(gpu, *[ctypes.c_void_p(t.data_ptr()) for t in d], sx, sy, 0,
+                                            ctypes.byref(res), st)
+        if rc:
+            check_error("raft_centersino_device")
+        if r:
+            td.append(time.perf_counter() - t0)
+    return {"lowpass": {"workload": f"{n} x {A} x {N} sinograms, Hann, padding 2, in place", "ms": ms_lp,
+                        "slices_per_s": n / (ms_lp / 1e3), "api": "sscRaft.lowpass -> getFilterLowPassMultiGPU",
+                        **io},
+            "axis_correction": {"workload": f"{n} x {A} x {N} sinograms shifted by 1.5 rays, in place", "ms": ms_ax,
+                                "slices_per_s": n / (ms_ax / 1e3),
+                                "api": "correct_rotation_axis -> getRotAxisCorrectionMultiGPU", **io},
+            "centersino": {"workload": f"one {sx} x {sy} frame pair mirrored about ray {axis}",
+                           "ms_host": 1e3 * statistics.median(ts), "ms_host_subpixel": 1e3 * statistics.median(tsp),
+                           "ms_device_frames": 1e3 * statistics.median(td), "offset": int(off),
+                           "offset_subpixel": float(off_sp), "offset_device": float(res.value),
+                           "api": "Centersino / Centersino_subpixel (findcentersino*), raft_centersino_device"}}
+
+
 # ---------------------------------------------------------------- tEMFQ --
 TEMFQ_ZPAD, TEMFQ_ITERS = 2, 10
 
@@ -682,6 +768,11 @@ def run_ours(args):
         if rank == 0:
             print(json.dumps({"quick": True, "op": "temfq", **r}), flush=True)
         return
+    if args.quick and args.op == "aux":
+        r = run_aux(dev, sino, reps=max(1, args.steps))
+        if rank == 0:
+            print(json.dumps({"quick": True, "op": "aux", **r}), flush=True)
+        return
     if args.quick and args.op == "radon":
         r = run_radon(dev, sm_max, nslices=args.slices, reps=max(1, args.steps), warm=max(1, args.warmup))
         if rank == 0:
@@ -761,6 +852,7 @@ def run_ours(args):
     warm_result = None if args.no_warm else run_warm(dev)
     flat_dark_result = None if args.no_flat_dark else run_flat_dark(dev, sino, hbm_peak=hbm_peak)
     temfq_result = None if args.no_temfq else run_temfq(dev)
+    aux_result = None if args.no_aux else run_aux(dev, sino)
 
     if rank == 0:
         value = ws * nsl / (ms_dev / 1e3)
@@ -808,6 +900,7 @@ def run_ours(args):
             "warm_start": warm_result,
             "flat_dark": flat_dark_result,
             "temfq": temfq_result,
+            "aux": aux_result,
             "clocks": clocks,
             "gpu_launches": int(launches),
         }
@@ -925,10 +1018,11 @@ def main():
     ap.add_argument("--no-warm", action="store_true")
     ap.add_argument("--no-flat-dark", action="store_true")
     ap.add_argument("--no-temfq", action="store_true")
+    ap.add_argument("--no-aux", action="store_true")
     ap.add_argument("--ref-op", default="fbp", choices=["fbp", "temfq"],
                     help="reference arm: the headline FBP, or tEMFQ on the tEM workload (comparison only)")
     ap.add_argument("--quick", action="store_true", help="device timing of one operator only (profiling)")
-    ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "radon", "tem", "ragged", "flat_dark", "bst",
+    ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "radon", "aux", "tem", "ragged", "flat_dark", "bst",
                                                         "temfq", "unet", "warm"])
     args = ap.parse_args()
     if args.impl == "reference":
