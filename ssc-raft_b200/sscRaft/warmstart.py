@@ -5,8 +5,9 @@ FBP reconstruction to an image that tEM starts from, instead of the uniform
 start the reference uses (em_methods.py:117-122).  The network runs on the
 library's own tensor-core kernels (raft_unet_* in libraft.so) for inference
 and training; PyTorch only provides device memory and streams.  Plain EM
-from a uniform start remains the fallback and the judge: the figure of merit
-is the time tEM needs to reach the data residual of plain 100-iteration EM.
+from a uniform start remains the fallback and sets the bar: the figure of
+merit is the time tEM needs to reach the data residual of plain 100-iteration
+EM.
 
 Everything here works on device tensors (torch CUDA).  Geometry: images on
 the EM grid (em_RT_kernel.cu:97-99); the FBP input is flipped in y and scaled
