@@ -349,6 +349,8 @@ void stage_proj_images(ProjLaunch &pl, void *scratch, cudaStream_t st)
 {
     if (pl.nslices <= 0) return;
     if (use_interleaved(pl.nslices)) {
+        // the projector indexes a pixel of the interleaved copies in 32 bits
+        RAFT_CHECK((size_t)pl.nx * pl.ny <= 0xffffffffull, "projector: image plane above 2^32 pixels");
         const int G = (pl.nslices + 7) / 8;
         float *il = (float *)scratch;
         float *ilT = il + (size_t)G * 8 * pl.nx * pl.ny;
