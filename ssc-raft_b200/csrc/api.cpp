@@ -9,6 +9,7 @@
 #include "engine.hpp"
 
 #include <cmath>
+#include <initializer_list>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -50,8 +51,6 @@ static bool parse_fbp_arrays(const float *paramf, const int *parami, FbpConfig &
     c.pixel_y = paramf[5];
     c.offset = paramf[6];
     // parameters.cu:201-203 (float arithmetic; plank*vc in double as there)
-    const float plank = 4.135667696E-15f;
-    (void)plank;
     float wavelength = (c.beta_delta == 0.0f) ? 1.0f : (float)((4.135667696E-15 * 299792458) / c.energy);
     c.paganin = wavelength * c.z2 * float(M_PI) * c.beta_delta / (c.pixel_x * c.pixel_x);
     if (c.nrays < 2 || c.nangles < 1 || c.nslices < 0 || c.pad < 0 || c.pad > 64) {
@@ -117,6 +116,31 @@ static bool check_gpus(const int *gpus, int ngpus)
             return false;
         }
     return true;
+}
+
+// Data pointers of a call with work to do must not be null (an empty batch
+// may pass null).
+static bool ptrs_ok(int nslices, std::initializer_list<const void *> ptrs, const char *name)
+{
+    if (nslices <= 0) return true;
+    for (const void *p : ptrs)
+        if (!p) {
+            set_error(std::string(name) + ": null data pointer");
+            return false;
+        }
+    return true;
+}
+
+// Operator / sinogram storage pairs of the FBP entry points: 0/0 (nearest,
+// reference), 1/1 (linear, FP32 pairs), 1/2 (linear, BF16 pairs).
+static bool fbp_mode_ok(int geometry, int store, const char *name)
+{
+    const bool ok = (geometry == GEOM_FBP_REF && store == STORE_F32) ||
+                    (geometry == GEOM_FBP_LIN && (store == STORE_PAIR_F32 || store == STORE_PAIR_BF16));
+    if (!ok)
+        set_error(std::string(name) + ": geometry/store must be 0/0 (nearest), 1/1 (linear fp32) or 1/2 "
+                                      "(linear bf16)");
+    return ok;
 }
 
 // Contiguous z-slabs of ceil(nslices/ngpus) slices, the last ones shorter or
@@ -324,6 +348,8 @@ int raft_fbp_device(int gpu, float *d_obj, const float *d_tomogram, const float 
     clear_error();
     FbpConfig cfg;
     if (!parse_fbp_arrays(paramf, parami, cfg, true)) return 1;
+    if (!fbp_mode_ok(geometry, store, "raft_fbp_device")) return 1;
+    if (!ptrs_ok(cfg.nslices, {d_obj, d_tomogram, angles}, "raft_fbp_device")) return 1;
     if (!check_gpus(&gpu, 1)) return 1;
     cfg.geometry = geometry;
     cfg.store = store;
@@ -400,6 +426,7 @@ int raft_background_device(int gpu, float *d_frames, const float *d_flat, const 
 {
     clear_error();
     if (!check_background(nrays, nangles, nslices, numflats, is_log)) return 1;
+    if (!ptrs_ok(nslices, {d_frames, d_flat, d_dark}, "raft_background_device")) return 1;
     if (!check_gpus(&gpu, 1)) return 1;
     try {
         DeviceState &ds = device_state(gpu);
@@ -478,11 +505,12 @@ int raft_em_ext(int kind, int gpu, float *obj, const float *data, const float *f
     int parami[10] = {nrays, nangles, nslices, nrays, 0, 0, 0, 1, niter, 0};
     EmConfig cfg;
     if (!parse_em_arrays(nullptr, parami, cfg)) return 1;
-    if (!check_gpus(&gpu, 1)) return 1;
     if (kind != 0 && kind != 1) {
         set_error("raft_em_ext: kind must be 0 (tEM) or 1 (eEM)");
         return 1;
     }
+    if (!ptrs_ok(nslices, {obj, data, angles, kind == 0 ? flat : obj}, "raft_em_ext")) return 1;
+    if (!check_gpus(&gpu, 1)) return 1;
     try {
         DeviceState &ds = device_state(gpu);
         std::lock_guard<std::mutex> lk(ds.mtx);
@@ -519,6 +547,11 @@ int raft_em_device(int kind, int gpu, float *d_obj, const float *d_data, const f
     int parami[10] = {nrays, nangles, nslices, nrays, 0, 0, 0, 1, niter, 0};
     EmConfig cfg;
     if (!parse_em_arrays(nullptr, parami, cfg)) return 1;
+    if (kind != 0 && kind != 1) {
+        set_error("raft_em_device: kind must be 0 (tEM) or 1 (eEM)");
+        return 1;
+    }
+    if (!ptrs_ok(nslices, {d_obj, d_data, angles, kind == 0 ? d_flat : d_obj}, "raft_em_device")) return 1;
     if (!check_gpus(&gpu, 1)) return 1;
     try {
         DeviceState &ds = device_state(gpu);
@@ -608,6 +641,7 @@ int raft_radon_device(int gpu, float *d_out, const float *d_phantom, const float
         set_error("invalid Radon sizes");
         return 1;
     }
+    if (!ptrs_ok(nslices, {d_out, d_phantom, angles}, "raft_radon_device")) return 1;
     if (!check_gpus(&gpu, 1)) return 1;
     try {
         DeviceState &ds = device_state(gpu);
@@ -667,6 +701,7 @@ int raft_centersino_device(int gpu, const float *d_frame0, const float *d_frame1
         set_error("raft_centersino_device: null result or unsupported frame size");
         return 1;
     }
+    if (!ptrs_ok(1, {d_frame0, d_frame180, d_dark, d_flat}, "raft_centersino_device")) return 1;
     if (!check_gpus(&gpu, 1)) return 1;
     try {
         DeviceState &ds = device_state(gpu);
@@ -769,6 +804,7 @@ int raft_bst_device(int gpu, float *d_obj, const float *d_tomogram, const float 
     clear_error();
     FbpConfig cfg;
     if (!parse_bst(paramf, parami, cfg)) return 1;
+    if (!ptrs_ok(cfg.nslices, {d_obj, d_tomogram}, "raft_bst_device")) return 1;
     if (!check_gpus(&gpu, 1)) return 1;
     try {
         DeviceState &ds = device_state(gpu);
@@ -841,6 +877,7 @@ int raft_temfq_device(int gpu, float *d_obj, const float *d_counts, const float 
     clear_error();
     TemfqConfig cfg;
     if (!parse_temfq(paramf, parami, cfg)) return 1;
+    if (!ptrs_ok(cfg.nslices, {d_obj, d_counts, d_flat, angles}, "raft_temfq_device")) return 1;
     if (!check_gpus(&gpu, 1)) return 1;
     try {
         DeviceState &ds = device_state(gpu);

@@ -76,3 +76,51 @@ def test_invalid_parameters_are_reported():
     pf[4] = 1.0
     assert libraft.raft_plan_window(_ptr(pf), _ptr(pi), 0, 0, _ptr(out)) == 0
     assert libraft.raft_last_error(buf, 256) == 0
+
+
+def test_device_entries_validate_arguments_before_any_gpu_call():
+    """The device-pointer entry points refuse a bad operator/storage pair, a
+    bad EM kind and null data pointers (when there are slices) with an error
+    status and message -- checked before any device is touched, so this runs
+    without a GPU.  An empty batch may pass null pointers."""
+    import sscRaft  # noqa: F401  (binds the argtypes)
+    from sscRaft.processing.alignments import rotationaxis  # noqa: F401
+    from sscRaft.rafttypes import libraft, _ptr
+    buf = ctypes.create_string_buffer(512)
+
+    def err(rc):
+        assert rc == 1
+        assert libraft.raft_last_error(buf, 512) == 1
+        return buf.value.decode()
+
+    N, A, n = 64, 30, 2
+    ang = np.linspace(0, np.pi, A, endpoint=False).astype(np.float32)
+    pf = np.array([0, 0, 1, 0, 1, 1, 0], np.float32)
+    pi = np.array([N, A, n, N, 2, 0, 0, 7, 0, 0], np.int32)
+    fake = ctypes.c_void_p(16)          # never dereferenced: the calls stop before any device work
+    for g, s in ((0, 1), (1, 0), (2, 0), (1, 3)):
+        assert "geometry/store" in err(libraft.raft_fbp_device(0, fake, fake, _ptr(ang), _ptr(pf), _ptr(pi),
+                                                               g, s, None))
+    assert "null data pointer" in err(libraft.raft_fbp_device(0, None, fake, _ptr(ang), _ptr(pf), _ptr(pi),
+                                                              0, 0, None))
+    assert "kind" in err(libraft.raft_em_device(2, 0, fake, fake, fake, _ptr(ang), N, A, n, 1, None, 1, None))
+    assert "null data pointer" in err(libraft.raft_em_device(0, 0, fake, fake, None, _ptr(ang), N, A, n, 1,
+                                                             None, 1, None))
+    assert "null data pointer" in err(libraft.raft_radon_device(0, fake, None, _ptr(ang), N, N, N, A, n, 1.0, 1.0,
+                                                                None))
+    assert "null data pointer" in err(libraft.raft_background_device(0, fake, None, fake, N, A, n, 1, 1, None))
+    pb = np.array([N, A, n, N, 2, 0, 0, 7, 0, 0], np.int32)
+    assert "null data pointer" in err(libraft.raft_bst_device(0, None, fake, _ptr(pf), _ptr(pb), None))
+    pq = np.array([N, A, n, N, 1, 0, 0, 1, 2, 0, 0], np.int32)
+    pqf = np.array([0.0, 0.0, 0.0], np.float32)
+    assert "null data pointer" in err(libraft.raft_temfq_device(0, fake, fake, None, _ptr(ang), _ptr(pqf), _ptr(pq),
+                                                                None))
+    res = ctypes.c_double(0)
+    assert "null data pointer" in err(libraft.raft_centersino_device(0, None, fake, fake, fake, 64, 64, 0,
+                                                                     ctypes.byref(res), None))
+    # an empty batch with null pointers passes the argument checks (it then
+    # needs a device: without one the call reports that instead)
+    pi[2] = 0
+    if libraft.raft_fbp_device(0, None, None, _ptr(ang), _ptr(pf), _ptr(pi), 0, 0, None):
+        libraft.raft_last_error(buf, 512)
+        assert "null data pointer" not in buf.value.decode()
