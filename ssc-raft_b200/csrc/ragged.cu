@@ -72,7 +72,7 @@ extern "C" int raft_ragged_device(int gpu, const raft_request *reqs, int nreq, i
             set_error("raft_ragged_device: request " + std::to_string(i) + " is invalid");
             return 1;
         }
-        if (q.kind == 0 && (q.pad < 0 || q.filter < 0 || q.filter > 9 || !(q.pixel > 0.f))) {
+        if (q.kind == 0 && (q.pad < 0 || q.pad > 64 || q.filter < 0 || q.filter > 9 || !(q.pixel > 0.f))) {
             set_error("raft_ragged_device: FBP request " + std::to_string(i) + " has invalid parameters");
             return 1;
         }
