@@ -42,6 +42,17 @@ I0 = 1.0e4
 BP_TRAFFIC_PER_LAUNCH = 783_763_456 + 518_802_944
 WORKLOAD = ("batched FBP: 512 slices x 2048^2, 1800 angles over [0,pi), 2048 bins, "
             "axis offset +3.5 px, Hann, padding 2")
+METRIC = "FBP slices/s at 2048^2 x 1800 angles"
+DATA = ("synthetic: 50 seeded random ellipses per slice, exact projections, Poisson I0=1e4, "
+        "-log transmission (no public dataset exists for this path)")
+
+
+def bench_config(ws):
+    """The `config` of both arms' lines (identical: the same workload; each
+    line's `slices_per_step` says how many of its slices one step covers)."""
+    return {"workload": WORKLOAD, "operator": "nearest-sample FBP (the reference's index rule), FP32",
+            "parallelism": f"slab x{ws}, no collective",
+            "l2": "inputs 7.5 GB/GPU > 126 MB L2: no flush needed"}
 
 
 def log(*a):
@@ -73,10 +84,25 @@ def slice_seed_base(rank, nslices):
 
 
 # ------------------------------------------------------------------ data --
+def synthetic_module():
+    """sscRaft/synthetic.py (numpy only) loaded by its file path, so that
+    making inputs does not import the sscRaft package and load its library
+    (the reference arm must map no library of this repository)."""
+    import importlib.util
+    name = "raft_bench_synthetic"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(
+            name, os.path.join(REPO, "ssc-raft_b200", "sscRaft", "synthetic.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        sys.modules[name] = mod
+    return sys.modules[name]
+
+
 def make_sinograms_gpu(nslices, seed_base, device):
     """Exact ellipse projections (50 ellipses/slice) + Poisson noise, on the GPU."""
     import torch
-    from sscRaft import synthetic as S
+    S = synthetic_module()
     ang = S.uniform_angles(N_ANGLES)
     th = torch.as_tensor(ang.astype(np.float64), device=device)[None, :, None]
     R = N_RAYS / 2.0
@@ -110,17 +136,25 @@ def fbp_params(nslices, blocksize=0):
 EM_N, EM_A, EM_SLICES, EM_ITERS, EM_I0 = 1024, 900, 64, 100, 1.0e4
 
 
-def make_tem_data(nslices, seed_base, device, N=EM_N, A=EM_A, I0=EM_I0, n_ell=20):
+def make_tem_data(nslices, seed_base, device, N=EM_N, A=EM_A, I0=EM_I0, n_ell=20, radon_lib=None):
     """Transmission data: ellipse phantoms with attenuation U[0,0.02] per pixel,
     projected with the library's own ray-tracing Radon transform (same geometry
     as the EM forward operator when nrays = N), each slice scaled so that its
     largest line integral is 3 (transmission >= 5%; unscaled 1024-pixel paths
     reach ~20 and starve the detector at I0 = 1e4), Poisson counts at flat I0,
     returned as transmission max(counts,1)/I0 (what tEM consumes after the
-    wrapper's exp(-x)) together with the phantom in EM units."""
+    wrapper's exp(-x)) together with the phantom in EM units.  `radon_lib`:
+    another library with the same getRadonRTMultiGPU export (the reference
+    arm passes the reference's) instead of this package's."""
     import torch
-    from sscRaft import synthetic as S
-    from sscRaft.rafttypes import libraft, check_error, _ptr
+    S = synthetic_module()
+    if radon_lib is None:
+        from sscRaft.rafttypes import libraft, check_error
+    else:
+        libraft, check_error = radon_lib, (lambda what: None)
+
+    def _ptr(a):
+        return a.ctypes.data_as(ctypes.c_void_p)
     ang = S.uniform_angles(A)
     imgs = torch.stack([S.phantom_image(S.ellipse_params(seed_base + k, n_ell, intensity=(0.0, 0.02)), N,
                                         xp=torch, device=device) for k in range(nslices)]).cpu().numpy()
@@ -323,17 +357,52 @@ def run_aux(dev, sino, reps=3):
                            "api": "Centersino / Centersino_subpixel (findcentersino*), raft_centersino_device"}}
 
 
+def run_fbp_noalloc(dev, sino, ang, nslices=32, reps=3):
+    """The headline FBP of `nslices` slices through raft_fbp_device_noalloc
+    (working memory from the library's fixed device array, planar
+    backprojector) and through raft_fbp_device (grow-only workspaces,
+    slice-interleaved backprojector) on the same device-resident sinograms:
+    device time per call and the largest difference of the two images."""
+    import torch
+    from sscRaft.rafttypes import libraft, check_error, _ptr
+    src = sino[:nslices]
+    pf, pi = fbp_params(nslices)
+    angp = np.ascontiguousarray(ang)
+    st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    outs, ms = {}, {}
+    for name in ("raft_fbp_device_noalloc", "raft_fbp_device"):
+        fn = getattr(libraft, name)
+        out = torch.empty((nslices, N_RAYS, N_RAYS), dtype=torch.float32, device=dev)
+        ts = []
+        for r in range(reps + 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            rc = fn(dev.index or 0, ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(src.data_ptr()), _ptr(angp),
+                    _ptr(pf), _ptr(pi), 0, 0, st)
+            e1.record()
+            if rc:
+                check_error(name)
+            torch.cuda.synchronize(dev)
+            if r:
+                ts.append(e0.elapsed_time(e1))
+        ms[name] = statistics.median(ts)
+        outs[name] = out
+    return {"workload": f"{nslices} slices of the headline FBP workload, device-resident",
+            "ms": ms, "slices_per_s": {k: nslices / (v / 1e3) for k, v in ms.items()},
+            "max_abs_diff": float((outs["raft_fbp_device_noalloc"] - outs["raft_fbp_device"]).abs().max())}
+
+
 # ---------------------------------------------------------------- tEMFQ --
 TEMFQ_ZPAD, TEMFQ_ITERS = 2, 10
 
 
-def temfq_inputs(nslices, dev):
+def temfq_inputs(nslices, dev, radon_lib=None):
     """tEMFQ inputs on the tEM workload (nslices x 1024^2, 900 angles over
     [0, pi), flat I0 = 1e4): counts, flat, a uniform start at the phantoms'
     mean attenuation, and the pixel size 2/(N-1) that puts the Fourier-slice
     projection in the units of the tEM data."""
     import torch
-    trans, ang, x_true = make_tem_data(nslices, 3_000_000, dev)
+    trans, ang, x_true = make_tem_data(nslices, 3_000_000, dev, radon_lib=radon_lib)
     counts = (trans * EM_I0).contiguous()
     flat = torch.full((nslices, EM_N), EM_I0, dtype=torch.float32, device=dev)
     x0 = float(np.mean(x_true))
@@ -853,12 +922,14 @@ def run_ours(args):
     flat_dark_result = None if args.no_flat_dark else run_flat_dark(dev, sino, hbm_peak=hbm_peak)
     temfq_result = None if args.no_temfq else run_temfq(dev)
     aux_result = None if args.no_aux else run_aux(dev, sino)
+    if aux_result is not None:
+        aux_result["fbp_noalloc"] = run_fbp_noalloc(dev, sino, ang)
 
     if rank == 0:
         value = ws * nsl / (ms_dev / 1e3)
         updates_step = nsl * N_RAYS * N_RAYS * N_ANGLES
         result = {
-            "metric": "FBP slices/s at 2048^2 x 1800 angles",
+            "metric": METRIC,
             "value": value,
             "unit": "slices/s",
             "n_gpus": ws,
@@ -869,25 +940,29 @@ def run_ours(args):
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f32",
-            "data": "synthetic: 50 seeded random ellipses per slice, exact projections, Poisson I0=1e4, "
-                    "-log transmission (no public dataset exists for this path)",
-            "config": {"workload": WORKLOAD, "operator": "nearest-sample (reference rule), FP32",
-                       "slices_per_gpu": nsl, "parallelism": f"slab x{ws}, no collective",
-                       "l2": "inputs 7.5 GB/GPU > 126 MB L2: no flush needed"},
+            "data": DATA,
+            "config": bench_config(ws),
+            "slices_per_step": nsl,
             "gups": ws * updates_step / (ms_dev / 1e3) / 1e9,
             "e2e": {"value": ws * nsl / (ms_e2e / 1e3), "unit": "slices/s", "ms_per_step": ms_e2e,
                     "api": "sscRaft.fbp -> getFBPMultiGPU, pinned host buffers",
                     "h2d_bytes_per_step": nsl * N_ANGLES * N_RAYS * 4,
                     "d2h_bytes_per_step": nsl * N_RAYS * N_RAYS * 4,
                     "max_abs_diff_vs_device_path": spot},
-            "roofline": {"bound": "hbm", "achieved": alg_bytes / bp_avg_s / 1e9, "peak": hbm_peak,
-                         "unit": "GB/s", "frac": alg_bytes / bp_avg_s / 1e9 / hbm_peak,
+            "roofline": {"bound": "smem-gather", "achieved": gups_bp, "peak": peak_gups, "unit": "GUPS",
+                         "frac": gups_bp / peak_gups,
+                         "kernel": "bp_kernel_s4<nearest,f32,interleaved>",
+                         "kernel_ms_per_launch": bp_avg_s * 1e3,
+                         "updates_per_launch": upd_per_launch,
+                         "peak_def": "148 SMs x SM clock (median sampled) x 32 updates/clk: 128 B/clk of "
+                                     "shared-memory data pipe / 4 B per update",
+                         "sm_mhz": sm_mhz,
                          "traffic": BP_TRAFFIC_PER_LAUNCH if chunk == 32 else None,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 32-slice "
                                            "launch (S4 interleaved, AB16), --set full capture",
                          "algorithmic_bytes_per_launch": alg_bytes,
-                         "kernel": "bp_kernel_s4<nearest,f32,interleaved>", "peak_kind": peak_kind,
-                         "note": "the backprojector is bounded by its shared-memory gather, see gather_roofline"},
+                         "hbm": {"achieved_gbs": alg_bytes / bp_avg_s / 1e9, "peak_gbs": hbm_peak,
+                                 "frac": alg_bytes / bp_avg_s / 1e9 / hbm_peak, "peak_kind": peak_kind}},
             "gather_roofline": {"achieved_gups": gups_bp, "peak_gups": peak_gups, "frac": gups_bp / peak_gups,
                                 "bytes_per_update": 4, "fp32_ops_per_update": 4, "sm_mhz": sm_mhz},
             "kernel_ms": {"filter_per_launch": f_ms / max(1, f_n), "bp_per_launch": bp_ms / max(1, bp_n),
@@ -937,7 +1012,8 @@ def run_reference(args):
     P, I = ctypes.c_void_p, ctypes.c_int
     lib.getFBPMultiGPU.argtypes = [P, I, P, P, P, P, P]
     g = np.array([local], np.intc)
-    pf, pi = fbp_params(S, blocksize=S)
+    # blocksize 0: the reference chooses its own slice block (process.cu:31-66)
+    pf, pi = fbp_params(S, blocksize=0)
     obj = np.zeros((S, N_RAYS, N_RAYS), np.float32)
     angp = np.ascontiguousarray(ang)
 
@@ -957,17 +1033,17 @@ def run_reference(args):
             ts.append(time.perf_counter() - t0)
     ms = 1e3 * sum(ts) / len(ts)
     value = S / (ms / 1e3)
-    sample = (f"{S} of 512 slices per step through the reference's own getFBPMultiGPU "
-              f"(reference CUDA sources built for sm_100a, host buffers, blocksize {S})")
+    sample = (f"{S} of the workload's 512 slices per step through the reference's own getFBPMultiGPU "
+              f"(its CUDA sources built for sm_100a, host buffers, blocksize chosen by the reference)")
     print(json.dumps({
-        "impl": "reference", "metric": "FBP slices/s at 2048^2 x 1800 angles", "value": value,
+        "impl": "reference", "metric": METRIC, "value": value,
         "unit": "slices/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (same generator and seeds as the ours arm)",
-        "config": {"workload": WORKLOAD, "operator": "reference nearest-sample FBP (padded 6144^2 grid)",
-                   "sample_slices_per_step": S},
+        "data": DATA, "config": bench_config(1),
+        "slices_per_step": S,
         "cpu_baseline": {"value": value, "unit": "slices/s", "cores": 1, "kind": "reference", "sample": sample},
-        "e2e": {"value": value, "unit": "slices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": value, "unit": "slices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "note": "the reference's call takes host buffers: its copies are inside every step"},
         "clocks": clk.summary(),
     }), flush=True)
 
@@ -977,11 +1053,12 @@ def run_reference_temfq(args, lib_path, dev, local):
     tEMFQ workload (host buffers), for comparison with the ours arm's temfq
     section; prints its own line."""
     S = args.ref_slices
-    counts, flat, ang, x0, dx = temfq_inputs(S, dev)
-    h_counts, h_flat = counts.cpu().numpy(), flat.cpu().numpy()
     lib = ctypes.CDLL(lib_path)
-    P, I = ctypes.c_void_p, ctypes.c_int
+    P, I, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
     lib.get_tEM_FQ_MultiGPU.argtypes = [P, I, P, P, P, P, P, P]
+    lib.getRadonRTMultiGPU.argtypes = [P, I, P, P, P, I, I, I, I, I, F, F]
+    counts, flat, ang, x0, dx = temfq_inputs(S, dev, radon_lib=lib)
+    h_counts, h_flat = counts.cpu().numpy(), flat.cpu().numpy()
     g = np.array([local], np.intc)
     pi = np.array([EM_N, EM_A, S, EM_N, TEMFQ_ZPAD, 0, 0, S, TEMFQ_ITERS, 1, S], np.int32)
     pf = np.array([dx, dx, 0.0], np.float32)
@@ -1010,7 +1087,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--slices", type=int, default=N_SLICES)
-    ap.add_argument("--ref-slices", type=int, default=4)
+    ap.add_argument("--ref-slices", type=int, default=32)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-radon", action="store_true")
     ap.add_argument("--no-em", action="store_true")

@@ -181,7 +181,8 @@ int raft_fbp_device(int gpu, float *d_obj, const float *d_tomogram, const float 
  * Working memory comes from one fixed 64 MiB device array inside the library, held by
  * every GPU that loads it until exit; the first call on a device looks up that array's
  * address (make it before any stream capture).  Calls share the array: calls whose work
- * overlaps on one GPU race.  Limits: N*(1+pad) <= 14080 with prime factors 2,3,5,7,
+ * overlaps on one GPU (other host threads, other streams) race.  Runs the planar
+ * backprojector, so large volumes take longer than through raft_fbp_device.  Limits: N*(1+pad) <= 14080 with prime factors 2,3,5,7,
  * nangles <= 32768, one slice's filtered rows + tables within 64 MiB; larger requests
  * return 1 with a message.  Synchronises `stream` before returning. */
 int raft_fbp_device_noalloc(int gpu, float *d_obj, const float *d_tomogram, const float *angles,

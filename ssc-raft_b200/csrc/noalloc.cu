@@ -22,7 +22,14 @@
 //
 // Set-up: the first call on each device (with that device current) looks up
 // the array's device address with cudaGetSymbolAddress; make that first call
-// before any stream capture.
+// before any stream capture.  The address belongs to the device's context:
+// like the library's other per-device state (streams, workspaces), it does
+// not survive a cudaDeviceReset by the host application.
+//
+// Every call ends by synchronising the stream it was given.  It always runs
+// the planar backprojector: the slice-interleaved rows raft_fbp_device uses
+// for four slices at a time need four slices' rows twice over (178 MB at
+// 2048^2 x 1800), beyond the array.
 #include "engine.hpp"
 
 #include <cmath>

@@ -1,0 +1,47 @@
+"""Run one call of the REFERENCE library (oracle/_ref/libraft_ref.so, built
+from the reference's own CUDA sources) in a process of its own, so that its
+exports never meet this repository's libraft.so in one address space.
+
+    python tests/ref_runner.py fbp IN.npz OUT.npz
+
+IN.npz holds the arguments with the reference's packing (`sino`, `angles`,
+`paramf`, `parami`); OUT.npz receives `out`.  Test infrastructure only."""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_LIB = os.path.join(REPO, "oracle", "_ref", "libraft_ref.so")
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def run_fbp(d):
+    """getFBPMultiGPU (fbp.cu:238-302) on GPU 0 with host buffers."""
+    lib = ctypes.CDLL(REF_LIB)
+    P, I = ctypes.c_void_p, ctypes.c_int
+    lib.getFBPMultiGPU.argtypes = [P, I, P, P, P, P, P]
+    sino = np.ascontiguousarray(d["sino"], np.float32)
+    ang = np.ascontiguousarray(d["angles"], np.float32)
+    pf = np.ascontiguousarray(d["paramf"], np.float32)
+    pi = np.ascontiguousarray(d["parami"], np.int32)
+    No = int(pi[3])
+    obj = np.zeros((sino.shape[0], No, No), np.float32)
+    g = np.array([0], np.intc)
+    lib.getFBPMultiGPU(_p(g), 1, _p(obj), _p(sino), _p(ang), _p(pf), _p(pi))
+    return obj
+
+
+def main():
+    kind, src, dst = sys.argv[1:4]
+    d = np.load(src)
+    out = {"fbp": run_fbp}[kind](d)
+    np.savez(dst, out=out)
+
+
+if __name__ == "__main__":
+    main()

@@ -116,3 +116,66 @@ def test_em_windows_in_bounds(N):
                 assert k.min() >= 0 and k.max() < W
         # the projector writes bins [0, N) at element (bin - wlo): inside the row
         assert -wlo >= 0 and N - 1 - wlo < Wg
+
+
+def _tiles(a, ty, tx):
+    """[Ye, Xe] -> [tiles_y, tiles_x, TY, TX]."""
+    return a.reshape(ty, TY, tx, TX).transpose(0, 2, 1, 3)
+
+
+def check_fbp_ref_vectorised(N, pad, pixel, angles):
+    """check_fbp_ref for large N: one angle's whole image at a time."""
+    pf = np.array([0, 0, 1, 0, pixel, pixel, 0], np.float32)
+    pi = np.array([N, len(angles), 1, N, pad, 0, 0, 5, 0, 0], np.int32)
+    wlo, Wg, W, align = plan(pf, pi, 0, 0)
+    Np, off = N * (1 + pad), (pad * N) // 2
+    xmin = f32(-f32(pixel) * f32(Np) / f32(2.0))
+    Xe, Ye = -(-N // TX) * TX, -(-N // TY) * TY
+    x = (xmin + (np.arange(Xe) + off).astype(f32) * f32(pixel)).astype(f32)
+    y = (xmin + (np.arange(Ye) + off).astype(f32) * f32(pixel)).astype(f32)
+    for th in angles:
+        c, s = np.cos(f32(th), dtype=f32), np.sin(f32(th), dtype=f32)
+        t = (x[None, :] * c - y[:, None] * s).astype(f32)
+        ti = _tiles(np.trunc(((t - xmin) / f32(pixel)).astype(f32)).astype(np.int64), Ye // TY, Xe // TX)
+        corners = np.minimum(np.minimum(ti[:, :, 0, 0], ti[:, :, 0, -1]), np.minimum(ti[:, :, -1, 0], ti[:, :, -1, -1]))
+        b = corners - 1 - wlo
+        b = b - ((b % align) + align) % align
+        assert b.min() >= 0 and b.max() <= Wg - W, (N, th, int(b.min()), int(b.max()), Wg, W)
+        k = ti - (wlo + b)[:, :, None, None]
+        # no pixel reaches the kernel's clamp at W - 1 from beyond the window
+        assert k.min() >= 0 and k.max() < W, (N, th, int(k.min()), int(k.max()), W)
+
+
+def check_fbp_lin_vectorised(N, pad, pixel, angles, store):
+    pf = np.array([0, 0, 1, 0, pixel, pixel, 0], np.float32)
+    pi = np.array([N, len(angles), 1, N, pad, 0, 0, 5, 0, 0], np.int32)
+    wlo, Wg, W, align = plan(pf, pi, 1, store)
+    Np, off = N * (1 + pad), (pad * N) // 2
+    c0 = off - 0.5 * Np
+    u0 = 0.5 * Np - wlo - 0.5
+    Xe, Ye = -(-N // TX) * TX, -(-N // TY) * TY
+    tx0 = (np.arange(Xe // TX) * TX)[None, :]
+    ty0 = (np.arange(Ye // TY) * TY)[:, None]
+    li = np.arange(TX, dtype=f32)
+    lj = np.arange(TY, dtype=f32)
+    for th in angles:
+        cd, sd = np.cos(float(f32(th))), -np.sin(float(f32(th)))
+        v00 = (tx0 + c0) * cd + (ty0 + c0) * sd + u0
+        vmin = v00 + min(0.0, (TX - 1) * cd) + min(0.0, (TY - 1) * sd)
+        b = np.floor(vmin).astype(np.int64) - 1
+        b = b - ((b % align) + align) % align
+        assert b.min() >= 0 and b.max() <= Wg - W
+        va = (v00 - b).astype(f32)
+        v = (va[:, :, None, None] + lj[None, None, :, None] * f32(sd) + li[None, None, None, :] * f32(cd)).astype(f32)
+        k = np.rint(v)
+        assert k.min() >= 0 and k.max() <= W - 1, (N, th, float(k.min()), float(k.max()), W)
+
+
+def test_fbp_windows_in_bounds_at_the_benchmark_size():
+    """2048^2 images, 1800 angles over [0, pi), padding 2 (the batched FBP
+    workload): every 15th angle plus the axis-aligned and diagonal ones."""
+    ang = (np.arange(1800) * (np.pi / 1800)).astype(np.float32)
+    pick = np.concatenate([ang[::15], np.array([np.pi / 4, np.pi / 2, 3 * np.pi / 4], np.float32)])
+    check_fbp_ref_vectorised(2048, 2, 1.0, pick)
+    check_fbp_lin_vectorised(2048, 2, 1.0, pick[::2], 1)
+    check_fbp_lin_vectorised(2048, 2, 1.0, pick[::2], 2)
