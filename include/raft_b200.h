@@ -67,8 +67,8 @@ void get_eEM_RT_MultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, floa
 
 /* Rotation-axis offset from the 0 and 180 degree frames [sizey][sizex] (host arrays) by
  * phase correlation, the reference's integer / sub-pixel searches (their candidate sets kept
- * as they are), on the calling thread's current device.  Frame sides must have only the
- * prime factors 2, 3, 5, 7.  Errors via raft_last_error (result 0).
+ * as they are), on the calling thread's current device.  Frame sides up to 14528 with prime
+ * factors 2, 3, 5, 7, about 7000 otherwise.  Errors via raft_last_error (result 0).
  * Replace findcentersino / findcentersino_subpixel / findcentersino16,
  * cuda/src/processing/rotation_axis.cu:429-451 (rafttypes.py:201-219). */
 int findcentersino(float *frame0, float *frame180, float *dark, float *flat, int sizex, int sizey);
@@ -97,7 +97,8 @@ void correctRotationAxis(float *tomoin, float *tomoout, int sizex, int sizey, in
 /* FBP by the backprojection slice theorem (Fourier regridding), packing as getFBPMultiGPU
  * (object N x N).  Angles are taken as uniform over [0, pi), as the reference's regridding
  * assumes (the Python wrapper passes linspace(0, pi, A)); `angles` and `nstreams` are unused.
- * Requires N*(1+pad) with prime factors 2, 3, 5, 7 only and <= 9472.
+ * Requires N*(1+pad) <= 14528 with prime factors 2, 3, 5, 7 only, or about 7000 with larger
+ * prime factors (transformed by Bluestein's algorithm).
  * Replaces getBSTMultiGPU, cuda/src/geometries/parallel/reconstruction_methods/bst.cu:674-734
  * (rafttypes.py:161-173). */
 void getBSTMultiGPU(int *gpus, int ngpus, float *obj, float *tomogram, float *angles, float *paramf,
@@ -113,7 +114,8 @@ int raft_bst_device(int gpu, float *d_obj, const float *d_tomogram, const float 
  * guess in / result out, angles uniform over [0, pi), flat [nslices][nrays];
  * parami = [nrays, nangles, nslices, objsize (= nrays), zpad, 0, 0, nflats, iterations,
  * interpolation (0 nearest, 1 bilinear), blocksize], paramf = [detector pixel x, y, tv (unused,
- * as in the reference)].  N even; N(1+zpad) and N(1+zpad)/2 with prime factors 2, 3, 5, 7.
+ * as in the reference)].  N even; N(1+zpad) up to 14528 with prime factors 2, 3, 5, 7, about
+ * 7000 otherwise.
  * Replaces get_tEM_FQ_MultiGPU, cuda/src/geometries/parallel/reconstruction_methods/
  * em_frequency.cu:333-398 (rafttypes.py:149-159). */
 void get_tEM_FQ_MultiGPU(int *gpus, int ngpus, float *count, float *obj, float *angles, float *flat,

@@ -218,7 +218,8 @@ static double centersino_entry(const T *frame0, const T *frame180, const T *dark
         return 0.0;
     }
     if (!centersino_shape_ok(sizex, sizey)) {
-        set_error(std::string(name) + ": frame sides must have only the prime factors 2, 3, 5, 7 (at most 14528)");
+        set_error(std::string(name) + ": frame sides too long for the shared-memory transforms (at most 14528 with "
+                                      "prime factors 2, 3, 5, 7, about 7000 otherwise)");
         return 0.0;
     }
     int dev = 0;
@@ -363,8 +364,8 @@ int raft_fbp_device(int gpu, float *d_obj, const float *d_tomogram, const float 
         FbpTables tb = fbp_tables(ds, fp, angles, st);
         const size_t tomo_ps = (size_t)cfg.nangles * cfg.nrays;
         const int chunk = std::max(1, std::min(cfg.nslices, cfg.blocksize > 0 ? cfg.blocksize : 32));
-        void *rows = ds.rows.get(fbp_rows_bytes(fp, chunk));
         void *il = fbp_il_bytes(fp, chunk) ? ds.il.get(fbp_il_bytes(fp, chunk)) : nullptr;
+        void *rows = (il && fbp_fused_il(fp)) ? nullptr : ds.rows.get(fbp_rows_bytes(fp, chunk));
         for (int s0 = 0; s0 < cfg.nslices; s0 += chunk) {
             const int ns = std::min(chunk, cfg.nslices - s0);
             fbp_chunk(ds, fp, tb, d_tomogram + tomo_ps * s0, d_obj + (size_t)fp.No * fp.No * s0, ns, rows, st, il);
@@ -772,7 +773,7 @@ static bool parse_bst(const float *paramf, const int *parami, FbpConfig &cfg)
     }
     BstPlanShape sh;
     if (!bst_plan_shape(sh, cfg.nrays, cfg.nangles, cfg.pad)) {
-        set_error("BST: the padded length N*(1+pad) must have only the prime factors 2, 3, 5, 7 and be at most 9472");
+        set_error("BST: the padded length N*(1+pad) is too long for the shared-memory transforms (at most 14528 with prime factors 2, 3, 5, 7; about 7000 otherwise)");
         return false;
     }
     return true;
@@ -845,8 +846,9 @@ static bool parse_temfq(const float *paramf, const int *parami, TemfqConfig &c)
     }
     if (c.nslices < 0 || c.niter < 0 || (c.interpolation != 0 && c.interpolation != 1) ||
         !temfq_shape_ok(c.nrays, c.nangles, c.zpad)) {
-        set_error("tEMFQ: unsupported sizes (N even; N(1+zpad) and N(1+zpad)/2 with prime factors 2, 3, 5, 7 "
-                  "only; N(1+zpad) <= 14528), or iterations < 0, or interpolation not 0/1");
+        set_error("tEMFQ: unsupported sizes (N even; the N(1+zpad)- and N(1+zpad)/2-point transforms must fit "
+                  "shared memory: N(1+zpad) <= 14528 with prime factors 2, 3, 5, 7, about 7000 otherwise), or "
+                  "iterations < 0, or interpolation not 0/1");
         return false;
     }
     return true;

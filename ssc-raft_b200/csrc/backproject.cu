@@ -667,28 +667,37 @@ static bool forced_tune(BpTune &t)
     return false;
 }
 
+bool bp_forced_planar()
+{
+    BpTune t;
+    return forced_tune(t) && t.S != 4;
+}
+
 // Pick (S, AB) for this configuration: the cached choice, else time every
 // candidate that fits shared memory on 8 to 32 slices of the real data
 // (store launches only -- they are idempotent), else a default.  With
 // a_il (the same launch on slice-interleaved rows) the S = 4 candidates are
-// timed on it; prep_il makes those rows and is called at most once.
+// timed on it; prep_il makes those rows and is called at most once.  With
+// il_only the rows exist only interleaved: the S = 4 candidates alone.
 template <class Prep>
 static BpTune choose_tune(const BpArgs &a, const BpArgs *a_il, Prep &&prep_il, int geometry, int store,
-                          cudaStream_t st)
+                          cudaStream_t st, bool il_only = false)
 {
     int dev = 0;
     cudaGetDevice(&dev);
-    const TuneKey key(dev, geometry, store + (a_il ? 16 : 0), a.No, a.W, a.nangles);
+    const TuneKey key(dev, geometry, store + (a_il ? 16 : 0) + (il_only ? 32 : 0), a.No, a.W, a.nangles);
     const int esize = store_bytes(store);
     BpTune forced;
-    if (forced_tune(forced) && bp_smem(forced.S, forced.AB, a.W, esize) <= kBpSmemMax) return forced;
+    if (forced_tune(forced) && bp_smem(forced.S, forced.AB, a.W, esize) <= kBpSmemMax && (!il_only || forced.S == 4))
+        return forced;
     {
         std::lock_guard<std::mutex> lk(g_tune_mtx);
         auto it = g_tune.find(key);
         if (it != g_tune.end()) return it->second;
     }
     BpTune best{2, 16};
-    if (bp_smem(best.S, best.AB, a.W, esize) > kBpSmemMax) best = {1, 8};
+    if (il_only) best = {4, 16};
+    if (bp_smem(best.S, best.AB, a.W, esize) > kBpSmemMax) best = {il_only ? 4 : 1, 8};
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(st, &cap);
     const bool can_tune = tuning_enabled() && a.update == 0 && cap == cudaStreamCaptureStatusNone;
@@ -698,6 +707,11 @@ static BpTune choose_tune(const BpArgs &a, const BpArgs *a_il, Prep &&prep_il, i
         BpArgs t0 = a;
         const long long tiles = (long long)((a.No + BP_TX - 1) / BP_TX) * ((a.No + BP_TY - 1) / BP_TY);
         const int want = (int)std::min<long long>(32, std::max<long long>(8, (4LL * 3 * 148 * 8 + tiles - 1) / tiles));
+        if (a.nslices < std::min(want, 8)) {
+            // too few slices to time the shapes fairly (a pipeline's small
+            // first chunk): run the default now, tune on a later launch
+            return best;
+        }
         t0.nslices = std::min(a.nslices, (want + 3) / 4 * 4);
         cudaEvent_t e0, e1;
         RAFT_CUDA(cudaEventCreate(&e0));
@@ -705,6 +719,7 @@ static BpTune choose_tune(const BpArgs &a, const BpArgs *a_il, Prep &&prep_il, i
         float best_ms = 1e30f;
         for (const BpTune &c : kTuneCandidates) {
             if (bp_smem(c.S, c.AB, a.W, esize) > kBpSmemMax) continue;
+            if (il_only && c.S != 4) continue;
             BpArgs t = t0;
             if (c.S == 4 && a_il) {
                 prep_il();
@@ -804,6 +819,14 @@ void launch_backproject(const BpLaunch &bl, cudaStream_t st)
     BpArgs a_il = a;
     a_il.filt = reinterpret_cast<const unsigned char *>(bl.il_ws);
     a_il.il = 1;
+    if (bl.il_ready) {
+        // the filter wrote the rows interleaved: four slices per CTA only
+        RAFT_CHECK(il_ok, "backprojector: interleaved rows need the workspace and 4-byte elements");
+        auto none = []() {};
+        const BpTune t = choose_tune(a_il, &a_il, none, bl.geometry, store, st, true);
+        launch_bp_any(a_il, bl.geometry, store, t, st);
+        return;
+    }
     bool il_done = false;
     auto prep_il = [&]() {
         if (il_done) return;

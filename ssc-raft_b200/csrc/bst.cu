@@ -41,6 +41,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -56,11 +57,8 @@ struct BstArgs {
     float2 *polar;          // [B][2A][Lh]
     float2 *T;              // [B][S][N]: rows inverse-transformed along x, crop columns
     float *obj;             // [B][N][N]
-    const float2 *tw;       // exp(-2 pi i k / Np)   (filter transforms)
-    const float2 *twL;      // exp(-2 pi i k / L)    (half-ray transforms)
-    const float2 *twS;      // exp(-2 pi i k / S)    (grid transforms)
+    FftPlan pN, pL, pS;     // transforms of the filter (Np), the half-rays (L), the grid (S)
     const float2 *G;        // filter weights [Np], or null for 'none'
-    RadixList rl, rlL, rlS;
     int N, A, Np, L, Lh, S, off, M;   // M = max(Np, L): shared-memory buffer length of the row kernel
     float w_half;           // half-ray weight (the centre sample gets half of it)
     float scale;
@@ -82,32 +80,44 @@ __global__ void __launch_bounds__(512) bst_rows_kernel(const BstArgs p)
     __syncthreads();
     float sgn1 = 1.f;   // the second row is sgn1 * z.y
     if (p.G) {
-        float2 *r = fft_forward(z, sm_bst + p.M, p.Np, p.rl, p.tw);
+        float2 *r = fft_run(z, sm_bst + p.M, p.pN);
         for (int k = threadIdx.x; k < p.Np; k += blockDim.x) {
             const float2 g = cmul(r[k], __ldg(&p.G[k]));
             r[k] = make_float2(g.x, -g.y);
         }
         __syncthreads();
         // forward transform of the conjugate = conjugate of the inverse
-        z = fft_forward(r, r == sm_bst ? sm_bst + p.M : sm_bst, p.Np, p.rl, p.tw);
+        z = fft_run(r, r == sm_bst ? sm_bst + p.M : sm_bst, p.pN);
         sgn1 = -1.f;
     }
+    // two buffers of M elements: the filtered pair z, and the other one.  The
+    // second row's half-rays are parked in its own (not yet written) polar row
+    // while the first row is transformed, then brought back.
     float2 *fa = (z == sm_bst) ? sm_bst + p.M : sm_bst;
-    float2 *fb = sm_bst + 2 * p.M;
+    float2 *fb = z;
     const int c = p.Np / 2, half = p.Np / 2;
     const size_t pb = (size_t)slice * 2 * p.A * p.Lh;
+    float2 *park = p.polar + pb + (size_t)a1 * p.Lh;       // half <= Lh entries
+    if (has1)
+        for (int idx = threadIdx.x; idx < half; idx += blockDim.x) {
+            const float w = idx == 0 ? 0.5f * p.w_half : p.w_half;
+            park[idx] = make_float2(w * sgn1 * z[c - 1 - idx].y, w * sgn1 * z[c + idx].y);
+        }
     for (int r = 0; r < (has1 ? 2 : 1); r++) {
         for (int idx = threadIdx.x; idx < p.L; idx += blockDim.x) {
             float2 h = make_float2(0.f, 0.f);
             if (idx < half) {
-                const float w = idx == 0 ? 0.5f * p.w_half : p.w_half;
-                const float2 lft = z[c - 1 - idx], rgt = z[c + idx];
-                h = r == 0 ? make_float2(w * lft.x, w * rgt.x) : make_float2(w * sgn1 * lft.y, w * sgn1 * rgt.y);
+                if (r == 0) {
+                    const float w = idx == 0 ? 0.5f * p.w_half : p.w_half;
+                    h = make_float2(w * z[c - 1 - idx].x, w * z[c + idx].x);
+                } else {
+                    h = park[idx];       // written by this same thread above
+                }
             }
             fa[idx] = h;
         }
         __syncthreads();
-        const float2 *H = fft_forward(fa, fb, p.L, p.rlL, p.twL);
+        const float2 *H = fft_run(fa, fb, p.pL);
         float2 *frow = p.polar + pb + (size_t)(a0 + r) * p.Lh;           // left half-ray (theta + pi)
         float2 *rrow = p.polar + pb + (size_t)(p.A + a0 + r) * p.Lh;     // right half-ray (theta)
         for (int k = threadIdx.x; k < p.Lh; k += blockDim.x) {
@@ -118,6 +128,9 @@ __global__ void __launch_bounds__(512) bst_rows_kernel(const BstArgs p)
             rrow[k] = make_float2(0.5f * (Zk.y + Zm.y) * sig, -0.5f * (Zk.x - Zm.x) * sig);
         }
         __syncthreads();
+        // the next row's input goes to the buffer the result is not in
+        fa = (H == fa) ? fb : fa;
+        fb = (fa == sm_bst) ? sm_bst + p.M : sm_bst;
     }
 }
 
@@ -155,7 +168,7 @@ __global__ void __launch_bounds__(512) bst_regrid_kernel(const BstArgs p)
         sm_bst[X] = make_float2(v.x * sgn, -v.y * sgn);   // conjugated: see bst_cols_kernel
     }
     __syncthreads();
-    const float2 *r = fft_forward(sm_bst, sm_bst + fft_span(S), S, p.rlS, p.twS);
+    const float2 *r = fft_run(sm_bst, sm_bst + fft_plan_span(p.pS), p.pS);
     float2 *trow = p.T + ((size_t)slice * S + Y) * p.N;
     for (int i = threadIdx.x; i < p.N; i += blockDim.x) trow[i] = r[p.off + i];
 }
@@ -169,9 +182,40 @@ __global__ void __launch_bounds__(512) bst_cols_kernel(const BstArgs p)
     const float2 *tcol = p.T + (size_t)slice * p.S * p.N + i;
     for (int Y = threadIdx.x; Y < p.S; Y += blockDim.x) sm_bst[Y] = tcol[(size_t)Y * p.N];
     __syncthreads();
-    const float2 *r = fft_forward(sm_bst, sm_bst + fft_span(p.S), p.S, p.rlS, p.twS);
+    const float2 *r = fft_run(sm_bst, sm_bst + fft_plan_span(p.pS), p.pS);
     float *o = p.obj + (size_t)slice * p.N * p.N + i;
     for (int j = threadIdx.x; j < p.N; j += blockDim.x) o[(size_t)j * p.N] = r[p.off + j].x / p.scale;
+}
+
+// Forward DFT in FP64 of a 7-smooth length (recursive decimation in time on
+// the smallest factor), for the Bluestein chirp spectrum.
+void dft_rec(const std::complex<double> *in, size_t stride, int n, std::complex<double> *out)
+{
+    if (n == 1) {
+        out[0] = in[0];
+        return;
+    }
+    int p = 2;
+    while (n % p) p++;
+    const int m = n / p;
+    for (int r = 0; r < p; r++) dft_rec(in + r * stride, stride * p, m, out + (size_t)r * m);
+    std::vector<std::complex<double>> tmp(n);
+    for (int k = 0; k < m; k++)
+        for (int q = 0; q < p; q++) {
+            std::complex<double> acc = 0.0;
+            for (int r = 0; r < p; r++) {
+                const double a = -2.0 * M_PI * (double)(((long long)r * (k + (long long)q * m)) % n) / (double)n;
+                acc += out[(size_t)r * m + k] * std::complex<double>(std::cos(a), std::sin(a));
+            }
+            tmp[(size_t)q * m + k] = acc;
+        }
+    std::copy(tmp.begin(), tmp.end(), out);
+}
+
+void dft_host(const std::vector<std::complex<double>> &in, std::vector<std::complex<double>> &out)
+{
+    out.assign(in.size(), 0.0);
+    dft_rec(in.data(), 1, (int)in.size(), out.data());
 }
 
 using BstKey = std::tuple<int, int, int, int, double, double>;
@@ -200,16 +244,56 @@ std::map<std::pair<int, int>, std::unique_ptr<FftTable>> g_fft_tables;
 
 }  // namespace
 
+int fft_plan_length(int n)
+{
+    int r[24], nr = 0;
+    if (n < 1) return 0;
+    if (factorize(n, r, nr)) return n;
+    for (int M = 2 * n - 1; M <= 8 * n; M++)
+        if (factorize(M, r, nr)) return M;
+    return 0;
+}
+
 const FftTable &fft_table(int device, int n)
 {
     std::lock_guard<std::mutex> lk(g_fft_mtx);
     auto &slot = g_fft_tables[{device, n}];
     if (!slot) {
         auto t = std::make_unique<FftTable>();
-        RAFT_CHECK(factorize(n, t->rl.r, t->rl.n), "FFT length with a prime factor above 7");
-        const std::vector<float2> h = fft_twiddles(n);
-        RAFT_CUDA(cudaMalloc(&t->tw, sizeof(float2) * n));
-        RAFT_CUDA(cudaMemcpy(t->tw, h.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+        const int M = fft_plan_length(n);
+        RAFT_CHECK(M > 0, "FFT length without a transform plan");
+        FftPlan &P = t->plan;
+        P.n = n;
+        P.M = M;
+        RAFT_CHECK(factorize(M, P.rl.r, P.rl.n), "FFT plan length");
+        if (M == n) {
+            t->rl = P.rl;
+            const std::vector<float2> h = fft_twiddles(n);
+            RAFT_CUDA(cudaMalloc(&t->tw, sizeof(float2) * n));
+            RAFT_CUDA(cudaMemcpy(t->tw, h.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+        } else {
+            // chirp w_j = exp(-i pi j^2 / n) (j^2 reduced mod 2n, exact in 64 bits)
+            // and the M-point transform of c_m = conj(w_|m|), |m| < n, in FP64
+            std::vector<float2> w(n);
+            std::vector<std::complex<double>> c(M, 0.0), C(M);
+            for (int j = 0; j < n; j++) {
+                const long long q = ((long long)j * j) % (2LL * n);
+                const double a = -M_PI * (double)q / (double)n;
+                w[j] = make_float2((float)std::cos(a), (float)std::sin(a));
+                const std::complex<double> cj(std::cos(a), -std::sin(a));
+                c[j] = cj;
+                if (j) c[M - j] = cj;
+            }
+            dft_host(c, C);
+            std::vector<float2> B(M);
+            for (int k = 0; k < M; k++) B[k] = make_float2((float)(C[k].real() / M), (float)(C[k].imag() / M));
+            RAFT_CUDA(cudaMalloc(&t->chirp, sizeof(float2) * n));
+            RAFT_CUDA(cudaMalloc(&t->B, sizeof(float2) * M));
+            RAFT_CUDA(cudaMemcpy(t->chirp, w.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+            RAFT_CUDA(cudaMemcpy(t->B, B.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
+            P.chirp = t->chirp;
+            P.B = t->B;
+        }
         slot = std::move(t);
     }
     return *slot;
@@ -218,25 +302,31 @@ const FftTable &fft_table(int device, int n)
 FftTable::~FftTable()
 {
     if (tw) cudaFree(tw);
+    if (chirp) cudaFree(chirp);
+    if (B) cudaFree(B);
 }
 
 constexpr size_t kBstSmemMax = 227 * 1024;
 
-static bool fft_len_ok(int n)
+// Buffer span of the transform plan of n (Bluestein lengths transform M > n
+// points); huge when n has no plan.
+static int plan_span(int n)
 {
-    int r[24], nr = 0;
-    return n >= 1 && factorize(n, r, nr);
+    const int M = fft_plan_length(n);
+    return M > 0 ? fft_span(M) : (1 << 28);
 }
 
 // Shared-memory buffer length of the row kernel: the padded row and both
 // transforms' ping-pong buffers (fft_span is not monotonic at its padding limit).
-static int bst_row_span(const BstCore &c) { return std::max({c.Np, fft_span(c.Np), fft_span(c.L)}); }
+static int bst_row_span(const BstCore &c)
+{
+    return std::max({c.Np, c.filtered ? plan_span(c.Np) : 0, plan_span(c.L)});
+}
 
 bool bst_core_ok(const BstCore &c)
 {
-    return c.N >= 2 && c.A >= 1 && c.L >= 2 && c.S >= 2 && fft_len_ok(c.L) && fft_len_ok(c.S) &&
-           (!c.filtered || fft_len_ok(c.Np)) && 3 * (size_t)bst_row_span(c) * sizeof(float2) <= kBstSmemMax &&
-           2 * (size_t)fft_span(c.S) * sizeof(float2) <= kBstSmemMax;
+    return c.N >= 2 && c.A >= 1 && c.L >= 2 && c.S >= 2 && 2 * (size_t)bst_row_span(c) * sizeof(float2) <= kBstSmemMax &&
+           2 * (size_t)plan_span(c.S) * sizeof(float2) <= kBstSmemMax;
 }
 
 bool bst_plan_shape(BstPlanShape &s, int N, int A, int pad)
@@ -282,18 +372,9 @@ void bst_run(int device, const BstCore &c, const float *d_tomo, float *d_obj, in
     a.T = (float2 *)((char *)workspace + ((polar + 255) & ~(size_t)255));
     a.obj = d_obj;
     a.G = c.G;
-    if (c.G) {
-        const FftTable &tN = fft_table(device, c.Np);
-        a.tw = tN.tw;
-        a.rl = tN.rl;
-    } else {
-        a.tw = nullptr;
-        a.rl = RadixList{};
-    }
-    a.twL = tL.tw;
-    a.rlL = tL.rl;
-    a.twS = tS.tw;
-    a.rlS = tS.rl;
+    a.pN = c.G ? fft_table(device, c.Np).plan : FftPlan{};
+    a.pL = tL.plan;
+    a.pS = tS.plan;
     a.N = c.N;
     a.A = c.A;
     a.Np = c.Np;
@@ -304,8 +385,8 @@ void bst_run(int device, const BstCore &c, const float *d_tomo, float *d_obj, in
     a.M = bst_row_span(c);
     a.w_half = c.w_half;
     a.scale = c.scale;
-    const int threads = fft_threads(std::max(c.M, c.S));
-    const size_t sm3 = 3 * (size_t)a.M * sizeof(float2), sm2 = 2 * (size_t)fft_span(c.S) * sizeof(float2);
+    const int threads = fft_threads(std::max({c.M, a.pN.M, a.pL.M, a.pS.M}));
+    const size_t sm3 = 2 * (size_t)a.M * sizeof(float2), sm2 = 2 * (size_t)fft_plan_span(a.pS) * sizeof(float2);
     static thread_local int configured = -1;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -331,7 +412,7 @@ void launch_bst(int device, const FbpConfig &cfg, const float *d_tomo, float *d_
 {
     BstPlanShape shape;
     RAFT_CHECK(bst_plan_shape(shape, cfg.nrays, cfg.nangles, cfg.pad),
-               "BST: the padded length N*(1+pad) must have only the prime factors 2, 3, 5, 7 and be at most 9472");
+               "BST: the padded length N*(1+pad) is too long for the shared-memory transforms (at most 14528 with prime factors 2, 3, 5, 7; about 7000 otherwise)");
     BstCore c;
     c.N = shape.N;
     c.A = shape.A;

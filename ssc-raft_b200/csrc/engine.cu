@@ -193,14 +193,32 @@ static void run_pipeline(DeviceState &ds, int nslices, int chunk, size_t in_ps, 
         if (!pin_src) pin[b] = ds.pin_in[b].get(in_ps * chunk);
         if (!pin_dst) pout[b] = ds.pin_out[b].get(out_ps * chunk);
     }
-    const int nch = (nslices + chunk - 1) / chunk;
+    // Chunk schedule: the first chunk's upload and the last chunk's download
+    // overlap no compute, so with enough slices both are kept small (four
+    // slices, a whole group of the four-slice backprojector) and the rest
+    // goes in full chunks.
+    std::vector<int> cs0, cns;
+    {
+        const int edge = (chunk >= 8 && nslices > 2 * chunk) ? 4 : 0;
+        int s = 0;
+        auto add = [&](int n) {
+            cs0.push_back(s);
+            cns.push_back(n);
+            s += n;
+        };
+        if (edge) add(edge);
+        const int mid_end = nslices - edge;
+        while (s < mid_end) add(std::min(chunk, mid_end - s));
+        if (edge) add(edge);
+    }
+    const int nch = (int)cs0.size();
     auto finalize = [&](int c) {
-        const int b = c & 1, s0 = c * chunk, ns = std::min(chunk, nslices - s0);
+        const int b = c & 1, s0 = cs0[c], ns = cns[c];
         RAFT_CUDA(cudaEventSynchronize(ds.ev_d2h[b]));
         if (!pin_dst) parallel_memcpy((char *)host_out + (size_t)s0 * out_ps, pout[b], (size_t)ns * out_ps);
     };
     for (int c = 0; c < nch; c++) {
-        const int b = c & 1, s0 = c * chunk, ns = std::min(chunk, nslices - s0);
+        const int b = c & 1, s0 = cs0[c], ns = cns[c];
         const void *src = (const char *)host_in + (size_t)s0 * in_ps;
         if (!pin_src) {
             if (c >= 2) RAFT_CUDA(cudaEventSynchronize(ds.ev_h2d[b]));
@@ -307,14 +325,23 @@ size_t fbp_rows_bytes(const FbpPrepared &fp, int nslices)
     return (size_t)nslices * fp.cfg.nangles * fp.win.Wg * store_bytes(fp.cfg.store);
 }
 
+bool fbp_fused_il(const FbpPrepared &fp)
+{
+    return fbp_il_bytes(fp, 1) > 0 && !bp_forced_planar();
+}
+
 void fbp_chunk(DeviceState &ds, const FbpPrepared &fp, const FbpTables &tb, const float *d_sino, float *d_img,
                int nslices, void *d_rows, cudaStream_t st, void *d_il)
 {
     (void)ds;
     if (nslices <= 0) return;
+    // with the interleave workspace and 4-byte elements the filter writes the
+    // four-slice interleaved rows the backprojector stages, directly
+    const bool fused = d_il && fbp_fused_il(fp);
     FilterLaunch fl;
     fl.sino = d_sino;
-    fl.out = d_rows;
+    fl.out = fused ? d_il : d_rows;
+    fl.interleaved = fused ? 1 : 0;
     fl.wt = tb.wt;
     fl.nrows = nslices * fp.cfg.nangles;
     fl.nangles = fp.cfg.nangles;
@@ -323,7 +350,7 @@ void fbp_chunk(DeviceState &ds, const FbpPrepared &fp, const FbpTables &tb, cons
     fl.store = fp.cfg.store;
     launch_filter(*fp.plan, fl, st);
     BpLaunch bl;
-    bl.filt = d_rows;
+    bl.filt = fused ? nullptr : d_rows;
     bl.img = d_img;
     bl.No = fp.No;
     bl.nangles = fp.cfg.nangles;
@@ -338,6 +365,7 @@ void fbp_chunk(DeviceState &ds, const FbpPrepared &fp, const FbpTables &tb, cons
     bl.snd = tb.snd;
     bl.err = tb.err;
     bl.il_ws = d_il;
+    bl.il_ready = fused ? 1 : 0;
     launch_backproject(bl, st);
 }
 
@@ -366,8 +394,8 @@ void fbp_host_slab(const FbpConfig &cfg, int device, float *obj, const float *to
     const size_t in_ps = (size_t)cfg.nangles * cfg.nrays * sizeof(float);
     const size_t out_ps = (size_t)fp.No * fp.No * sizeof(float);
     const int chunk = auto_chunk(nslices, in_ps, cfg.blocksize);
-    void *rows = ds.rows.get(fbp_rows_bytes(fp, chunk));
     void *il = fbp_il_bytes(fp, chunk) ? ds.il.get(fbp_il_bytes(fp, chunk)) : nullptr;
+    void *rows = (il && fbp_fused_il(fp)) ? nullptr : ds.rows.get(fbp_rows_bytes(fp, chunk));
     run_pipeline(ds, nslices, chunk, in_ps, out_ps, tomo, obj, [&](void *din, void *dout, int ns, cudaStream_t st) {
         fbp_chunk(ds, fp, tb, (const float *)din, (float *)dout, ns, rows, st, il);
     });
@@ -436,8 +464,9 @@ void temfq_host_slab(const TemfqConfig &cfg, int device, float *obj, const float
 {
     if (nslices <= 0) return;
     const int N = cfg.nrays, A = cfg.nangles;
-    RAFT_CHECK(temfq_shape_ok(N, A, cfg.zpad), "tEMFQ: unsupported sizes (N even; N(1+zpad) and N(1+zpad)/2 "
-                                               "with prime factors 2, 3, 5, 7 only; N(1+zpad) <= 14528)");
+    RAFT_CHECK(temfq_shape_ok(N, A, cfg.zpad), "tEMFQ: unsupported sizes (N even; the N(1+zpad)- and "
+                                               "N(1+zpad)/2-point transforms must fit shared memory: N(1+zpad) <= "
+                                               "14528 with prime factors 2, 3, 5, 7, about 7000 otherwise)");
     DeviceState &ds = device_state(device);
     std::lock_guard<std::mutex> lk(ds.mtx);
     RAFT_CUDA(cudaSetDevice(device));
@@ -487,7 +516,7 @@ void bst_host_slab(const FbpConfig &cfg, int device, float *obj, const float *to
     if (nslices <= 0) return;
     BstPlanShape sh;
     RAFT_CHECK(bst_plan_shape(sh, cfg.nrays, cfg.nangles, cfg.pad),
-               "BST: the padded length N*(1+pad) must have only the prime factors 2, 3, 5, 7 and be at most 9472");
+               "BST: the padded length N*(1+pad) is too long for the shared-memory transforms (at most 14528 with prime factors 2, 3, 5, 7; about 7000 otherwise)");
     DeviceState &ds = device_state(device);
     std::lock_guard<std::mutex> lk(ds.mtx);
     RAFT_CUDA(cudaSetDevice(device));
@@ -505,7 +534,7 @@ void bst_device(const FbpConfig &cfg, int device, float *d_obj, const float *d_t
 {
     BstPlanShape sh;
     RAFT_CHECK(bst_plan_shape(sh, cfg.nrays, cfg.nangles, cfg.pad),
-               "BST: the padded length N*(1+pad) must have only the prime factors 2, 3, 5, 7 and be at most 9472");
+               "BST: the padded length N*(1+pad) is too long for the shared-memory transforms (at most 14528 with prime factors 2, 3, 5, 7; about 7000 otherwise)");
     DeviceState &ds = device_state(device);
     const int chunk = bst_chunk_slices(sh, nslices, cfg.blocksize);
     void *ws = ds.rows.get(bst_workspace_bytes(sh, chunk));

@@ -78,10 +78,15 @@ struct FbpTables {
 };
 FbpTables fbp_tables(DeviceState &ds, const FbpPrepared &fp, const float *h_angles, cudaStream_t st);
 // d_il (optional, fbp_il_bytes): workspace for the slice-interleaved rows the
-// nearest backprojector reads with four slices per CTA; null keeps the planar rows.
+// backprojector reads with four slices per CTA (4-byte elements: nearest f32,
+// bf16 pairs), written by the filter directly (d_rows may then be null);
+// null keeps the planar rows.
 void fbp_chunk(DeviceState &ds, const FbpPrepared &fp, const FbpTables &tb, const float *d_sino, float *d_img,
                int nslices, void *d_rows, cudaStream_t st, void *d_il = nullptr);
 size_t fbp_rows_bytes(const FbpPrepared &fp, int nslices);
+// True when fbp_chunk, given the interleave workspace, has the filter write
+// interleaved rows directly (no plain rows needed).
+bool fbp_fused_il(const FbpPrepared &fp);
 size_t fbp_il_bytes(const FbpPrepared &fp, int nslices);
 
 // Host-buffer FBP of one slab on one device (the body of getFBPMultiGPU).

@@ -257,13 +257,59 @@ __device__ __forceinline__ float2 *fft_forward(float2 *a, float2 *b, int Np, con
 }
 
 
+// ------------------------------------------------------- any length --
+// A forward DFT of any length n held in shared memory: directly when n has
+// only the prime factors 2, 3, 5, 7, otherwise by Bluestein's chirp-z
+// algorithm (L. Bluestein, "A linear filtering approach to the computation of
+// the discrete Fourier transform", 1970): with w_j = exp(-i pi j^2 / n),
+//   X_k = w_k sum_j (x_j w_j) conj(w_(k-j)),
+// a circular convolution of length M >= 2n - 1 (M 7-smooth) computed with two
+// M-point transforms and the precomputed transform of the chirp.
+struct FftPlan {
+    int n = 0, M = 0;                 // M == n: direct transform
+    RadixList rl{};                   // radices of M
+    const float2 *chirp = nullptr;    // w_j, j < n                     (Bluestein)
+    const float2 *B = nullptr;        // FFT_M(c) / M, c_m = conj(w_|m|)  (Bluestein)
+};
+// Elements each of the two shared-memory buffers of a transform needs.
+__host__ __device__ inline int fft_plan_span(const FftPlan &P) { return fft_span(P.M); }
+
+// Forward DFT of a[0..n) (plain order) with a, b holding fft_plan_span(P)
+// elements each; returns the buffer holding the n results (plain order).
+__device__ __forceinline__ float2 *fft_run(float2 *a, float2 *b, const FftPlan &P)
+{
+    if (P.M == P.n) return fft_forward(a, b, P.n, P.rl, nullptr);
+    const int n = P.n, M = P.M;
+    for (int j = threadIdx.x; j < M; j += blockDim.x)
+        a[j] = j < n ? cmul(a[j], __ldg(&P.chirp[j])) : make_float2(0.f, 0.f);
+    __syncthreads();
+    float2 *r = fft_forward(a, b, M, P.rl, nullptr);
+    for (int k = threadIdx.x; k < M; k += blockDim.x) {
+        const float2 g = cmul(r[k], __ldg(&P.B[k]));
+        r[k] = make_float2(g.x, -g.y);
+    }
+    __syncthreads();
+    // FFT(conj(FFT(a) B)) = conj of the circular convolution (B carries 1/M)
+    float2 *o = (r == a) ? b : a;
+    float2 *r2 = fft_forward(r, o, M, P.rl, nullptr);
+    for (int k = threadIdx.x; k < n; k += blockDim.x)
+        r2[k] = cmul(make_float2(r2[k].x, -r2[k].y), __ldg(&P.chirp[k]));
+    __syncthreads();
+    return r2;
+}
+
 // Device twiddles and radix list of one length, cached per (device, n) for
-// the life of the process (defined in bst.cu).
+// the life of the process (defined in bst.cu); lengths with a prime factor
+// above 7 carry the Bluestein tables.
 struct FftTable {
-    RadixList rl;
+    RadixList rl;                     // radices of n (direct lengths)
     float2 *tw = nullptr;
+    FftPlan plan;                     // any length
+    float2 *chirp = nullptr, *B = nullptr;
     ~FftTable();
 };
 const FftTable &fft_table(int device, int n);
+// Transform length the plan of n runs (n, or Bluestein's M); 0 if none fits 24 passes.
+int fft_plan_length(int n);
 
 }  // namespace raft

@@ -24,6 +24,8 @@
 #include "profile.hpp"
 #include "fft.cuh"
 
+#include <cooperative_groups.h>
+
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -116,6 +118,7 @@ void filter_spectrum_host(int geometry, int ftype, int Np, double paganin, doubl
 
 // ============================================================== host: plan
 constexpr size_t kFilterSmemMax = 220 * 1024;
+static int cluster_size_for(int Np, int *radix, int &nradix);
 
 bool build_filter_plan(FilterPlan &plan, int geometry, int ftype, int N, int pad, double paganin,
                        double reg, double offset, double pixel, int device)
@@ -127,11 +130,22 @@ bool build_filter_plan(FilterPlan &plan, int geometry, int ftype, int N, int pad
     plan.off = (pad * N) / 2;
     const int Np = plan.Np;
     plan.skip = (ftype == FILTER_NONE);
-    if (plan.skip) return true;
+    plan.cluster = 0;
+    if (plan.skip) {
+        // pad + copy only; rows beyond one CTA's shared memory go through the cluster kernel
+        if (2 * (size_t)fft_span(Np) * sizeof(float2) > kFilterSmemMax)
+            plan.cluster = cluster_size_for(Np, plan.radix, plan.nradix);
+        return true;
+    }
 
     const size_t smem = 2 * (size_t)fft_span(Np) * sizeof(float2);   // ping-pong buffers
     plan.fft = factorize(Np, plan.radix, plan.nradix) && smem <= kFilterSmemMax;
     plan.threads = fft_threads(Np);
+    if (!plan.fft) {
+        // too long for one CTA: a cluster of CTAs, m = Np / C points each
+        plan.cluster = cluster_size_for(Np, plan.radix, plan.nradix);
+        plan.fft = plan.cluster > 0;
+    }
     std::vector<double> hre(Np), him(Np);
     filter_spectrum_host(geometry, ftype, Np, paganin, reg, offset, pixel, hre.data(), him.data());
     if (plan.fft) {
@@ -176,7 +190,45 @@ struct PackArgs {
     void *out;
     const float *wt;
     int nangles, wlo, Wg, store, Np;
+    int il;        // 1: rows interleaved by slice in groups of four ([group][angle][Wg][4], 4-byte elements)
 };
+
+// Rows are filtered in pairs of neighbouring angles of one slice (the real and
+// imaginary parts of one complex transform); a slice with an odd number of
+// angles ends with a single row.  Pairs never mix slices, so a slice's result
+// does not depend on the batch it came in.  For interleaved output the four
+// slices of a group are the four fastest-varying CTAs, so the stores that
+// fill each 16-byte element of the output arrive together.
+struct RowPair {
+    int k, a0;      // slice, first angle (a0 + 1 is the second row when it exists)
+};
+__device__ __forceinline__ RowPair row_pair(int p, int nangles, int il)
+{
+    const int PA = (nangles + 1) / 2;
+    RowPair rp;
+    if (il) {
+        const int rest = p >> 2;
+        rp.k = 4 * (rest / PA) + (p & 3);
+        rp.a0 = 2 * (rest % PA);
+    } else {
+        rp.k = p / PA;
+        rp.a0 = 2 * (p % PA);
+    }
+    return rp;
+}
+// Row pairs (CTAs) one filter launch over nslices slices runs.
+static inline long long row_pairs(int nslices, int nangles, int il)
+{
+    const long long PA = (nangles + 1) / 2;
+    return il ? (long long)((nslices + 3) / 4) * 4 * PA : (long long)nslices * PA;
+}
+
+// Index of window element e of (slice k, angle a) in the output rows.
+__device__ __forceinline__ size_t out_index(const PackArgs &a, int k, int ang, int e)
+{
+    return a.il ? (((size_t)(k >> 2) * a.nangles + ang) * a.Wg + e) * 4 + (k & 3)
+                : ((size_t)k * a.nangles + ang) * a.Wg + e;
+}
 
 __device__ __forceinline__ float row_value(const float2 *z, int u, int Np, int part)
 {
@@ -185,40 +237,60 @@ __device__ __forceinline__ float row_value(const float2 *z, int u, int Np, int p
     return part == 0 ? c.x : -c.y;
 }
 
-// Write window row `row` (part 0: real part, 1: negated imaginary part) of the
-// filtered padded row held in z, scaled by the angle weight.
-__device__ __forceinline__ void pack_row(const float2 *z, int row, int part, const PackArgs &a)
+// Store window element e of (slice k, angle ang) from the filtered samples
+// v0 = row[u], v1 = row[u + 1] (already weighted).
+__device__ __forceinline__ void store_elem(const PackArgs &a, int k, int ang, int e, float v0, float v1)
 {
-    const float w = a.wt ? a.wt[row % a.nangles] : 1.f;
-    const size_t rb = (size_t)row * a.Wg;
+    const size_t o = out_index(a, k, ang, e);
+    if (a.store == STORE_F32) {
+        reinterpret_cast<float *>(a.out)[o] = v0;
+    } else {
+        const float mid = 0.5f * (v0 + v1), dif = v1 - v0;
+        if (a.store == STORE_PAIR_F32)
+            reinterpret_cast<float2 *>(a.out)[o] = make_float2(mid, dif);
+        else
+            reinterpret_cast<__nv_bfloat162 *>(a.out)[o] = __floats2bfloat162_rn(mid, dif);
+    }
+}
+
+// Write the window row of (slice k, angle ang) (part 0: real part, 1: negated
+// imaginary part) of the filtered padded row held in z, scaled by the angle weight.
+__device__ __forceinline__ void pack_row(const float2 *z, int k, int ang, int part, const PackArgs &a)
+{
+    const float w = a.wt ? a.wt[ang] : 1.f;
     for (int e = threadIdx.x; e < a.Wg; e += blockDim.x) {
         const int u = a.wlo + e;
         const float v0 = row_value(z, u, a.Np, part) * w;
-        if (a.store == STORE_F32) {
-            reinterpret_cast<float *>(a.out)[rb + e] = v0;
-        } else {
-            const float v1 = row_value(z, u + 1, a.Np, part) * w;
-            const float mid = 0.5f * (v0 + v1), dif = v1 - v0;
-            if (a.store == STORE_PAIR_F32)
-                reinterpret_cast<float2 *>(a.out)[rb + e] = make_float2(mid, dif);
-            else
-                reinterpret_cast<__nv_bfloat162 *>(a.out)[rb + e] = __floats2bfloat162_rn(mid, dif);
-        }
+        const float v1 = a.store == STORE_F32 ? 0.f : row_value(z, u + 1, a.Np, part) * w;
+        store_elem(a, k, ang, e, v0, v1);
     }
+}
+
+// Zero window rows of a slice beyond the batch (interleaved output only: the
+// group's 16-byte elements are read whole).
+__device__ __forceinline__ void zero_rows(int k, int a0, const PackArgs &a)
+{
+    for (int ang = a0; ang < min(a0 + 2, a.nangles); ang++)
+        for (int e = threadIdx.x; e < a.Wg; e += blockDim.x) store_elem(a, k, ang, e, 0.f, 0.f);
 }
 
 // ================================================== kernel: FFT filter
 // two CTAs per SM (registers capped at 64: two 512-thread CTAs, or 384 + 384)
 __global__ void __launch_bounds__(512, 2)
-filter_fft_kernel(const float *__restrict__ sino, int N, int Np, int off, int nrows,
+filter_fft_kernel(const float *__restrict__ sino, int N, int Np, int off, int nslices,
                   const float2 *__restrict__ H, const float2 *__restrict__ tw, RadixList rl,
                   PackArgs pk, int skip, float *lowpass_out)
 {
     extern __shared__ float2 smem_fft[];
     float2 *z = smem_fft;
     float2 *zb = smem_fft + fft_span(Np);
-    const int r0 = 2 * blockIdx.x, r1 = r0 + 1;
-    const bool has1 = r1 < nrows;
+    const RowPair rp = row_pair(blockIdx.x, pk.nangles, pk.il);
+    if (rp.k >= nslices) {
+        zero_rows(rp.k, rp.a0, pk);
+        return;
+    }
+    const int r0 = rp.k * pk.nangles + rp.a0, r1 = r0 + 1;
+    const bool has1 = rp.a0 + 1 < pk.nangles;
     const float *s0 = sino + (size_t)r0 * N;
     const float *s1 = sino + (size_t)r1 * N;
     // edge-replicating pad (padding.cu:140-178) of both rows into one complex row
@@ -253,19 +325,225 @@ filter_fft_kernel(const float *__restrict__ sino, int N, int Np, int off, int nr
         }
         return;
     }
-    pack_row(z, r0, 0, pk);
-    if (has1) pack_row(z, r1, 1, pk);
+    pack_row(z, rp.k, rp.a0, 0, pk);
+    if (has1) pack_row(z, rp.k, rp.a0 + 1, 1, pk);
+}
+
+// ============================================ kernel: cluster FFT filter
+// Padded rows too long for one CTA's shared memory (two ping-pong buffers of
+// Np complex values) are filtered by a cluster of C CTAs (thread-block
+// cluster, distributed shared memory), each holding m = Np / C values, with a
+// four-step decomposition Np = m * C that needs only two exchanges between
+// the CTAs:
+//   forward  X[k1 + m k2] = sum_i2 W_C^(i2 k2) W_Np^(i2 k1) FFT_m(x[C i1 + i2])[k1]
+//   inverse  (a forward transform of the conjugate, conjugated)
+//            y[C i1 + i2] = FFT_m over k1 of W_Np^(i2 k1) sum_k2 W_C^(i2 k2) X'[k1 + m k2]
+// CTA rank r holds the row in the strided order x[C i1 + r] (i1 < m), so the
+// m-point transforms are local; the C-point transforms of the middle step run
+// in registers, one k1 per thread over this CTA's block of k1, reading the C
+// values from the C CTAs' shared memory; the spectral multiply (weight,
+// axis-shift phase, normalisation) sits between the forward and the inverse
+// C-point transforms in the same registers.  The results are bit-for-bit
+// independent of which CTA computed them, but not of C: a row is filtered
+// identically by every launch of the same length.
+template <int C>
+__device__ __forceinline__ void small_dft(float2 (&v)[C])
+{
+    if constexpr (C == 2 || C == 3 || C == 4 || C == 5 || C == 7 || C == 8) {
+        Dft<C>::run(v);
+    } else {
+        float2 in[C];
+#pragma unroll
+        for (int r = 0; r < C; r++) in[r] = v[r];
+#pragma unroll
+        for (int q = 0; q < C; q++) {
+            float2 acc = in[0];
+#pragma unroll
+            for (int r = 1; r < C; r++) {
+                float sn, cs;
+                sincospif(-2.0f * (float)((r * q) % C) / (float)C, &sn, &cs);
+                acc = cadd(acc, cmul(in[r], make_float2(cs, sn)));
+            }
+            v[q] = acc;
+        }
+    }
+}
+
+// exp(-2 pi i e / n) for an integer exponent 0 <= e < n
+__device__ __forceinline__ float2 root_of_unity(int e, int n)
+{
+    float sn, cs;
+    sincospif(-2.0f * (float)e / (float)n, &sn, &cs);
+    return make_float2(cs, sn);
+}
+
+// Elements of one of the cluster kernel's two buffers: the m-point transform's
+// span, and at least the C * ceil(m / C) values of the middle step.
+__host__ __device__ inline int cluster_span(int m, int C) { return max(fft_span(m), C * ((m + C - 1) / C)); }
+
+template <int C>
+__global__ void __launch_bounds__(512)
+filter_fft_cluster_kernel(const float *__restrict__ sino, int N, int Np, int off, int nslices,
+                          const float2 *__restrict__ H, RadixList rl, PackArgs pk, int skip, float *lowpass_out)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const int m = Np / C, T = blockDim.x, tid = threadIdx.x;
+    extern __shared__ float2 smem_fft[];
+    float2 *bufA = smem_fft, *bufB = smem_fft + cluster_span(m, C);
+    const RowPair rp = row_pair(blockIdx.x / C, pk.nangles, pk.il);
+    if (rp.k >= nslices) {        // the whole cluster: no cluster barrier is reached
+        if (rank == 0) zero_rows(rp.k, rp.a0, pk);
+        return;
+    }
+    const int r0 = rp.k * pk.nangles + rp.a0, r1 = r0 + 1;
+    const bool has1 = rp.a0 + 1 < pk.nangles;
+    const float *s0 = sino + (size_t)r0 * N;
+    const float *s1 = sino + (size_t)r1 * N;
+    // edge-replicating pad (padding.cu:140-178), this CTA's strided share
+    for (int i1 = tid; i1 < m; i1 += T) {
+        int i = C * i1 + rank - off;
+        i = i < 0 ? 0 : (i > N - 1 ? N - 1 : i);
+        bufA[i1] = make_float2(__ldg(&s0[i]), has1 ? __ldg(&s1[i]) : 0.f);
+    }
+    __syncthreads();
+    float2 *R = bufA;
+    if (skip) {
+        // no transform: match the conjugation convention of the output step
+        for (int i1 = tid; i1 < m; i1 += T) bufA[i1].y = -bufA[i1].y;
+    } else {
+    float2 *Y = fft_forward(bufA, bufB, m, rl, nullptr);     // plain order, same buffer in every CTA
+    float2 *Wb = (Y == bufA) ? bufB : bufA;
+    cl.sync();
+    // middle step for this CTA's block of k1: gather the C values, forward
+    // C-point DFT (with the W_Np^(i2 k1) twiddles), spectral multiply and
+    // conjugation, C-point DFT and twiddles of the inverse
+    const int kb = (m + C - 1) / C, k1s = rank * kb, k1e = min(m, k1s + kb);
+    for (int k1 = k1s + tid; k1 < k1e; k1 += T) {
+        float2 v[C];
+#pragma unroll
+        for (int i2 = 0; i2 < C; i2++) {
+            const float2 y = cl.map_shared_rank(Y, i2)[k1];
+            v[i2] = i2 ? cmul(y, root_of_unity(i2 * k1, Np)) : y;
+        }
+        small_dft<C>(v);
+#pragma unroll
+        for (int k2 = 0; k2 < C; k2++) {
+            const float2 g = cmul(v[k2], __ldg(&H[k1 + m * k2]));
+            v[k2] = make_float2(g.x, -g.y);
+        }
+        small_dft<C>(v);
+#pragma unroll
+        for (int i2 = 0; i2 < C; i2++)
+            Wb[(k1 - k1s) * C + i2] = i2 ? cmul(v[i2], root_of_unity(i2 * k1, Np)) : v[i2];
+    }
+    cl.sync();
+    // this CTA's i2 = rank: its values of every k1, from the CTA owning the k1
+    for (int k1 = tid; k1 < m; k1 += T) {
+        const int own = k1 / kb;
+        Y[k1] = cl.map_shared_rank(Wb, own)[(k1 - own * kb) * C + rank];
+    }
+    cl.sync();   // every CTA has read the Wb buffers before they are overwritten
+    R = fft_forward(Y, Wb, m, rl, nullptr);                  // conj of the filtered row, strided order
+    }
+    cl.sync();
+    // output: element u of the filtered row sits in CTA u % C at u / C
+    auto at = [&](int u) -> float2 {
+        return cl.map_shared_rank(R, u % C)[u / C];
+    };
+    if (lowpass_out) {
+        const int ib = (N + C - 1) / C;
+        for (int i = rank * ib + tid; i < min(N, (rank + 1) * ib); i += T) {
+            const float2 c = at(off + i);
+            lowpass_out[(size_t)r0 * N + i] = c.x;
+            if (has1) lowpass_out[(size_t)r1 * N + i] = -c.y;
+        }
+    } else {
+        const int eb = (pk.Wg + C - 1) / C;
+        const int e0 = rank * eb, e1 = min(pk.Wg, e0 + eb);
+        for (int part = 0; part < (has1 ? 2 : 1); part++) {
+            const int ang = rp.a0 + part;
+            const float w = pk.wt ? pk.wt[ang] : 1.f;
+            for (int e = e0 + tid; e < e1; e += T) {
+                const int u = pk.wlo + e;
+                auto val = [&](int v) -> float {
+                    if (v < 0 || v >= Np) return 0.f;
+                    const float2 c = at(v);
+                    return (part == 0 ? c.x : -c.y) * w;
+                };
+                store_elem(pk, rp.k, ang, e, val(u), pk.store == STORE_F32 ? 0.f : val(u + 1));
+            }
+        }
+    }
+    cl.sync();   // keep this CTA's shared memory until every CTA has read it
+}
+
+// Smallest cluster size C (2..8) for which Np = m * C with m a transform
+// length of the shared-memory FFT whose two buffers fit one CTA; 0 if none.
+static int cluster_size_for(int Np, int *radix, int &nradix)
+{
+    for (int C = 2; C <= 8; C++) {
+        if (Np % C) continue;
+        const int m = Np / C;
+        if (2 * (size_t)cluster_span(m, C) * sizeof(float2) > kFilterSmemMax) continue;
+        if (factorize(m, radix, nradix)) return C;
+    }
+    return 0;
+}
+
+template <int C>
+static void launch_cluster_filter(const FilterPlan &plan, const FilterLaunch &fl, const PackArgs &pk, float *lp,
+                                  cudaStream_t st)
+{
+    const int m = plan.Np / C;
+    const size_t smem = 2 * (size_t)cluster_span(m, C) * sizeof(float2);
+    RadixList rl;
+    rl.n = plan.nradix;
+    for (int i = 0; i < rl.n; i++) rl.r[i] = plan.radix[i];
+    RAFT_CUDA(cudaFuncSetAttribute(filter_fft_cluster_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)kFilterSmemMax));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(C * row_pairs(fl.nrows / fl.nangles, fl.nangles, pk.il)));
+    cfg.blockDim = dim3((unsigned)fft_threads(m));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    ProfScope ps(PROF_FILTER, st);
+    RAFT_CUDA(cudaLaunchKernelEx(&cfg, filter_fft_cluster_kernel<C>, fl.sino, plan.N, plan.Np, plan.off,
+                                 fl.nrows / fl.nangles,
+                                 (const float2 *)plan.d_H, rl, pk, plan.skip ? 1 : 0, lp));
 }
 
 // ============================================ kernel: direct convolution
 // Any Np (used when Np has a prime factor > 7 or does not fit shared memory).
 __global__ void __launch_bounds__(256)
-filter_direct_kernel(const float *__restrict__ sino, int N, int Np, int off, int nrows,
+filter_direct_kernel(const float *__restrict__ sino, int N, int Np, int off, int nslices,
                      const float *__restrict__ h, PackArgs pk, int skip, float *lowpass_out)
 {
     extern __shared__ float2 z[];   // z[u].x = padded row, then filtered value
     float *p = reinterpret_cast<float *>(z + Np);  // Np floats
-    const int row = blockIdx.x;
+    // one row per CTA; for interleaved output the group's four slices run side by side
+    int k, ang;
+    if (pk.il) {
+        const int rest = blockIdx.x >> 2;
+        k = 4 * (rest / pk.nangles) + (blockIdx.x & 3);
+        ang = rest % pk.nangles;
+    } else {
+        k = blockIdx.x / pk.nangles;
+        ang = blockIdx.x % pk.nangles;
+    }
+    if (k >= nslices) {
+        for (int e = threadIdx.x; e < pk.Wg; e += blockDim.x) store_elem(pk, k, ang, e, 0.f, 0.f);
+        return;
+    }
+    const int row = k * pk.nangles + ang;
     const float *s = sino + (size_t)row * N;
     for (int n = threadIdx.x; n < Np; n += blockDim.x) {
         int i = n - off;
@@ -292,7 +570,7 @@ filter_direct_kernel(const float *__restrict__ sino, int N, int Np, int off, int
         for (int i = threadIdx.x; i < N; i += blockDim.x) lowpass_out[(size_t)row * N + i] = z[off + i].x;
         return;
     }
-    pack_row(z, row, 0, pk);
+    pack_row(z, k, ang, 0, pk);
 }
 
 void launch_filter(const FilterPlan &plan, const FilterLaunch &fl, cudaStream_t st)
@@ -305,8 +583,25 @@ void launch_filter(const FilterPlan &plan, const FilterLaunch &fl, cudaStream_t 
     pk.Wg = fl.Wg;
     pk.store = fl.store;
     pk.Np = plan.Np;
+    pk.il = fl.interleaved;
     float *lp = fl.out_padded ? reinterpret_cast<float *>(fl.out) : nullptr;
     if (fl.nrows <= 0) return;
+    RAFT_CHECK(fl.nangles > 0 && fl.nrows % fl.nangles == 0, "filter: rows must be whole slices of nangles rows");
+    RAFT_CHECK(!fl.interleaved || (!lp && store_bytes(fl.store) == 4),
+               "filter: interleaved output takes 4-byte window elements");
+    const int nsl = fl.nrows / fl.nangles;
+    if (plan.cluster) {
+        switch (plan.cluster) {
+        case 2: launch_cluster_filter<2>(plan, fl, pk, lp, st); break;
+        case 3: launch_cluster_filter<3>(plan, fl, pk, lp, st); break;
+        case 4: launch_cluster_filter<4>(plan, fl, pk, lp, st); break;
+        case 5: launch_cluster_filter<5>(plan, fl, pk, lp, st); break;
+        case 6: launch_cluster_filter<6>(plan, fl, pk, lp, st); break;
+        case 7: launch_cluster_filter<7>(plan, fl, pk, lp, st); break;
+        default: launch_cluster_filter<8>(plan, fl, pk, lp, st); break;
+        }
+        return;
+    }
     if (plan.fft || plan.skip) {
         RadixList rl;
         rl.n = plan.skip ? 0 : plan.nradix;
@@ -323,17 +618,17 @@ void launch_filter(const FilterPlan &plan, const FilterLaunch &fl, cudaStream_t 
             configured_dev = dev;
         }
         ProfScope ps(PROF_FILTER, st);
-        filter_fft_kernel<<<(fl.nrows + 1) / 2, T, smem, st>>>(
-            fl.sino, plan.N, plan.Np, plan.off, fl.nrows, plan.d_H, plan.d_tw, rl, pk,
-            plan.skip ? 1 : 0, lp);
+        filter_fft_kernel<<<(unsigned)row_pairs(nsl, fl.nangles, pk.il), T, smem, st>>>(
+            fl.sino, plan.N, plan.Np, plan.off, nsl, plan.d_H, plan.d_tw, rl, pk, plan.skip ? 1 : 0, lp);
     } else {
         const size_t smem = (size_t)plan.Np * (sizeof(float2) + sizeof(float));
         RAFT_CHECK(smem <= kFilterSmemMax, "filter: padded row too long for the direct filter");
         RAFT_CUDA(cudaFuncSetAttribute(filter_direct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kFilterSmemMax));
         ProfScope ps(PROF_FILTER, st);
-        filter_direct_kernel<<<fl.nrows, 256, smem, st>>>(fl.sino, plan.N, plan.Np, plan.off, fl.nrows,
-                                                          plan.d_h, pk, 0, lp);
+        const unsigned rows = (unsigned)(pk.il ? (long long)((nsl + 3) / 4) * 4 * fl.nangles : fl.nrows);
+        filter_direct_kernel<<<rows, 256, smem, st>>>(fl.sino, plan.N, plan.Np, plan.off, nsl, plan.d_h, pk, 0,
+                                                      lp);
     }
     RAFT_CUDA(cudaGetLastError());
 }

@@ -24,10 +24,31 @@
 #include "raft.hpp"
 #include "profile.hpp"
 
+#include <cstdlib>
+
 namespace raft {
 
-constexpr int PJ_RAYS = 32;
-constexpr int PJ_ANGLES = 8;
+constexpr int PJ_WARPS = 8;   // 256 threads per block
+
+// Thread -> (ray, angle) shapes.  A warp covers RW neighbouring rays at 32/RW
+// neighbouring angles; a block covers BR rays x BA angles.  The lanes of a
+// warp load their samples together.  With one angle per warp (RW = 32) the
+// 32 pixels lie on a line across the ray direction, one pixel apart: along an
+// image row near 0 degrees, but on ~23 different rows (23 cache lines) near
+// 45 degrees.  Rays of neighbouring angles at the same detector position
+// sample points only |s| * dtheta apart (s = distance from the rotation
+// centre), so a warp of a few rays at several angles touches far fewer lines.
+// That is what limits single-slice projection (one 4-byte pixel per lane: the
+// L1 tag stage, one line per cycle); eight interleaved slices per lane (32
+// bytes) are bound by the L1 data stage instead, where one angle per warp
+// measured fastest.  Each thread still sums its own ray's samples in order,
+// so every shape gives the same bits.
+template <int RW> struct PjShape {
+    static constexpr int AW = 32 / RW;            // angles per warp
+    static constexpr int BR = RW >= 4 ? 32 : 16;  // rays per block
+    static constexpr int BA = 256 / BR;           // angles per block
+    static constexpr int WR = BR / RW;            // warps along the rays
+};
 
 __device__ __forceinline__ double warp_sum(double v)
 {
@@ -51,12 +72,14 @@ __device__ __forceinline__ void ldg_v8(const float *p, float (&w)[8])
                  : "l"(p));
 }
 
-template <int EM, int EPI, int S, int IL>
+template <int EM, int EPI, int S, int IL, int RW>
 __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx, const int by, const int bz)
 {
     static_assert(!IL || S == 8, "interleaved images hold groups of 8 slices");
-    const int i = bx * PJ_RAYS + threadIdx.x;     // ray
-    const int j = by * PJ_ANGLES + threadIdx.y;   // angle
+    using Sh = PjShape<RW>;
+    const int w = threadIdx.y, lane = threadIdx.x;
+    const int i = bx * Sh::BR + (w % Sh::WR) * RW + lane % RW;     // ray
+    const int j = by * Sh::BA + (w / Sh::WR) * Sh::AW + lane / RW;  // angle
     const int k0 = bz * S;                        // first slice
     const int nsl = min(S, p.nslices - k0);
     const bool valid = (i < p.nrays) && (j < p.nangles);
@@ -102,11 +125,15 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
 #pragma unroll
                         for (int q = 0; q < 8; q++) v[u][q] = w[q];
                     } else {
-                        const bool in = (X >= 0) & (X < limx) & (Y >= 0) & (Y < limy);
-                        const size_t off = (size_t)(in ? Y : 0) * sy + (size_t)(in ? X : 0) * sx;
-                        const float *pix = img + off;
+                        // 32-bit pixel index (the launch checks nx * ny < 2^32), predicated loads
+                        const bool in = ((unsigned)X < (unsigned)limx) & ((unsigned)Y < (unsigned)limy);
+                        const unsigned pix = (unsigned)Y * (unsigned)sy + (unsigned)X * (unsigned)sx;
 #pragma unroll
-                        for (int q = 0; q < S; q++) v[u][q] = (in && q < nsl) ? __ldg(pix + q * plane) : 0.f;
+                        for (int q = 0; q < S; q++) {
+                            float val = 0.f;
+                            if (in && q < nsl) val = __ldg(img + q * plane + pix);
+                            v[u][q] = val;
+                        }
                     }
                 }
 #pragma unroll
@@ -120,18 +147,17 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
                 const float y = __fmaf_rn(t, stheta, __fmul_rn(s, ctheta));
                 const int X = (int)((x + 1) / ddx);
                 const int Y = (int)((y + 1) / ddy);
-                if ((X >= 0) & (X < limx) & (Y >= 0) & (Y < limy)) {
-                    const size_t off = (size_t)Y * sy + (size_t)X * sx;
+                if (((unsigned)X < (unsigned)limx) & ((unsigned)Y < (unsigned)limy)) {
+                    const unsigned pix = (unsigned)Y * (unsigned)sy + (unsigned)X * (unsigned)sx;
                     if constexpr (IL) {
                         float w[8];
-                        ldg_v8(img + off * 8, w);
+                        ldg_v8(img + (size_t)pix * 8, w);
 #pragma unroll
                         for (int q = 0; q < S; q++) linesum[q] += w[q];
                     } else {
-                        const float *pix = img + off;
 #pragma unroll
                         for (int q = 0; q < S; q++)
-                            if (q < nsl) linesum[q] += __ldg(pix + q * plane);
+                            if (q < nsl) linesum[q] += __ldg(img + q * plane + pix);
                     }
                 }
             }
@@ -199,7 +225,7 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
     if constexpr (EPI != 0) {
         if (p.metrics) {
             // FP64 per-slice sums: warp shuffle, then across the block's warps
-            __shared__ double red[3][S][PJ_ANGLES];
+            __shared__ double red[3][S][PJ_WARPS];
 #pragma unroll
             for (int q = 0; q < S; q++) {
                 const double a0 = warp_sum(r2[q]), a1 = warp_sum(y2[q]), a2 = warp_sum(nll[q]);
@@ -214,7 +240,7 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
                 const int q = threadIdx.x / 3, c = threadIdx.x - 3 * q;
                 if (q < nsl) {
                     double sum = 0.0;
-                    for (int w = 0; w < PJ_ANGLES; w++) sum += red[c][q][w];
+                    for (int w = 0; w < PJ_WARPS; w++) sum += red[c][q][w];
                     atomicAdd(&p.metrics[(size_t)(k0 + q) * 3 + c], sum);
                 }
             }
@@ -222,17 +248,37 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
     }
 }
 
-template <int EM, int EPI, int S, int IL>
-__global__ void __launch_bounds__(PJ_RAYS * PJ_ANGLES)
+template <int EM, int EPI, int S, int IL, int RW>
+__global__ void __launch_bounds__(32 * PJ_WARPS)
 project_kernel(const ProjLaunch p)
 {
-    project_block<EM, EPI, S, IL>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    project_block<EM, EPI, S, IL, RW>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Shapes: eight interleaved slices per thread one angle per warp, fewer
+// slices (planar images, the ragged projector) four rays at eight angles per
+// warp.  RAFT_PJ_RW=32/16/8/4/2 forces one shape for the planar launches.
+constexpr int kPjRwIl = 32, kPjRwPlanar = 4;
+static int pj_rw_planar()
+{
+    static const int rw = [] {
+        const char *e = getenv("RAFT_PJ_RW");
+        const int v = e ? atoi(e) : kPjRwPlanar;
+        return (v == 32 || v == 16 || v == 8 || v == 4 || v == 2) ? v : kPjRwPlanar;
+    }();
+    return rw;
+}
+
+int project_blocks_per_slice(int nrays, int nangles)
+{
+    using Sh = PjShape<kPjRwPlanar>;
+    return ((nrays + Sh::BR - 1) / Sh::BR) * ((nangles + Sh::BA - 1) / Sh::BA);
 }
 
 // Ragged projector: one launch over many single-slice requests of different
 // sizes; block b belongs to the request r with blk_start[r] <= b < blk_start[r+1].
 template <int EM, int EPI>
-__global__ void __launch_bounds__(PJ_RAYS * PJ_ANGLES)
+__global__ void __launch_bounds__(32 * PJ_WARPS)
 project_ragged_kernel(const ProjLaunch *__restrict__ reqs, const int *__restrict__ blk_start, int nreq)
 {
     __shared__ int s_r;
@@ -249,8 +295,8 @@ project_ragged_kernel(const ProjLaunch *__restrict__ reqs, const int *__restrict
     const int r = s_r;
     const ProjLaunch &p = reqs[r];
     const int local = blockIdx.x - blk_start[r];
-    const int nbx = (p.nrays + PJ_RAYS - 1) / PJ_RAYS;
-    project_block<EM, EPI, 1, 0>(p, local % nbx, local / nbx, 0);
+    const int nbx = (p.nrays + PjShape<kPjRwPlanar>::BR - 1) / PjShape<kPjRwPlanar>::BR;
+    project_block<EM, EPI, 1, 0, kPjRwPlanar>(p, local % nbx, local / nbx, 0);
 }
 
 void launch_project_ragged(const ProjLaunch *d_reqs, const int *d_blk_start, int nreq, int total_blocks, int em,
@@ -258,7 +304,7 @@ void launch_project_ragged(const ProjLaunch *d_reqs, const int *d_blk_start, int
 {
     if (nreq <= 0 || total_blocks <= 0) return;
     ProfScope ps(PROF_PROJECT, st);
-    dim3 block(PJ_RAYS, PJ_ANGLES);
+    dim3 block(32, PJ_WARPS);
     if (!em) project_ragged_kernel<0, 0><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
     else if (epilogue == 1) project_ragged_kernel<1, 1><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
     else if (epilogue == 2) project_ragged_kernel<1, 2><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
@@ -371,23 +417,42 @@ void stage_proj_images(ProjLaunch &pl, void *scratch, cudaStream_t st)
     }
 }
 
+template <int EM, int EPI, int S, int IL, int RW>
+static void launch_project_shape(const ProjLaunch &pl, cudaStream_t st)
+{
+    using Sh = PjShape<RW>;
+    dim3 grid((pl.nrays + Sh::BR - 1) / Sh::BR, (pl.nangles + Sh::BA - 1) / Sh::BA, (pl.nslices + S - 1) / S);
+    project_kernel<EM, EPI, S, IL, RW><<<grid, dim3(32, PJ_WARPS), 0, st>>>(pl);
+}
+
+template <int EM, int EPI, int S>
+static void launch_project_planar(const ProjLaunch &pl, cudaStream_t st)
+{
+    switch (pj_rw_planar()) {
+    case 32: launch_project_shape<EM, EPI, S, 0, 32>(pl, st); break;
+    case 16: launch_project_shape<EM, EPI, S, 0, 16>(pl, st); break;
+    case 8: launch_project_shape<EM, EPI, S, 0, 8>(pl, st); break;
+    case 2: launch_project_shape<EM, EPI, S, 0, 2>(pl, st); break;
+    default: launch_project_shape<EM, EPI, S, 0, 4>(pl, st); break;
+    }
+}
+
 template <int EM, int EPI>
 static void launch_project_s(const ProjLaunch &pl, int S, cudaStream_t st)
 {
-    dim3 block(PJ_RAYS, PJ_ANGLES);
-    dim3 grid((pl.nrays + PJ_RAYS - 1) / PJ_RAYS, (pl.nangles + PJ_ANGLES - 1) / PJ_ANGLES,
-              (pl.nslices + S - 1) / S);
     ProfScope ps(PROF_PROJECT, st);
-    if (S == 8) project_kernel<EM, EPI, 8, 1><<<grid, block, 0, st>>>(pl);
-    else if (S == 4) project_kernel<EM, EPI, 4, 0><<<grid, block, 0, st>>>(pl);
-    else if (S == 2) project_kernel<EM, EPI, 2, 0><<<grid, block, 0, st>>>(pl);
-    else project_kernel<EM, EPI, 1, 0><<<grid, block, 0, st>>>(pl);
+    if (S == 8) launch_project_shape<EM, EPI, 8, 1, kPjRwIl>(pl, st);
+    else if (S == 4) launch_project_planar<EM, EPI, 4>(pl, st);
+    else if (S == 2) launch_project_planar<EM, EPI, 2>(pl, st);
+    else launch_project_planar<EM, EPI, 1>(pl, st);
     RAFT_CUDA(cudaGetLastError());
 }
 
 void launch_project(const ProjLaunch &pl, cudaStream_t st)
 {
     if (pl.nslices <= 0 || pl.nangles <= 0 || pl.nrays <= 0) return;
+    // the projector indexes a pixel of a plane in 32 bits
+    RAFT_CHECK((size_t)pl.nx * pl.ny <= 0xffffffffull, "projector: image plane above 2^32 pixels");
     RAFT_CHECK((pl.il == nullptr) == (pl.ilT == nullptr) && (pl.il == nullptr) == (pl.il_zero == nullptr),
                "projector: interleaved copies come with their transposed copy and zero pixel");
     const int S = pl.il ? 8 : (pl.nslices >= 4 ? 4 : (pl.nslices >= 2 ? 2 : 1));

@@ -79,6 +79,7 @@ enum FilterType : int {
 struct FilterPlan {
     int N = 0, Np = 0, pad = 0, off = 0;
     int fft = 0;                 // 1: mixed-radix FFT path, 0: direct circular convolution
+    int cluster = 0;             // > 1: FFT by a cluster of this many CTAs (radix = of Np / cluster)
     int nradix = 0;
     int radix[24] = {};
     int threads = 0;             // CTA size of the FFT kernel
@@ -104,6 +105,8 @@ struct FilterLaunch {
     int wlo = 0, Wg = 0;
     int store = STORE_F32;
     int out_padded = 0;            // lowpass: centre N bins, unweighted float
+    int interleaved = 0;           // 1: window rows interleaved by slice in groups of four
+                                   //    ([ceil(slices/4)][nangles][Wg][4], 4-byte elements, absent slices 0)
 };
 
 void launch_filter(const FilterPlan &plan, const FilterLaunch &fl, cudaStream_t st);
@@ -155,12 +158,18 @@ struct BpLaunch {
     const double *csd = nullptr, *snd = nullptr;  // FP64 angle tables
     int *err = nullptr;                           // device error flag
     // optional workspace of bp_il_bytes(): lets launches of four slices per
-    // CTA read the rows interleaved by slice (made here)
+    // CTA read the rows interleaved by slice (made here from filt)
     void *il_ws = nullptr;
+    // 1: il_ws already holds the rows interleaved by slice (filt unused);
+    //    only four-slice shapes run
+    int il_ready = 0;
 };
 
 void launch_backproject(const BpLaunch &bl, cudaStream_t st);
 size_t bp_il_bytes(int nslices, int nangles, int Wg, int esize);
+// True when RAFT_BP_TUNE forces a shape of fewer than four slices per CTA
+// (which reads plain, not interleaved, rows).
+bool bp_forced_planar();
 
 // Backprojector launch shape chosen by the autotuner: S slices per CTA
 // (sharing each pixel's position arithmetic) and AB angles per pipeline stage.
@@ -215,6 +224,8 @@ void launch_project(const ProjLaunch &pl, cudaStream_t st);
 // blk_start[r] <= b < blk_start[r+1] (device arrays).
 void launch_project_ragged(const ProjLaunch *d_reqs, const int *d_blk_start, int nreq, int total_blocks, int em,
                            int epilogue, cudaStream_t st);
+// Blocks the ragged projector runs for one single-slice request.
+int project_blocks_per_slice(int nrays, int nangles);
 
 // out[k][x][y] = in[k][y][x] for each of nslices planes.
 void launch_transpose(const float *in, float *out, int nx, int ny, int nslices, cudaStream_t st);

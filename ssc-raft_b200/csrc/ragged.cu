@@ -68,7 +68,8 @@ extern "C" int raft_ragged_device(int gpu, const raft_request *reqs, int nreq, i
     int em_iters = -1;
     for (int i = 0; i < nreq; i++) {
         const raft_request &q = reqs[i];
-        if ((q.kind != 0 && q.kind != 1) || q.nrays < 2 || q.nangles < 2 || !q.angles || !q.d_data || !q.d_out) {
+        if ((q.kind != 0 && q.kind != 1) || q.nrays < 2 || q.nrays > 65536 || q.nangles < 2 || !q.angles ||
+            !q.d_data || !q.d_out) {
             set_error("raft_ragged_device: request " + std::to_string(i) + " is invalid");
             return 1;
         }
@@ -246,7 +247,7 @@ extern "C" int raft_ragged_device(int gpu, const raft_request *reqs, int nreq, i
             p.windowed = 1;
             p.wlo = E[k].ep.win.wlo;
             p.Wg = E[k].ep.win.Wg;
-            blk[k + 1] = blk[k] + ((N + 31) / 32) * ((A + 7) / 8);
+            blk[k + 1] = blk[k] + project_blocks_per_slice(N, A);
         }
         RaggedBp rbF, rbD, rbU;
         if (!F.empty()) ragged_bp_prepare(rbF, bF.data(), (int)F.size(), geometry, store, ws + o_rb_fbp);

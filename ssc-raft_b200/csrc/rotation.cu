@@ -58,8 +58,7 @@ __global__ void cross_frame_kernel(float2 *f, float2 *g, const T *frame0, const 
 // data + r * seq_stride, element k at + k * elem_stride.  inverse: unnormalised
 // inverse (conjugate, forward, conjugate).
 __global__ void __launch_bounds__(512)
-fft_strided_kernel(float2 *data, int n, size_t seq_stride, size_t elem_stride, RadixList rl, const float2 *tw,
-                   int inverse)
+fft_strided_kernel(float2 *data, int n, size_t seq_stride, size_t elem_stride, FftPlan P, int inverse)
 {
     extern __shared__ float2 sm_rot[];
     float2 *base = data + (size_t)blockIdx.x * seq_stride;
@@ -68,7 +67,7 @@ fft_strided_kernel(float2 *data, int n, size_t seq_stride, size_t elem_stride, R
         sm_rot[k] = inverse ? make_float2(v.x, -v.y) : v;
     }
     __syncthreads();
-    const float2 *r = fft_forward(sm_rot, sm_rot + fft_span(n), n, rl, tw);
+    const float2 *r = fft_run(sm_rot, sm_rot + fft_plan_span(P), P);
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const float2 v = r[k];
         base[(size_t)k * elem_stride] = inverse ? make_float2(v.x, -v.y) : v;
@@ -163,14 +162,15 @@ __global__ void peak_subpixel_kernel(const float2 *f, int sizex, int sizey, unsi
 void fft2(int device, float2 *data, int sizex, int sizey, int inverse, cudaStream_t st)
 {
     const FftTable &tx = fft_table(device, sizex), &ty = fft_table(device, sizey);
-    const size_t smx = 2 * (size_t)fft_span(sizex) * sizeof(float2), smy = 2 * (size_t)fft_span(sizey) * sizeof(float2);
+    const size_t smx = 2 * (size_t)fft_plan_span(tx.plan) * sizeof(float2),
+                 smy = 2 * (size_t)fft_plan_span(ty.plan) * sizeof(float2);
     RAFT_CUDA(cudaFuncSetAttribute(fft_strided_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)std::max(smx, smy)));
     count_launch();
-    fft_strided_kernel<<<sizey, fft_threads(sizex), smx, st>>>(data, sizex, sizex, 1, tx.rl, tx.tw, inverse);
+    fft_strided_kernel<<<sizey, fft_threads(tx.plan.M), smx, st>>>(data, sizex, sizex, 1, tx.plan, inverse);
     RAFT_CUDA(cudaGetLastError());
     count_launch();
-    fft_strided_kernel<<<sizex, fft_threads(sizey), smy, st>>>(data, sizey, 1, sizex, ty.rl, ty.tw, inverse);
+    fft_strided_kernel<<<sizex, fft_threads(ty.plan.M), smy, st>>>(data, sizey, 1, sizex, ty.plan, inverse);
     RAFT_CUDA(cudaGetLastError());
 }
 
@@ -178,11 +178,10 @@ void fft2(int device, float2 *data, int sizex, int sizey, int inverse, cudaStrea
 
 bool centersino_shape_ok(int sizex, int sizey)
 {
-    int r[24], n = 0;
     const size_t lim = 227 * 1024;
-    return sizex >= 1 && sizey >= 1 && factorize(sizex, r, n) && factorize(sizey, r, n) &&
-           2 * (size_t)fft_span(sizex) * sizeof(float2) <= lim && 2 * (size_t)fft_span(sizey) * sizeof(float2) <= lim &&
-           (unsigned long long)sizex * sizey < 0xffffffffull;
+    const int Mx = fft_plan_length(sizex), My = fft_plan_length(sizey);
+    return sizex >= 1 && sizey >= 1 && Mx > 0 && My > 0 && 2 * (size_t)fft_span(Mx) * sizeof(float2) <= lim &&
+           2 * (size_t)fft_span(My) * sizeof(float2) <= lim && (unsigned long long)sizex * sizey < 0xffffffffull;
 }
 
 template <typename T>

@@ -43,8 +43,7 @@ struct FstArgs {
     float *model;           // [B][A][N]: flat * exp(-projection)
     const float *flat;      // [B][N]
     const float *cs, *sn;   // [A]
-    const float2 *tw;
-    RadixList rl;
+    FftPlan pL;             // L-point transforms
     int N, A, L, interp;
     float scale;
 };
@@ -64,7 +63,7 @@ __global__ void __launch_bounds__(512) fst_rows_kernel(const FstArgs p)
         sm_fst[c] = make_float2(v, 0.f);
     }
     __syncthreads();
-    const float2 *r = fft_forward(sm_fst, sm_fst + fft_span(L), L, p.rl, p.tw);
+    const float2 *r = fft_run(sm_fst, sm_fst + fft_plan_span(p.pL), p.pL);
     float2 *dst = p.rows + ((size_t)b * N + q) * L;
     for (int c = threadIdx.x; c < L; c += blockDim.x) dst[c] = r[c];
 }
@@ -79,7 +78,7 @@ __global__ void __launch_bounds__(512) fst_cols_kernel(const FstArgs p)
     const float2 *col = p.rows + (size_t)b * N * L + c;
     for (int q = threadIdx.x; q < N; q += blockDim.x) sm_fst[q < h ? q : q + L - N] = col[(size_t)q * L];
     __syncthreads();
-    const float2 *r = fft_forward(sm_fst, sm_fst + fft_span(L), L, p.rl, p.tw);
+    const float2 *r = fft_run(sm_fst, sm_fst + fft_plan_span(p.pL), p.pL);
     float2 *dst = p.spec + ((size_t)b * L + c) * L;
     for (int y = threadIdx.x; y < L; y += blockDim.x) dst[y] = r[y];
 }
@@ -139,7 +138,7 @@ __global__ void __launch_bounds__(512) fst_sino_kernel(const FstArgs p)
         sm_fst[qq] = make_float2(v.x, -v.y);               // conjugate: inverse = conj(forward(conj))
     }
     __syncthreads();
-    const float2 *H = fft_forward(sm_fst, sm_fst + fft_span(L), L, p.rl, p.tw);
+    const float2 *H = fft_run(sm_fst, sm_fst + fft_plan_span(p.pL), p.pL);
     const float *fl = p.flat + (size_t)b * N;
     float *out = p.model + ((size_t)b * p.A + a) * N;
     for (int i = threadIdx.x; i < N; i += blockDim.x) {
@@ -176,8 +175,8 @@ bool temfq_shape_ok(int N, int A, int zpad)
     const int L = N * (1 + zpad);
     if ((N * (zpad + 1)) % 2) return false;
     BstCore c = temfq_bst_core(N, A, zpad);
-    int r[24], n = 0;
-    return factorize(L, r, n) && 2 * (size_t)fft_span(L) * sizeof(float2) <= 227 * 1024 && bst_core_ok(c);
+    const int M = fft_plan_length(L);
+    return M > 0 && 2 * (size_t)fft_span(M) * sizeof(float2) <= 227 * 1024 && bst_core_ok(c);
 }
 
 BstCore temfq_bst_core(int N, int A, int zpad)
@@ -218,8 +217,9 @@ void temfq_run(int device, const TemfqConfig &cfg, float *d_obj, const float *d_
                const float *d_cs, const float *d_sn, int nslices, void *workspace, cudaStream_t st)
 {
     const int N = cfg.nrays, A = cfg.nangles, zpad = cfg.zpad, L = N * (1 + zpad);
-    RAFT_CHECK(temfq_shape_ok(N, A, zpad), "tEMFQ: unsupported sizes (N even; N(1+zpad) and N(1+zpad)/2 with "
-                                           "prime factors 2, 3, 5, 7 only; N(1+zpad) <= 14528)");
+    RAFT_CHECK(temfq_shape_ok(N, A, zpad), "tEMFQ: unsupported sizes (N even; the N(1+zpad)- and N(1+zpad)/2-point "
+                                           "transforms must fit shared memory: N(1+zpad) <= 14528 with prime factors "
+                                           "2, 3, 5, 7, about 7000 otherwise)");
     if (nslices <= 0) return;
     const size_t B = nslices, n_img = B * N * N;
     auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
@@ -253,16 +253,15 @@ void temfq_run(int device, const TemfqConfig &cfg, float *d_obj, const float *d_
     f.flat = d_flat;
     f.cs = d_cs;
     f.sn = d_sn;
-    f.tw = t.tw;
-    f.rl = t.rl;
+    f.pL = t.plan;
     f.N = N;
     f.A = A;
     f.L = L;
     f.interp = cfg.interpolation;
     // em_frequency.cu:166: dx / L, or 1 / L when dx <= 0 (the latter in double)
     f.scale = cfg.dx > 0.f ? cfg.dx / (float)L : (float)(1.0 / (float)L);
-    const size_t sm = 2 * (size_t)fft_span(L) * sizeof(float2);
-    const int threads = fft_threads(L);
+    const size_t sm = 2 * (size_t)fft_plan_span(f.pL) * sizeof(float2);
+    const int threads = fft_threads(f.pL.M);
     RAFT_CUDA(cudaFuncSetAttribute(fst_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     RAFT_CUDA(cudaFuncSetAttribute(fst_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     RAFT_CUDA(cudaFuncSetAttribute(fst_sino_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));

@@ -71,8 +71,9 @@ def bstGPU(tomogram, angles, gpus, dic, obj=None, nstreams=0):
     reference): same dictionary as fbpGPU; the rotation axis offset is
     truncated to an integer and the angles must be uniform over [0, pi)
     (fbp() passes linspace(0, pi, A, endpoint=False)).  The padded length
-    N*(1+padding) must have only the prime factors 2, 3, 5, 7 (and be at most
-    9472).  Returns obj [slices, N, N] (written in place when given)."""
+    N*(1+padding) must fit the shared-memory transforms: at most 14528 when its
+    prime factors are 2, 3, 5, 7, about 7000 otherwise (Bluestein's algorithm).
+    Returns obj [slices, N, N] (written in place when given)."""
     gpus_arr, ngpus = _gpus(gpus)
     nrays = tomogram.shape[-1]
     nangles = tomogram.shape[-2]

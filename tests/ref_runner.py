@@ -2,7 +2,7 @@
 from the reference's own CUDA sources) in a process of its own, so that its
 exports never meet this repository's libraft.so in one address space.
 
-    python tests/ref_runner.py fbp IN.npz OUT.npz
+    python tests/ref_runner.py fbp|bst IN.npz OUT.npz
 
 IN.npz holds the arguments with the reference's packing (`sino`, `angles`,
 `paramf`, `parami`); OUT.npz receives `out`.  Test infrastructure only."""
@@ -36,10 +36,25 @@ def run_fbp(d):
     return obj
 
 
+def run_bst(d):
+    """getBSTMultiGPU (bst.cu:674-734) on GPU 0 with host buffers."""
+    lib = ctypes.CDLL(REF_LIB)
+    P, I = ctypes.c_void_p, ctypes.c_int
+    lib.getBSTMultiGPU.argtypes = [P, I, P, P, P, P, P, I]
+    sino = np.ascontiguousarray(d["sino"], np.float32)
+    ang = np.ascontiguousarray(d["angles"], np.float32)
+    pf = np.ascontiguousarray(d["paramf"], np.float32)
+    pi = np.ascontiguousarray(d["parami"], np.int32)
+    obj = np.zeros((sino.shape[0], int(pi[3]), int(pi[3])), np.float32)
+    g = np.array([0], np.intc)
+    lib.getBSTMultiGPU(_p(g), 1, _p(obj), _p(sino), _p(ang), _p(pf), _p(pi), 0)
+    return obj
+
+
 def main():
     kind, src, dst = sys.argv[1:4]
     d = np.load(src)
-    out = {"fbp": run_fbp}[kind](d)
+    out = {"fbp": run_fbp, "bst": run_bst}[kind](d)
     np.savez(dst, out=out)
 
 

@@ -5,7 +5,8 @@ Tolerances: rel-L2 <= 5e-6 against the reference library's own outputs
 (fixtures with nangles == nrays; measured <= 4.7e-7) and <= 1e-5 against the
 FP64 oracle; the regridding geometry is float in all three, the FFTs float
 here and in the reference, FP64 in the oracle.
-Chunked / whole / device-entry runs are bit-identical."""
+Chunked / whole / device-entry runs are bit-identical.  Lengths with a prime
+factor above 7 (Bluestein transforms): <= 1e-5 against both."""
 import ctypes
 import glob
 import os
@@ -73,7 +74,58 @@ def test_bst_python_entry_and_chunking():
     assert np.array_equal(d_out.cpu().numpy(), whole)
 
 
-def test_bst_unsupported_length_raises():
-    sino = np.zeros((1, 11, 11), np.float32)
+def test_bst_prime_factor_length_vs_oracle_and_reference(oracle, tmp_path):
+    """N = 88 = 8 x 11 at padding 2: 264-point transforms by Bluestein's
+    algorithm (the reference runs them through cuFFT), vs the FP64 oracle and
+    the reference's own getBSTMultiGPU in a fresh process."""
+    import subprocess
+    import sys
+    from conftest import REF_LIB, REPO
+    N = A = 88
+    ang = np.linspace(0, np.pi, A, endpoint=False).astype(np.float32)
+    sino, _ = sino_case(N, A, 2, seed=88, angles=ang)
+    out = _bst(sino, 2, 5, 1)
+    ref = oracle.bst(sino, 5, 2, offset=1)
+    assert rel_l2(out, ref) <= 1e-5, rel_l2(out, ref)
+    if not os.path.exists(REF_LIB):
+        pytest.skip("reference library not built (oracle/build_ref.sh)")
+    pf, pi = fbp_params(N, A, 2, pad=2, ftype=5, offset=1.0)
+    src, dst = tmp_path / "in.npz", tmp_path / "out.npz"
+    np.savez(src, sino=sino, angles=ang, paramf=pf, parami=pi)
+    subprocess.run([sys.executable, os.path.join(REPO, "tests", "ref_runner.py"), "bst", str(src), str(dst)],
+                   check=True, timeout=600)
+    err = rel_l2(out, np.load(dst)["out"])
+    assert err <= 1e-5, err
+
+
+def test_bst_too_long_length_raises():
+    sino = np.zeros((1, 4, 3671), np.float32)
     with pytest.raises(RuntimeError):
-        _bst(sino, 0, 7)                     # Np = 11 has a prime factor above 7
+        _bst(sino, 1, 7)                     # Np = 2 x 3671: its transform would not fit shared memory
+
+
+def test_bst_4096_pad2_vs_reference_library(tmp_path):
+    """A 4096-bin detector at the default padding 2 (12288-point transforms,
+    above what one CTA held before the row kernel parked the second row's
+    half-rays): vs the reference's own getBSTMultiGPU on the same inputs, run
+    in a fresh process (its half-ray padding is freshly allocated device
+    memory, zero there); angles = rays, as the reference's padding needs."""
+    import subprocess
+    import sys
+    from conftest import REF_LIB, REPO
+    N = A = 4096
+    ang = np.linspace(0, np.pi, A, endpoint=False).astype(np.float32)
+    sino, _ = sino_case(N, A, 1, seed=4096, angles=ang, n_ell=12)
+    out = _bst(sino, 2, 5, 1)
+    assert np.all(np.isfinite(out))
+    if not os.path.exists(REF_LIB):
+        pytest.skip("reference library not built (oracle/build_ref.sh)")
+    pf, pi = fbp_params(N, A, 1, pad=2, ftype=5, offset=1.0)
+    src, dst = tmp_path / "in.npz", tmp_path / "out.npz"
+    np.savez(src, sino=sino, angles=ang, paramf=pf, parami=pi)
+    subprocess.run([sys.executable, os.path.join(REPO, "tests", "ref_runner.py"), "bst", str(src), str(dst)],
+                   check=True, timeout=600)
+    ref = np.load(dst)["out"]
+    err = rel_l2(out, ref)
+    print(f"BST 4096^2 pad 2 vs reference library: rel-L2 {err:.3e}")
+    assert err <= 1e-5, err

@@ -73,8 +73,17 @@ def test_rotaxis_correction_vs_reference_and_oracle(oracle):
             assert rel_l2(out, oracle.rotaxis(d["tomo"], float(off))) <= 1e-5
 
 
-def test_centersino_unsupported_size_raises():
+@pytest.mark.parametrize("sizex,sizey,axis", [(176, 44, 80.0), (143, 64, 70.5)])
+def test_centersino_prime_factor_sizes_vs_oracle(oracle, sizex, sizey, axis):
+    # 176 = 16 x 11, 44 = 4 x 11, 143 = 11 x 13: Bluestein transforms
     from sscRaft.processing import Centersino
-    z = np.ones((10, 11), np.float32)
+    from golden.make_golden import frame_pair
+    f0, f1, dk, ft = frame_pair(sizex, sizey, axis, seed=sizex + sizey)
+    assert Centersino(f0, f1, ft, dk) == oracle.centersino(f0, f1, dk, ft)
+
+
+def test_centersino_too_long_size_raises():
+    from sscRaft.processing import Centersino
+    z = np.ones((10, 7919), np.float32)      # 7919 is prime: its transform would not fit shared memory
     with pytest.raises(RuntimeError):
         Centersino(z, z, z, z)

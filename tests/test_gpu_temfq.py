@@ -9,7 +9,8 @@ are float here (own FFT) and in the reference (cuFFT), FP64 in the oracle,
 and the EM update multiplies their rounding into the object each iteration.
 Nearest-neighbour cases use angle sets whose samples stay at least 4e-4 away
 from a rounding tie, so the fast and the libm cosine pick the same sample.
-Chunked, whole, Python and device-entry runs are bit-identical."""
+Chunked, whole, Python and device-entry runs are bit-identical.  Lengths with
+a prime factor above 7 (Bluestein transforms): <= 2e-5 against the oracle."""
 import ctypes
 import glob
 import os
@@ -95,7 +96,16 @@ def test_temfq_chunking_python_and_device_entry():
     assert np.array_equal(d_counts.cpu().numpy(), counts)
 
 
-def test_temfq_unsupported_length_raises():
-    counts = np.ones((1, 8, 22), np.float32)
+def test_temfq_prime_factor_lengths_vs_oracle(oracle):
+    # N = 44 = 4 x 11, zpad 1: 88- and 44-point transforms by Bluestein's algorithm
+    counts, flat, ang = temfq_counts(44, 44, 1, 0.02, seed=44)
+    out = _temfq(counts, flat, ang, 1, 1, 3, 0.02)
+    ref = oracle.temfq(counts, flat, ang, 1, 1, 3, dx=0.02)
+    assert rel_l2(out, ref) <= 2e-5, rel_l2(out, ref)
+
+
+def test_temfq_too_long_length_raises():
+    # 7342 = 2 x 3671: Bluestein would need a transform beyond shared memory
+    counts = np.ones((1, 1, 7342), np.float32)
     with pytest.raises(RuntimeError):
-        _temfq(counts, np.ones((1, 22), np.float32), np.zeros(8, np.float32), 1, 1, 1, 0.0)   # 44 = 4 x 11
+        _temfq(counts, np.ones((1, 7342), np.float32), np.zeros(1, np.float32), 0, 1, 1, 0.0)
