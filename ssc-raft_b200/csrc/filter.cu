@@ -123,7 +123,6 @@ static int cluster_size_for(int Np, int *radix, int &nradix);
 bool build_filter_plan(FilterPlan &plan, int geometry, int ftype, int N, int pad, double paganin,
                        double reg, double offset, double pixel, int device)
 {
-    (void)device;
     plan.N = N;
     plan.pad = pad;
     plan.Np = N * (1 + pad);
@@ -141,10 +140,26 @@ bool build_filter_plan(FilterPlan &plan, int geometry, int ftype, int N, int pad
     const size_t smem = 2 * (size_t)fft_span(Np) * sizeof(float2);   // ping-pong buffers
     plan.fft = factorize(Np, plan.radix, plan.nradix) && smem <= kFilterSmemMax;
     plan.threads = fft_threads(Np);
+    plan.bs_M = 0;
     if (!plan.fft) {
         // too long for one CTA: a cluster of CTAs, m = Np / C points each
         plan.cluster = cluster_size_for(Np, plan.radix, plan.nradix);
         plan.fft = plan.cluster > 0;
+    }
+    if (!plan.fft) {
+        // a prime factor above 7: Bluestein's algorithm (two M-point transforms
+        // per direction) when its buffers fit one CTA, else direct convolution
+        const int M = fft_plan_length(Np);
+        if (M > 0 && 2 * (size_t)fft_span(M) * sizeof(float2) <= kFilterSmemMax) {
+            const FftTable &t = fft_table(device, Np);
+            plan.bs_M = M;
+            plan.bs_chirp = t.plan.chirp;
+            plan.bs_B = t.plan.B;
+            plan.nradix = t.plan.rl.n;
+            for (int i = 0; i < plan.nradix; i++) plan.radix[i] = t.plan.rl.r[i];
+            plan.threads = fft_threads(M);
+            plan.fft = 1;
+        }
     }
     std::vector<double> hre(Np), him(Np);
     filter_spectrum_host(geometry, ftype, Np, paganin, reg, offset, pixel, hre.data(), him.data());
@@ -278,12 +293,11 @@ __device__ __forceinline__ void zero_rows(int k, int a0, const PackArgs &a)
 // two CTAs per SM (registers capped at 64: two 512-thread CTAs, or 384 + 384)
 __global__ void __launch_bounds__(512, 2)
 filter_fft_kernel(const float *__restrict__ sino, int N, int Np, int off, int nslices,
-                  const float2 *__restrict__ H, const float2 *__restrict__ tw, RadixList rl,
-                  PackArgs pk, int skip, float *lowpass_out)
+                  const float2 *__restrict__ H, FftPlan P, PackArgs pk, int skip, float *lowpass_out)
 {
     extern __shared__ float2 smem_fft[];
     float2 *z = smem_fft;
-    float2 *zb = smem_fft + fft_span(Np);
+    float2 *zb = smem_fft + fft_plan_span(P);
     const RowPair rp = row_pair(blockIdx.x, pk.nangles, pk.il);
     if (rp.k >= nslices) {
         zero_rows(rp.k, rp.a0, pk);
@@ -301,7 +315,7 @@ filter_fft_kernel(const float *__restrict__ sino, int N, int Np, int off, int ns
     }
     __syncthreads();
     if (!skip) {
-        z = fft_forward(z, zb, Np, rl, tw);
+        z = fft_run(z, zb, P);
         // spectral multiply, then conjugate so that a second forward FFT
         // yields the conjugated inverse transform
         for (int k = threadIdx.x; k < Np; k += blockDim.x) {
@@ -309,8 +323,8 @@ filter_fft_kernel(const float *__restrict__ sino, int N, int Np, int off, int ns
             z[k] = make_float2(g.x, -g.y);
         }
         __syncthreads();
-        zb = (z == smem_fft) ? smem_fft + fft_span(Np) : smem_fft;
-        z = fft_forward(z, zb, Np, rl, tw);
+        zb = (z == smem_fft) ? smem_fft + fft_plan_span(P) : smem_fft;
+        z = fft_run(z, zb, P);
     } else {
         // no transform: match the conjugation convention of pack_row
         for (int k = threadIdx.x; k < Np; k += blockDim.x) z[k].y = -z[k].y;
@@ -603,11 +617,15 @@ void launch_filter(const FilterPlan &plan, const FilterLaunch &fl, cudaStream_t 
         return;
     }
     if (plan.fft || plan.skip) {
-        RadixList rl;
-        rl.n = plan.skip ? 0 : plan.nradix;
-        for (int i = 0; i < rl.n; i++) rl.r[i] = plan.radix[i];
+        FftPlan P;
+        P.n = plan.Np;
+        P.M = plan.bs_M > 0 ? plan.bs_M : plan.Np;
+        P.rl.n = plan.skip ? 0 : plan.nradix;
+        for (int i = 0; i < P.rl.n; i++) P.rl.r[i] = plan.radix[i];
+        P.chirp = plan.bs_chirp;
+        P.B = plan.bs_B;
         const int T = plan.skip ? 256 : plan.threads;
-        const size_t smem = 2 * (size_t)fft_span(plan.Np) * sizeof(float2);
+        const size_t smem = 2 * (size_t)fft_plan_span(P) * sizeof(float2);
         static thread_local int configured_dev = -1;
         int dev = 0;
         cudaGetDevice(&dev);
@@ -619,7 +637,7 @@ void launch_filter(const FilterPlan &plan, const FilterLaunch &fl, cudaStream_t 
         }
         ProfScope ps(PROF_FILTER, st);
         filter_fft_kernel<<<(unsigned)row_pairs(nsl, fl.nangles, pk.il), T, smem, st>>>(
-            fl.sino, plan.N, plan.Np, plan.off, nsl, plan.d_H, plan.d_tw, rl, pk, plan.skip ? 1 : 0, lp);
+            fl.sino, plan.N, plan.Np, plan.off, nsl, plan.d_H, P, pk, plan.skip ? 1 : 0, lp);
     } else {
         const size_t smem = (size_t)plan.Np * (sizeof(float2) + sizeof(float));
         RAFT_CHECK(smem <= kFilterSmemMax, "filter: padded row too long for the direct filter");

@@ -80,6 +80,8 @@ struct FilterPlan {
     int N = 0, Np = 0, pad = 0, off = 0;
     int fft = 0;                 // 1: mixed-radix FFT path, 0: direct circular convolution
     int cluster = 0;             // > 1: FFT by a cluster of this many CTAs (radix = of Np / cluster)
+    int bs_M = 0;                // > 0: Bluestein transforms of this length (radix = of bs_M)
+    const float2 *bs_chirp = nullptr, *bs_B = nullptr;   // Bluestein tables (cached per device and length)
     int nradix = 0;
     int radix[24] = {};
     int threads = 0;             // CTA size of the FFT kernel

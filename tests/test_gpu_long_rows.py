@@ -6,7 +6,9 @@ memory, four-step transform, C = the smallest of 2..8 that fits).  Vs the
 FP64 oracle: FBP nearest (given the GPU fast-intrinsic sin/cos values)
 rel-L2 <= 2e-5 (also with the 'none' filter, which only pads), linear FP32
 <= 1e-5, lowpass <= 1e-5; lowpass with 'none' leaves its input unchanged
-(the reference returns early).
+(the reference returns early).  Rows whose length has a prime factor above
+7 are transformed by Bluestein's algorithm, or, when its buffers do not fit,
+filtered by direct circular convolution: <= 2e-5 against the oracle.
 """
 import numpy as np
 import pytest
@@ -48,6 +50,21 @@ def test_fbp_long_rows_vs_oracle(N, A, ftype, offset, oracle):
         err = rel_l2(lin, ref)
         print(f"N={N} linear FP32 vs oracle: {err:.3e}")
         assert err <= 1e-5, err
+
+
+@pytest.mark.parametrize("N,A", [
+    (61, 20),       # Np = 183 = 3 x 61: Bluestein transforms (M = 375)
+    (2447, 8),      # Np = 7341 = 3 x 2447: Bluestein would not fit, direct circular convolution
+])
+def test_fbp_prime_factor_rows_vs_oracle(N, A, oracle):
+    from sscRaft.rafttypes import fast_sincos
+    sino, ang = sino_case(N, A, 1, seed=N + 1, n_ell=6)
+    pf, pi = fbp_params(N, A, 1, pad=2, ftype=5, offset=1.5)
+    out = _fbp(sino, ang, pf, pi)
+    ref = oracle.fbp(sino, ang, oracle.MODE_REF, 5, 2, offset=1.5, trig=fast_sincos(ang, 0))
+    err = rel_l2(out, ref)
+    print(f"N={N} (Np={3 * N}) nearest vs oracle: {err:.3e}")
+    assert err <= 2e-5, err
 
 
 def test_lowpass_long_rows_vs_oracle(oracle):

@@ -64,3 +64,52 @@ def test_two_rank_gloo_timing_and_seeds():
         assert p.exitcode == 0
     assert [r[1] for r in res] == [11.0, 11.0]
     assert res[0][2] + 512 <= res[1][2]               # disjoint per-rank slice seeds
+
+
+def _slab_worker(rank, world, port, out):
+    """One rank of a slab-split reconstruction: its slices (the C ABI's slab
+    partition), reconstructed by the FP64 oracle standing in for the rank's
+    GPU, gathered on every rank."""
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for p in ("ssc-raft_b200", "oracle", "tests"):
+        sys.path.insert(0, os.path.join(root, p))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import oracle
+    from helpers import sino_case
+    n, N, A = 5, 48, 40
+    sino, ang = sino_case(N, A, n, seed=77)
+    st, ct = part(n, world)
+    mine = oracle.fbp(sino[st[rank]:st[rank] + ct[rank]], ang, oracle.MODE_LIN, 5, 2) if ct[rank] else \
+        np.zeros((0, N, N))
+    parts = [None] * world
+    dist.all_gather_object(parts, (int(st[rank]), mine))
+    vol = np.zeros((n, N, N))
+    for s0, blk in parts:
+        vol[s0:s0 + len(blk)] = blk
+    out.put((rank, vol))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_slab_split_reconstruction_equals_whole():
+    import torch.multiprocessing as mp
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+    import oracle
+    from helpers import sino_case
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_slab_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=300) for _ in procs), key=lambda r: r[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    sino, ang = sino_case(48, 40, 5, seed=77)
+    whole = oracle.fbp(sino, ang, oracle.MODE_LIN, 5, 2)
+    for _, vol in res:
+        np.testing.assert_array_equal(vol, whole)
