@@ -336,6 +336,10 @@ bool conv3x3_tc_supported(int C0, int C1, int W);
 int conv3x3_tc(const void *x0, int C0, const void *x1, int C1, const void *w, const float *bias, void *y, void *y1,
                int Cy0, int N, int H, int W, int Cout, int relu, cudaStream_t st);
 int conv3x3_tc_error();
+// Weight (and bias) gradient of the 3x3 convolution on tcgen05 (unet_tc.cu);
+// 0 = launched, 1 = launch error, 2 = shape not handled (W % 64, Cout not 32/64/128/256).
+int conv3x3_wgrad_tc(const void *dy, const void *x0, int C0, const void *x1, int C1, float *dw, float *dbias, int N,
+                     int H, int W, int Cout, cudaStream_t st);
 void conv3x3_tc_set_halo(int on);
 
 }  // namespace raft

@@ -644,6 +644,11 @@ int raft_unet_conv_wgrad(const void *dy, const void *x0, int C0, const void *x1,
                          int N, int H, int W, int Cout, void *stream)
 {
     if (C0 % 32 || C1 % 32 || Cout % 32) return 1;
+    if (g_conv_path != 1) {
+        const int rc = conv3x3_wgrad_tc(dy, x0, C0, x1, C1, dw, dbias, N, H, W, Cout, (cudaStream_t)stream);
+        if (rc != 2) return rc;
+        if (g_conv_path == 2) return 1;
+    }
     const int Cin = C0 + C1;
     const long total = (long)N * H * W;
     const int ppc = 2048;

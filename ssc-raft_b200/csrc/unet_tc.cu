@@ -34,6 +34,7 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <mutex>
 
 namespace raft {
@@ -531,6 +532,351 @@ bool encode_w(CUtensorMap *m, const void *ptr, int Cout, int Cin, int KC, int BN
 
 bool g_halo = true;   // halo tiles for the 32 -> 32 channel layers (raft_unet_set_conv_halo)
 
+// =========================================================== weight gradient
+// dW[co][tap][ci] = sum over pixels p of dY[p][co] * X[p + tap][ci] as a GEMM
+// D[(tap, ci)][co] with K = pixels, on tcgen05 (M = 128 rows of (tap, ci),
+// N = Cout, K = 16, BF16 x BF16 -> FP32 in TMEM).  Both operands are NHWC
+// tensors whose contiguous dimension is the channel, while the MMA wants K
+// (the pixels) contiguous, so each k-block of 64 pixels (one image row
+// segment) is transposed in shared memory:
+//   * TMA lands four 32-channel input boxes (one (tap, channel chunk) each,
+//     the 3x3 shift and the border from the box coordinates and the TMA
+//     zero fill) and the dY box, with 64- or 128-byte swizzled rows;
+//   * four warps move them into the K-major 128-byte-swizzled operand
+//     layout with ldmatrix.trans (8x8 blocks out of the swizzled staging,
+//     conflict-free) and stmatrix (rows into the operand's swizzled chunks),
+//     then fence the generic-proxy writes for the tensor cores;
+//   * one thread issues four MMAs per k-block into one TMEM accumulator.
+// A CTA owns one 128-row block of D and a contiguous range of k-blocks; its
+// accumulator goes to a per-CTA partial, and a second kernel adds the
+// partials in a fixed order (deterministic; no atomics).  Warp roles as the
+// forward kernel: 0 TMA, 1 TMEM/MMA, 2-5 transpose, then epilogue.  Every
+// wait is bounded.
+constexpr int WG_KB = 64;       // pixels per k-block
+constexpr int WG_THREADS = 192;
+
+struct WgTcArgs {
+    int N, H, W, C0, C1, Cout;
+    int nchunks;                // 9 * Cin / 32 rows blocks of 32
+    int mtiles, splits;
+    long long kblocks, kper;    // N * H * (W / 64) k-blocks, per split
+    float *part;                // [splits][mtiles * 128][Cout]
+    int *err;
+};
+
+__device__ __forceinline__ void ldsm_x4_trans(uint32_t addr, uint32_t (&r)[4])
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr)
+                 : "memory");
+}
+
+__device__ __forceinline__ void stsm_x4(uint32_t addr, const uint32_t (&r)[4])
+{
+    asm volatile("stmatrix.sync.aligned.m8n8.x4.shared.b16 [%0], {%1,%2,%3,%4};" ::"r"(addr), "r"(r[0]), "r"(r[1]),
+                 "r"(r[2]), "r"(r[3])
+                 : "memory");
+}
+
+template <int BN, int ST>
+__global__ void __launch_bounds__(WG_THREADS, 1)
+    wgrad_tc_kernel(const __grid_constant__ CUtensorMap mx0, const __grid_constant__ CUtensorMap mx1,
+                    const __grid_constant__ CUtensorMap mdy, const WgTcArgs a)
+{
+    constexpr int STG_A = 4 * WG_KB * 64;           // four [64 px][32 ch] boxes, 64-byte rows
+    constexpr int STG_B = WG_KB * BN * 2;           // [64 px][BN ch]: one 64-byte-row box (BN 32) or
+                                                    // BN/64 boxes of 128-byte rows
+    constexpr int OP_A = 128 * 128, OP_B = BN * 128;
+    constexpr int STAGE = STG_A + STG_B + OP_A + OP_B;
+    static_assert(STAGE % 1024 == 0 && (BN == 32 || BN % 64 == 0) && BN <= 256, "stage layout");
+    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(TC_M >> 4) << 24);
+    constexpr uint32_t TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + ST * STAGE);
+    uint64_t *stg_empty = full + ST;
+    uint64_t *opfull = stg_empty + ST;
+    uint64_t *op_empty = opfull + ST;
+    uint64_t *accf = op_empty + ST;
+    uint64_t *drain = accf + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < ST; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&stg_empty[s], 4);
+            mbar_init(&opfull[s], 4);
+            mbar_init(&op_empty[s], 1);
+        }
+        mbar_init(accf, 1);
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    const int mtile = (int)(blockIdx.x % (unsigned)a.mtiles), split = (int)(blockIdx.x / (unsigned)a.mtiles);
+    const long long kb0 = (long long)split * a.kper;
+    const long long kb1 = kb0 + a.kper < a.kblocks ? kb0 + a.kper : a.kblocks;
+    const int nk = kb1 > kb0 ? (int)(kb1 - kb0) : 0;
+    const int cpt = (a.C0 + a.C1) / 32;            // channel chunks per tap
+    const int xbl = a.W / WG_KB;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ TMA
+        if (lane == 0) {
+            int nvalid = 0;
+            for (int c = 0; c < 4; ++c) nvalid += (mtile * 4 + c < a.nchunks) ? 1 : 0;
+            const uint32_t bytes = (uint32_t)(nvalid * WG_KB * 64 + STG_B);
+            bool ok = true;
+            int g = 0;
+            for (; g < nk && ok; ++g) {
+                const int s = g % ST;
+                const uint32_t u = (uint32_t)(g / ST);
+                if (u >= 1 && !(ok = tc_wait(&stg_empty[s], (u - 1) & 1, abort_flag, a.err))) break;
+                const long long kb = kb0 + g;
+                const int xb = (int)(kb % xbl);
+                const long long r = kb / xbl;
+                const int y = (int)(r % a.H), n = (int)(r / a.H), x0 = xb * WG_KB;
+                uint8_t *st = base + s * STAGE;
+                mbar_arrive_expect_tx(&full[s], bytes);
+                for (int c = 0; c < 4; ++c) {
+                    const int q = mtile * 4 + c;
+                    if (q >= a.nchunks) break;
+                    const int tap = q / cpt, ch = (q % cpt) * 32;
+                    const int ky = tap / 3 - 1, kx = tap % 3 - 1;
+                    if (ch < a.C0) tma_load_4d(st + c * WG_KB * 64, &mx0, ch, x0 + kx, y + ky, n, &full[s]);
+                    else tma_load_4d(st + c * WG_KB * 64, &mx1, ch - a.C0, x0 + kx, y + ky, n, &full[s]);
+                }
+                if (BN == 32) {
+                    tma_load_4d(st + STG_A, &mdy, 0, x0, y, n, &full[s]);
+                } else {
+                    for (int b = 0; b < BN / 64; ++b)
+                        tma_load_4d(st + STG_A + b * WG_KB * 128, &mdy, 64 * b, x0, y, n, &full[s]);
+                }
+            }
+            // every issued load lands before the CTA may exit
+            for (int s = 0; s < ST && s < g; ++s)
+                mbar_wait_bounded(&full[s], (uint32_t)((g - 1 - s) / ST) & 1, TC_WAIT_LIMIT);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA
+        if (lane == 0) {
+            bool ok = true;
+            for (int g = 0; g < nk && ok; ++g) {
+                const int s = g % ST;
+                const uint32_t u = (uint32_t)(g / ST);
+                if (!(ok = tc_wait(&opfull[s], u & 1, abort_flag, a.err))) break;
+                tc_fence_after();
+                const uint32_t sa = smem_u32(base + s * STAGE + STG_A + STG_B);
+                const uint64_t ad = umma_desc(sa, 1024, 2), bd = umma_desc(sa + OP_A, 1024, 2);
+#pragma unroll
+                for (int j = 0; j < WG_KB / 16; ++j)
+                    tc_mma(tmem, ad + (uint64_t)(2 * j), bd + (uint64_t)(2 * j), IDESC, (g | j) != 0);
+                tc_commit(&op_empty[s]);
+            }
+            if (ok) tc_commit(accf);
+            tc_commit(drain);
+            mbar_wait_bounded(drain, 0, TC_WAIT_LIMIT);
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------- transpose, epilogue
+        const int tw = warp - 2, j = lane >> 3, i = lane & 7;
+        bool ok = true;
+        for (int g = 0; g < nk && ok; ++g) {
+            const int s = g % ST;
+            const uint32_t u = (uint32_t)(g / ST);
+            if (!(ok = tc_wait(&full[s], u & 1, abort_flag, a.err))) break;
+            if (u >= 1 && !(ok = tc_wait(&op_empty[s], (u - 1) & 1, abort_flag, a.err))) break;
+            uint8_t *st = base + s * STAGE;
+            const uint32_t stgA = smem_u32(st), stgB = stgA + STG_A, opA = stgB + STG_B, opB = opA + OP_A;
+            uint32_t r[4];
+            // A: this warp's chunk (tw); its [64 px][32 ch] box has 64-byte rows,
+            // 16-byte chunk k of row p at (k ^ ((p >> 1) & 3)).  Op k: pixels
+            // 8k..8k+7, channel blocks 0..3 (matrix j = channel block j).
+            if (mtile * 4 + tw < a.nchunks) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int px = 8 * k + i;
+                    ldsm_x4_trans(stgA + tw * WG_KB * 64 + px * 64 + ((j ^ ((px >> 1) & 3)) << 4), r);
+                    const int row = 32 * tw + 8 * j + i;       // (tap, ci) row of this matrix row
+                    stsm_x4(opA + row * 128 + ((k ^ (row & 7)) << 4), r);
+                }
+            }
+            // B: BN rows (output channels) x 64 px; op o: pixel block o % 8,
+            // channel blocks 4 (o / 8) .. + 3
+#pragma unroll 1
+            for (int o = tw; o < BN / 4; o += 4) {
+                const int pb = o & 7, cb = 4 * (o >> 3) + j, px = 8 * pb + i;
+                uint32_t src;
+                if (BN == 32) src = stgB + px * 64 + ((cb ^ ((px >> 1) & 3)) << 4);
+                else src = stgB + (cb >> 3) * (WG_KB * 128) + px * 128 + (((cb & 7) ^ (px & 7)) << 4);
+                ldsm_x4_trans(src, r);
+                const int row = 8 * cb + i;
+                stsm_x4(opB + row * 128 + ((pb ^ (row & 7)) << 4), r);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&stg_empty[s]);
+                mbar_arrive(&opfull[s]);
+            }
+        }
+        // epilogue: this warp's 32 TMEM lanes = 32 rows of the block
+        if (ok && nk > 0 && tc_wait(accf, 0, abort_flag, a.err)) {
+            tc_fence_after();
+            const int q = warp & 3;
+            const int row = mtile * 128 + 32 * q + lane;
+            float *dst = a.part + ((size_t)split * a.mtiles * 128 + row) * BN;
+            const bool valid = row < a.nchunks * 32;
+#pragma unroll 1
+            for (int c = 0; c < BN / 32; ++c) {
+                uint32_t v[32];
+                tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * c), v);
+                if (valid) {
+#pragma unroll
+                    for (int e = 0; e < 32; e += 4)
+                        *reinterpret_cast<float4 *>(dst + 32 * c + e) =
+                            make_float4(__uint_as_float(v[e]), __uint_as_float(v[e + 1]), __uint_as_float(v[e + 2]),
+                                        __uint_as_float(v[e + 3]));
+                }
+            }
+        } else if (nk == 0) {
+            // an empty range still contributes its (zero) partial
+            const int q = warp & 3;
+            const int row = mtile * 128 + 32 * q + lane;
+            float *dst = a.part + ((size_t)split * a.mtiles * 128 + row) * BN;
+            if (row < a.nchunks * 32)
+                for (int e = 0; e < BN; ++e) dst[e] = 0.f;
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+// dw[co][r] += sum over splits of part[split][r][co], r = tap * Cin + ci < rows
+__global__ void wgrad_reduce_kernel(const float *__restrict__ part, float *__restrict__ dw, int splits, int rows,
+                                    int prow, int Cout)
+{
+    const size_t n = (size_t)rows * Cout;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int co = (int)(e % Cout);
+        const int r = (int)(e / Cout);
+        float acc = 0.f;
+        for (int sp = 0; sp < splits; ++sp) acc += part[((size_t)sp * prow + r) * Cout + co];
+        dw[(size_t)co * rows + r] += acc;
+    }
+}
+
+// dbias[co] += sum over pixels of dy[p][co]: per-block partial sums over a
+// pixel range (256 threads = Cout channels x 256 / Cout pixel lanes, four
+// independent sums each), then a fixed-order sum of the partials
+__global__ void __launch_bounds__(256)
+bias_partial_kernel(const bf16 *__restrict__ dy, float *__restrict__ part, long long P, int Cout, long long per)
+{
+    __shared__ float red[256];
+    const int L = 256 / Cout, co = threadIdx.x % Cout, pl = threadIdx.x / Cout;
+    const long long p0 = (long long)blockIdx.x * per, p1 = p0 + per < P ? p0 + per : P;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    long long p = p0 + pl;
+    for (; p + 3LL * L < p1; p += 4LL * L) {
+        a0 += __bfloat162float(dy[p * Cout + co]);
+        a1 += __bfloat162float(dy[(p + L) * Cout + co]);
+        a2 += __bfloat162float(dy[(p + 2LL * L) * Cout + co]);
+        a3 += __bfloat162float(dy[(p + 3LL * L) * Cout + co]);
+    }
+    for (; p < p1; p += L) a0 += __bfloat162float(dy[p * Cout + co]);
+    red[threadIdx.x] = (a0 + a1) + (a2 + a3);
+    __syncthreads();
+    if (threadIdx.x < Cout) {
+        float sum = 0.f;
+        for (int l = 0; l < L; ++l) sum += red[l * Cout + threadIdx.x];
+        part[(size_t)blockIdx.x * Cout + threadIdx.x] = sum;
+    }
+}
+
+__global__ void bias_reduce_kernel(const float *__restrict__ part, float *__restrict__ dbias, int nblk, int Cout)
+{
+    const int co = blockIdx.x * blockDim.x + threadIdx.x;
+    if (co >= Cout) return;
+    float acc = 0.f;
+    for (int b = 0; b < nblk; ++b) acc += part[(size_t)b * Cout + co];
+    dbias[co] += acc;
+}
+
+template <int BN>
+constexpr int wg_stages()
+{
+    return (196 * 1024) / (4 * WG_KB * 64 + WG_KB * BN * 2 + 128 * 128 + BN * 128) > 4
+               ? 4
+               : (196 * 1024) / (4 * WG_KB * 64 + WG_KB * BN * 2 + 128 * 128 + BN * 128);
+}
+
+template <int BN>
+int launch_wgrad_tc(const CUtensorMap &m0, const CUtensorMap &m1, const CUtensorMap &mdy, const WgTcArgs &a,
+                    cudaStream_t st)
+{
+    constexpr int ST = wg_stages<BN>();
+    constexpr size_t SMEM =
+        (size_t)ST * (4 * WG_KB * 64 + WG_KB * BN * 2 + 128 * 128 + BN * 128) + 1024 + 256;
+    auto kern = wgrad_tc_kernel<BN, ST>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM) != cudaSuccess) return 1;
+    count_launch();
+    kern<<<a.mtiles * a.splits, WG_THREADS, SMEM, st>>>(m0, m1, mdy, a);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// Tensor map of an NHWC activation for the weight gradient: boxes of
+// (bc channels, 64 pixels, 1 row, 1 image), 64-byte (bc 32) or 128-byte (bc 64) swizzled rows.
+bool encode_wg(CUtensorMap *m, const void *ptr, int C, int N, int H, int W, int bc)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return false;
+    cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+    cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+    cuuint32_t box[4] = {(cuuint32_t)bc, (cuuint32_t)WG_KB, 1, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(ptr), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, bc == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Grow-only per-device workspace of the weight gradient's partial sums.
+float *wgrad_workspace(int device, size_t floats)
+{
+    static std::mutex mu;
+    static float *buf[64] = {};
+    static size_t cap[64] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    if (device < 0 || device >= 64) return nullptr;
+    if (cap[device] < floats) {
+        if (buf[device]) cudaFree(buf[device]);
+        buf[device] = nullptr;
+        cap[device] = 0;
+        if (cudaMalloc(&buf[device], floats * sizeof(float)) != cudaSuccess) return nullptr;
+        cap[device] = floats;
+    }
+    return buf[device];
+}
+
 }  // namespace
 
 void conv3x3_tc_set_halo(int on) { g_halo = on != 0; }
@@ -620,6 +966,71 @@ int conv3x3_tc(const void *x0, int C0, const void *x1, int C1, const void *w, co
     case 3264: return launch_tc<32, 64>(m0, m1, mw, a, st);
     default: return launch_tc<32, 32>(m0, m1, mw, a, st);
     }
+}
+
+// 0 = launched, 1 = launch error, 2 = shape not handled here (caller uses the mma.sync kernel)
+int conv3x3_wgrad_tc(const void *dy, const void *x0, int C0, const void *x1, int C1, float *dw, float *dbias, int N,
+                     int H, int W, int Cout, cudaStream_t st)
+{
+    if (C0 % 32 || C1 % 32 || C0 <= 0 || W % WG_KB || N < 1 || H < 1) return 2;
+    if (!(Cout == 32 || Cout == 64 || Cout == 128 || Cout == 256)) return 2;
+    const int Cin = C0 + C1;
+    WgTcArgs a;
+    a.N = N;
+    a.H = H;
+    a.W = W;
+    a.C0 = C0;
+    a.C1 = C1;
+    a.Cout = Cout;
+    a.nchunks = 9 * Cin / 32;
+    a.mtiles = (a.nchunks + 3) / 4;
+    a.kblocks = (long long)N * H * (W / WG_KB);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // about two CTAs per SM over all row blocks, at least 8 k-blocks each
+    long long splits = std::max(1LL, (2LL * sms + a.mtiles - 1) / a.mtiles);
+    splits = std::min(splits, std::max(1LL, a.kblocks / 8));
+    a.kper = (a.kblocks + splits - 1) / splits;
+    a.splits = (int)((a.kblocks + a.kper - 1) / a.kper);
+    a.err = tc_err_flag(dev);
+    const long long P = (long long)N * H * W;
+    const int bias_blk = dbias ? (int)std::min<long long>(4 * sms, std::max(1LL, P / 256)) : 0;
+    const size_t part_floats = (size_t)a.splits * a.mtiles * 128 * Cout;
+    float *ws = wgrad_workspace(dev, part_floats + (size_t)bias_blk * Cout);
+    if (!ws) return 1;
+    a.part = ws;
+    CUtensorMap m0, m1, mdy;
+    if (!encode_wg(&m0, x0, C0, N, H, W, 32)) return 2;
+    if (C1 > 0) {
+        if (!encode_wg(&m1, x1, C1, N, H, W, 32)) return 2;
+    } else {
+        m1 = m0;
+    }
+    if (!encode_wg(&mdy, dy, Cout, N, H, W, Cout == 32 ? 32 : 64)) return 2;
+    int rc;
+    switch (Cout) {
+    case 32: rc = launch_wgrad_tc<32>(m0, m1, mdy, a, st); break;
+    case 64: rc = launch_wgrad_tc<64>(m0, m1, mdy, a, st); break;
+    case 128: rc = launch_wgrad_tc<128>(m0, m1, mdy, a, st); break;
+    default: rc = launch_wgrad_tc<256>(m0, m1, mdy, a, st); break;
+    }
+    if (rc) return rc;
+    const int rows = 9 * Cin;
+    count_launch();
+    wgrad_reduce_kernel<<<(unsigned)std::min<size_t>(((size_t)rows * Cout + 255) / 256, 148 * 16), 256, 0, st>>>(
+        a.part, dw, a.splits, rows, a.mtiles * 128, Cout);
+    if (cudaGetLastError() != cudaSuccess) return 1;
+    if (dbias) {
+        float *bp = ws + part_floats;
+        const long long per = (P + bias_blk - 1) / bias_blk;
+        count_launch();
+        bias_partial_kernel<<<bias_blk, 256, 0, st>>>((const bf16 *)dy, bp, P, Cout, per);
+        count_launch();
+        bias_reduce_kernel<<<(Cout + 255) / 256, 256, 0, st>>>(bp, dbias, bias_blk, Cout);
+        if (cudaGetLastError() != cudaSuccess) return 1;
+    }
+    return 0;
 }
 
 // Reads and clears the tensor-core convolution's error flag of the current device

@@ -6,7 +6,8 @@ tiles along a row (W >= 128, W not a multiple of 128), several whole rows per
 tile (W = 64, 32, with H not a multiple of the rows per tile), 32- and
 64-channel k-blocks, a concatenated second input, output-channel tiles of 32 to
 256 and several tiles per pixel block (Cout = 384), the split output of the
-data gradient; no pipeline wait runs out."""
+data gradient; no pipeline wait runs out.  The weight gradient on tcgen05
+against the oracle and the mma.sync kernel."""
 import numpy as np
 import pytest
 
@@ -119,3 +120,47 @@ def test_tc_conv_halo_tiles(oracle, N, H, W, C0, C1):
     ref = oracle.conv3x3(xc, _f64(w), _f64(b), relu=True)
     assert rel_l2(_f64(y_halo), ref) <= 1e-2, rel_l2(_f64(y_halo), ref)
     assert rel_l2(_f64(y_halo), _f64(y_tap)) <= 2e-3, rel_l2(_f64(y_halo), _f64(y_tap))
+
+
+def _wgrad(dy, x0, x1, N, H, W, C0, C1, Co, path):
+    import torch
+    from sscRaft import warmstart as ws
+    from sscRaft.rafttypes import libraft
+    dw = torch.full((Co, 3, 3, C0 + C1), 0.25, device="cuda")      # the gradient accumulates into dw
+    db = torch.full((Co,), -0.5, device="cuda")
+    assert libraft.raft_unet_set_conv_path(path) == 0
+    try:
+        assert libraft.raft_unet_conv_wgrad(ws._p(dy), ws._p(x0), C0, ws._p(x1), C1, ws._p(dw), ws._p(db),
+                                            N, H, W, Co, None) == 0
+        torch.cuda.synchronize()
+        assert libraft.raft_unet_conv_error() == 0
+    finally:
+        libraft.raft_unet_set_conv_path(0)
+    return _f64(dw) - 0.25, _f64(db) + 0.5
+
+
+@pytest.mark.parametrize("N,H,W,C0,C1,Co", [
+    (2, 5, 64, 32, 0, 32),        # level-0 shape: 9 row blocks of 32 in three 128-row tiles
+    (1, 4, 128, 32, 32, 64),      # concatenated input
+    (1, 3, 192, 96, 0, 32),       # 27 row blocks: a partly filled last tile
+    (2, 3, 64, 64, 64, 128),
+    (1, 2, 64, 256, 256, 256),    # 144 row blocks, 256 output channels
+])
+def test_tc_wgrad_vs_oracle_and_mma_sync(oracle, N, H, W, C0, C1, Co):
+    """Weight and bias gradients on tcgen05 (operands transposed in shared
+    memory, split over the pixels, partials summed in a fixed order) vs the
+    FP64 oracle on the BF16 inputs (rel-L2 <= 1e-4, FP32 accumulation of exact
+    BF16 products) and vs the mma.sync kernel (<= 1e-5)."""
+    import torch
+    torch.manual_seed(11 + H + W + C0 + C1 + Co)
+    x0 = _bf(torch.randn(N, H, W, C0, device="cuda"))
+    x1 = _bf(torch.randn(N, H, W, C1, device="cuda")) if C1 else None
+    dy = _bf(torch.randn(N, H, W, Co, device="cuda"))
+    dw_tc, db_tc = _wgrad(dy, x0, x1, N, H, W, C0, C1, Co, 2)
+    dw_ms, db_ms = _wgrad(dy, x0, x1, N, H, W, C0, C1, Co, 1)
+    xc = _f64(x0) if x1 is None else np.concatenate([_f64(x0), _f64(x1)], axis=-1)
+    ref = oracle.conv3x3_wgrad(_f64(dy), xc)
+    assert rel_l2(dw_tc, ref) <= 1e-4, rel_l2(dw_tc, ref)
+    assert rel_l2(dw_tc, dw_ms) <= 1e-5, rel_l2(dw_tc, dw_ms)
+    ref_db = _f64(dy).sum(axis=(0, 1, 2))
+    assert rel_l2(db_tc, ref_db) <= 1e-4, rel_l2(db_tc, ref_db)
