@@ -578,6 +578,40 @@ def run_unet(dev, samples=256, reps=3):
             "max_abs_output": float(out["mma_sync"].abs().max())}
 
 
+def run_unet_train(dev, batch=16, reps=5):
+    """One training step of the warm-start U-Net (forward, MSE, backward with
+    the tcgen05 convolutions and weight gradients, Adam) on a batch of 512^2
+    images: device time per step, and the same with the weight gradient on
+    the mma.sync kernel for comparison."""
+    import torch
+    from sscRaft import warmstart as W
+    from sscRaft.rafttypes import libraft
+    net = W.UNet(dev, seed=1)
+    g = torch.Generator(device=dev).manual_seed(3)
+    img = torch.rand((batch, 512, 512), generator=g, device=dev) * 0.01
+    tgt = torch.rand((batch, 512, 512), generator=g, device=dev) * 0.01
+    scale = torch.ones((batch,), device=dev)
+    ms = {}
+    for name, path in (("tcgen05", 0), ("mma_sync", 1)):
+        libraft.raft_unet_set_conv_path(path)
+        try:
+            for _ in range(2):
+                net.train_step(img, tgt, scale, 1e-5)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                net.train_step(img, tgt, scale, 1e-5)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            ms[name] = e0.elapsed_time(e1) / reps
+        finally:
+            libraft.raft_unet_set_conv_path(0)
+    net.check()
+    return {"workload": f"U-Net training step, batch {batch} x 512^2 (forward, MSE, backward, Adam)",
+            "ms_per_step": ms, "speedup_tcgen05_vs_mma_sync": ms["mma_sync"] / ms["tcgen05"]}
+
+
 # ----------------------------------------------------------- ragged batch --
 def run_ragged(dev, nreq=96, seed=5_000_000, em_iters=30):
     """96 requests, side log-uniform in [256, 2048], angles U[180, 1800], bins =
@@ -826,6 +860,11 @@ def run_ours(args):
         r = run_unet(dev, samples=args.slices, reps=max(1, args.steps))
         if rank == 0:
             print(json.dumps({"quick": True, "op": "unet", **r}), flush=True)
+        return
+    if args.quick and args.op == "unet_train":
+        r = run_unet_train(dev, reps=max(1, args.steps))
+        if rank == 0:
+            print(json.dumps({"quick": True, "op": "unet_train", **r}), flush=True)
         return
     if args.quick and args.op == "warm":
         r = run_warm(dev, samples=args.slices)
@@ -1100,7 +1139,7 @@ def main():
                     help="reference arm: the headline FBP, or tEMFQ on the tEM workload (comparison only)")
     ap.add_argument("--quick", action="store_true", help="device timing of one operator only (profiling)")
     ap.add_argument("--op", default="nearest", choices=["nearest", "linear", "linear_bf16", "radon", "aux", "tem", "ragged", "flat_dark", "bst",
-                                                        "temfq", "unet", "warm"])
+                                                        "temfq", "unet", "unet_train", "warm"])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -274,6 +274,11 @@ int raft_unet_set_conv_path(int path);
 /* tcgen05 convolution of the 32 -> 32 channel layers (W >= 128): 1 = halo tiles (one input
  * box per 32-channel chunk serves all nine taps; default), 0 = one input box per tap. */
 int raft_unet_set_conv_halo(int on);
+/* tcgen05 weight gradient (W a multiple of 64; Cout 32, 64, 128 or 256; other shapes and
+ * raft_unet_set_conv_path(1) use the mma.sync kernel): 1 = for Cout <= 128 one CTA per
+ * 32-channel input chunk with all nine taps, the input staged once per 64-pixel k-block
+ * (default); 0 = 128-row blocks of (tap, channel) for every layer. */
+int raft_unet_set_wgrad_nine(int on);
 /* 1 if a bounded pipeline wait of the tcgen05 convolution ran out since the last call
  * (the flag is then cleared); synchronises the current device. */
 int raft_unet_conv_error(void);

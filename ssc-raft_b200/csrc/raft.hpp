@@ -340,6 +340,7 @@ int conv3x3_tc_error();
 // 0 = launched, 1 = launch error, 2 = shape not handled (W % 64, Cout not 32/64/128/256).
 int conv3x3_wgrad_tc(const void *dy, const void *x0, int C0, const void *x1, int C1, float *dw, float *dbias, int N,
                      int H, int W, int Cout, cudaStream_t st);
+void conv3x3_wgrad_tc_set_nine(int on);
 void conv3x3_tc_set_halo(int on);
 
 }  // namespace raft

@@ -297,6 +297,23 @@ __global__ void relu_bwd_kernel(const bf16 *y, const bf16 *dy, bf16 *dpre, size_
         dpre[e] = __bfloat162float(y[e]) > 0.f ? dy[e] : __float2bfloat16(0.f);
 }
 
+// Eight elements per thread as 16-byte vectors (n % 8 == 0, 16-byte aligned):
+// the same selection, decided on the bits (y > 0 <=> sign clear and nonzero).
+__global__ void relu_bwd_v8_kernel(const uint4 *y, const uint4 *dy, uint4 *dpre, size_t n8)
+{
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n8; e += (size_t)gridDim.x * blockDim.x) {
+        const uint4 a = y[e], g = dy[e];
+        const uint32_t av[4] = {a.x, a.y, a.z, a.w}, gv[4] = {g.x, g.y, g.z, g.w};
+        uint32_t o[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int16_t lo = (int16_t)(av[q] & 0xffffu), hi = (int16_t)(av[q] >> 16);
+            o[q] = (lo > 0 ? (gv[q] & 0xffffu) : 0u) | (hi > 0 ? (gv[q] & 0xffff0000u) : 0u);
+        }
+        dpre[e] = make_uint4(o[0], o[1], o[2], o[3]);
+    }
+}
+
 // 2x2 average pooling, NHWC
 __global__ void pool_fwd_kernel(const bf16 *x, bf16 *y, int N, int H, int W, int C)
 {
@@ -552,6 +569,46 @@ __global__ void head_bwd_kernel(const bf16 *h, const float *w, const float *g, b
     if ((threadIdx.x & 31) == 0) atomicAdd(db, lb);
 }
 
+// The same with a pixel's C channels (C % 8 == 0, C <= 64) moved as 16-byte vectors.
+__global__ void head_bwd_v8_kernel(const bf16 *h, const float *w, const float *g, bf16 *dh, float *dw, float *db,
+                                   int N, int HW, int C)
+{
+    const size_t n = (size_t)N * HW;
+    float lw[64];
+    for (int c = 0; c < C; c++) lw[c] = 0.f;
+    float lb = 0.f;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const float gp = g[p];
+        lb += gp;
+        const uint4 *hv = reinterpret_cast<const uint4 *>(h + p * C);
+        uint4 *dv = reinterpret_cast<uint4 *>(dh + p * C);
+        for (int c8 = 0; c8 < C / 8; c8++) {
+            const uint4 v = hv[c8];
+            const __nv_bfloat162 *hh = reinterpret_cast<const __nv_bfloat162 *>(&v);
+            uint4 o;
+            __nv_bfloat162 *oo = reinterpret_cast<__nv_bfloat162 *>(&o);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int c = 8 * c8 + 2 * q;
+                const float2 f = __bfloat1622float2(hh[q]);
+                lw[c] += gp * f.x;
+                lw[c + 1] += gp * f.y;
+                oo[q] = __floats2bfloat162_rn(gp * w[c], gp * w[c + 1]);
+            }
+            dv[c8] = o;
+        }
+    }
+    for (int c = 0; c < C; c++) {
+        float v = lw[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&dw[c], v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lb += __shfl_xor_sync(0xffffffffu, lb, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(db, lb);
+}
+
 // Adam on FP32 master weights; writes the BF16 compute copy (wb may be null)
 __global__ void adam_kernel(float *w, float *m, float *v, const float *g, bf16 *wb, size_t n, float lr, float b1,
                             float b2, float eps, float c1, float c2)
@@ -572,6 +629,22 @@ __global__ void add_bf16_kernel(bf16 *y, const bf16 *x, size_t n)
 {
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
         y[e] = __float2bfloat16(__bfloat162float(y[e]) + __bfloat162float(x[e]));
+}
+
+__global__ void add_bf16_v8_kernel(uint4 *y, const uint4 *x, size_t n8)
+{
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n8; e += (size_t)gridDim.x * blockDim.x) {
+        uint4 a = y[e];
+        const uint4 b = x[e];
+        __nv_bfloat162 *pa = reinterpret_cast<__nv_bfloat162 *>(&a);
+        const __nv_bfloat162 *pb = reinterpret_cast<const __nv_bfloat162 *>(&b);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const float2 fa = __bfloat1622float2(pa[q]), fb = __bfloat1622float2(pb[q]);
+            pa[q] = __floats2bfloat162_rn(fa.x + fb.x, fa.y + fb.y);
+        }
+        y[e] = a;
+    }
 }
 
 __global__ void f32_to_bf16_kernel(const float *a, bf16 *b, size_t n)
@@ -611,6 +684,14 @@ int raft_unet_set_conv_path(int path)
 int raft_unet_set_conv_halo(int on)
 {
     conv3x3_tc_set_halo(on);
+    return 0;
+}
+
+// Nine-tap CTAs of the tcgen05 weight gradient where Cout <= 128 (1, the
+// default) or 128-row blocks of (tap, channel) for every layer (0).
+int raft_unet_set_wgrad_nine(int on)
+{
+    conv3x3_wgrad_tc_set_nine(on);
     return 0;
 }
 
@@ -670,7 +751,12 @@ int raft_unet_flip_weights(const void *w, void *wt, int Cout, int Cin, void *str
 int raft_unet_relu_bwd(const void *y, const void *dy, void *dpre, size_t n, void *stream)
 {
     count_launch();
-    relu_bwd_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const bf16 *)y, (const bf16 *)dy, (bf16 *)dpre, n);
+    if (n % 8 == 0 && ((uintptr_t)y | (uintptr_t)dy | (uintptr_t)dpre) % 16 == 0)
+        relu_bwd_v8_kernel<<<grid_for(n / 8), 256, 0, (cudaStream_t)stream>>>(
+            (const uint4 *)y, (const uint4 *)dy, (uint4 *)dpre, n / 8);
+    else
+        relu_bwd_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const bf16 *)y, (const bf16 *)dy,
+                                                                       (bf16 *)dpre, n);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
@@ -744,6 +830,9 @@ int raft_unet_head(int backward, const void *h, const float *w, const float *b, 
     if (!backward)
         head_fwd_kernel<<<grid_for((size_t)N * HW), 256, 0, (cudaStream_t)stream>>>((const bf16 *)h, w, b, img, scale,
                                                                                     out_or_grad, N, HW, C);
+    else if (C % 8 == 0 && C <= 64 && ((uintptr_t)h | (uintptr_t)dh) % 16 == 0)
+        head_bwd_v8_kernel<<<grid_for((size_t)N * HW), 256, 0, (cudaStream_t)stream>>>((const bf16 *)h, w, out_or_grad,
+                                                                                       (bf16 *)dh, dw, db, N, HW, C);
     else
         head_bwd_kernel<<<grid_for((size_t)N * HW), 256, 0, (cudaStream_t)stream>>>((const bf16 *)h, w, out_or_grad,
                                                                                     (bf16 *)dh, dw, db, N, HW, C);
@@ -770,7 +859,10 @@ int raft_unet_adam(float *w, float *m, float *v, const float *g, void *wb, size_
 int raft_unet_add(void *y, const void *x, size_t n, void *stream)
 {
     count_launch();
-    add_bf16_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((bf16 *)y, (const bf16 *)x, n);
+    if (n % 8 == 0 && ((uintptr_t)y | (uintptr_t)x) % 16 == 0)
+        add_bf16_v8_kernel<<<grid_for(n / 8), 256, 0, (cudaStream_t)stream>>>((uint4 *)y, (const uint4 *)x, n / 8);
+    else
+        add_bf16_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((bf16 *)y, (const bf16 *)x, n);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 

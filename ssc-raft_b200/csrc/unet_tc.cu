@@ -531,6 +531,7 @@ bool encode_w(CUtensorMap *m, const void *ptr, int Cout, int Cin, int KC, int BN
 }
 
 bool g_halo = true;   // halo tiles for the 32 -> 32 channel layers (raft_unet_set_conv_halo)
+bool g_wgrad_nine = true;   // nine-tap weight-gradient CTAs where Cout <= 128 (raft_unet_set_wgrad_nine)
 
 // =========================================================== weight gradient
 // dW[co][tap][ci] = sum over pixels p of dY[p][co] * X[p + tap][ci] as a GEMM
@@ -772,6 +773,238 @@ __global__ void __launch_bounds__(WG_THREADS, 1)
     }
 }
 
+// All nine taps per CTA (Cout <= 128): the CTA owns one 32-channel input chunk
+// and all 288 (tap, channel) rows -- three M = 128 blocks, the third a quarter
+// full -- so a k-block stages the input once as three 66-pixel row boxes
+// (rows y-1..y+1, columns x0-1..x0+64, the TMA zero fill outside the image)
+// and every tap's operand rows are transposed out of them at a column offset.
+// The staging ring is deeper than the operand ring: the loads of several
+// k-blocks are in flight while the tensor cores work through the operands.
+constexpr int WG9_BOX = 66;                   // pixels per row box (64 + the two neighbours)
+constexpr int WG9_BOXB = 4608;                // one box's slot: 66 x 64 bytes, 512-byte aligned
+
+template <int BN>
+__host__ __device__ constexpr int wg9_stg_bytes()
+{
+    return (3 * WG9_BOXB + WG_KB * BN * 2 + 1023) / 1024 * 1024;
+}
+template <int BN>
+__host__ __device__ constexpr int wg9_op_bytes()
+{
+    return BN * 128 + 288 * 128;             // [opB | opA]; the third block reads 96 rows past opA
+}
+constexpr int WG9_SLACK = 96 * 128;
+
+template <int BN, int STS, int STO>
+__global__ void __launch_bounds__(WG_THREADS, 1)
+    wgrad_tc9_kernel(const __grid_constant__ CUtensorMap mx0, const __grid_constant__ CUtensorMap mx1,
+                     const __grid_constant__ CUtensorMap mdy, const WgTcArgs a)
+{
+    constexpr int STG = wg9_stg_bytes<BN>(), OPS = wg9_op_bytes<BN>();
+    static_assert(OPS % 1024 == 0 && (BN == 32 || BN == 64 || BN == 128), "layout");
+    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(TC_M >> 4) << 24);
+    constexpr uint32_t TMEM_COLS = 3 * BN <= 128 ? 128 : 3 * BN <= 256 ? 256 : 512;
+    constexpr uint32_t TX = 3 * WG9_BOX * 64 + WG_KB * BN * 2;
+
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    uint8_t *stg = base;                                   // STS staging slots
+    uint8_t *ops = base + STS * STG;                       // STO operand slots (+ slack)
+    uint64_t *full = reinterpret_cast<uint64_t *>(ops + STO * OPS + WG9_SLACK);
+    uint64_t *sfree = full + STS;
+    uint64_t *opfull = sfree + STS;
+    uint64_t *opfree = opfull + STO;
+    uint64_t *accf = opfree + STO;
+    uint64_t *drain = accf + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&sfree[s], 4);
+        }
+        for (int s = 0; s < STO; ++s) {
+            mbar_init(&opfull[s], 4);
+            mbar_init(&opfree[s], 1);
+        }
+        mbar_init(accf, 1);
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    const int cchunks = (a.C0 + a.C1) / 32, Cin = a.C0 + a.C1;
+    const int cc = (int)(blockIdx.x % (unsigned)cchunks), split = (int)(blockIdx.x / (unsigned)cchunks);
+    const long long kb0 = (long long)split * a.kper;
+    const long long kb1 = kb0 + a.kper < a.kblocks ? kb0 + a.kper : a.kblocks;
+    const int nk = kb1 > kb0 ? (int)(kb1 - kb0) : 0;
+    const int xbl = a.W / WG_KB;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ TMA
+        if (lane == 0) {
+            const int ch = cc * 32;
+            const CUtensorMap *mx = ch < a.C0 ? &mx0 : &mx1;
+            const int chx = ch < a.C0 ? ch : ch - a.C0;
+            bool ok = true;
+            int g = 0;
+            for (; g < nk && ok; ++g) {
+                const int s = g % STS;
+                const uint32_t u = (uint32_t)(g / STS);
+                if (u >= 1 && !(ok = tc_wait(&sfree[s], (u - 1) & 1, abort_flag, a.err))) break;
+                const long long kb = kb0 + g;
+                const int xb = (int)(kb % xbl);
+                const long long r = kb / xbl;
+                const int y = (int)(r % a.H), n = (int)(r / a.H), x0 = xb * WG_KB;
+                // slot: the dY box(es) first (1024-byte aligned, as the 128-byte
+                // swizzle needs), then the three input row boxes (512-byte aligned)
+                uint8_t *st = stg + s * STG;
+                mbar_arrive_expect_tx(&full[s], TX);
+                if (BN == 32) {
+                    tma_load_4d(st, &mdy, 0, x0, y, n, &full[s]);
+                } else {
+                    for (int b = 0; b < BN / 64; ++b)
+                        tma_load_4d(st + b * WG_KB * 128, &mdy, 64 * b, x0, y, n, &full[s]);
+                }
+                for (int ky = 0; ky < 3; ++ky)
+                    tma_load_4d(st + WG_KB * BN * 2 + ky * WG9_BOXB, mx, chx, x0 - 1, y + ky - 1, n, &full[s]);
+            }
+            for (int s = 0; s < STS && s < g; ++s)
+                mbar_wait_bounded(&full[s], (uint32_t)((g - 1 - s) / STS) & 1, TC_WAIT_LIMIT);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA
+        if (lane == 0) {
+            bool ok = true;
+            for (int g = 0; g < nk && ok; ++g) {
+                const int s = g % STO;
+                const uint32_t u = (uint32_t)(g / STO);
+                if (!(ok = tc_wait(&opfull[s], u & 1, abort_flag, a.err))) break;
+                tc_fence_after();
+                const uint32_t sb = smem_u32(ops + s * OPS), sa = sb + BN * 128;
+                const uint64_t bd = umma_desc(sb, 1024, 2);
+#pragma unroll
+                for (int mb = 0; mb < 3; ++mb) {
+                    const uint64_t ad = umma_desc(sa + (uint32_t)(mb * 128 * 128), 1024, 2);
+#pragma unroll
+                    for (int j = 0; j < WG_KB / 16; ++j)
+                        tc_mma(tmem + (uint32_t)(mb * BN), ad + (uint64_t)(2 * j), bd + (uint64_t)(2 * j), IDESC,
+                               (g | j) != 0);
+                }
+                tc_commit(&opfree[s]);
+            }
+            if (ok) tc_commit(accf);
+            tc_commit(drain);
+            mbar_wait_bounded(drain, 0, TC_WAIT_LIMIT);
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------- transpose, epilogue
+        const int tw = warp - 2, j = lane >> 3, i = lane & 7;
+        bool ok = true;
+        for (int g = 0; g < nk && ok; ++g) {
+            const int ss = g % STS, so = g % STO;
+            if (!(ok = tc_wait(&full[ss], (uint32_t)(g / STS) & 1, abort_flag, a.err))) break;
+            if (g >= STO && !(ok = tc_wait(&opfree[so], (uint32_t)(g / STO - 1) & 1, abort_flag, a.err))) break;
+            const uint32_t sy = smem_u32(stg + ss * STG), sx = sy + WG_KB * BN * 2;
+            const uint32_t opB = smem_u32(ops + so * OPS), opA = opB + BN * 128;
+            uint32_t r[4];
+            // A: op o -> tap o / 8, pixels 8 (o % 8) ..; tap (ky, kx) reads box ky at
+            // pixel offset kx (the box starts one pixel left of x0); 64-byte rows,
+            // 16-byte chunk k of row p at (k ^ ((p >> 1) & 3))
+#pragma unroll 2
+            for (int o = tw; o < 72; o += 4) {
+                const int tap = o >> 3, k = o & 7, ky = tap / 3, kx = tap - 3 * ky;
+                const int p = 8 * k + i + kx;
+                ldsm_x4_trans(sx + ky * WG9_BOXB + p * 64 + ((j ^ ((p >> 1) & 3)) << 4), r);
+                const int row = 32 * tap + 8 * j + i;
+                stsm_x4(opA + row * 128 + ((k ^ (row & 7)) << 4), r);
+            }
+#pragma unroll 1
+            for (int o = tw; o < BN / 4; o += 4) {
+                const int pb = o & 7, cb = 4 * (o >> 3) + j, px = 8 * pb + i;
+                uint32_t src;
+                if (BN == 32) src = sy + px * 64 + ((cb ^ ((px >> 1) & 3)) << 4);
+                else src = sy + (cb >> 3) * (WG_KB * 128) + px * 128 + (((cb & 7) ^ (px & 7)) << 4);
+                ldsm_x4_trans(src, r);
+                const int row = 8 * cb + i;
+                stsm_x4(opB + row * 128 + ((pb ^ (row & 7)) << 4), r);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&sfree[ss]);
+                mbar_arrive(&opfull[so]);
+            }
+        }
+        if (ok && nk > 0 && tc_wait(accf, 0, abort_flag, a.err)) {
+            tc_fence_after();
+            const int q = warp & 3;
+#pragma unroll 1
+            for (int mb = 0; mb < 3; ++mb) {
+                const int row = mb * 128 + 32 * q + lane;      // tap * 32 + channel of the chunk
+                const bool valid = row < 288;
+                const int rg = (row >> 5) * Cin + cc * 32 + (row & 31);
+                float *dst = a.part + ((size_t)split * 9 * Cin + (valid ? rg : 0)) * BN;
+#pragma unroll 1
+                for (int c = 0; c < BN / 32; ++c) {
+                    uint32_t v[32];
+                    tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(mb * BN + 32 * c), v);
+                    if (valid) {
+#pragma unroll
+                        for (int e = 0; e < 32; e += 4)
+                            *reinterpret_cast<float4 *>(dst + 32 * c + e) =
+                                make_float4(__uint_as_float(v[e]), __uint_as_float(v[e + 1]),
+                                            __uint_as_float(v[e + 2]), __uint_as_float(v[e + 3]));
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+template <int BN>
+constexpr int wg9_stages_stg()
+{
+    return (int)((224 * 1024 - 2 * wg9_op_bytes<BN>() - WG9_SLACK - 1280) / wg9_stg_bytes<BN>()) > 8
+               ? 8
+               : (int)((224 * 1024 - 2 * wg9_op_bytes<BN>() - WG9_SLACK - 1280) / wg9_stg_bytes<BN>());
+}
+
+template <int BN>
+int launch_wgrad_tc9(const CUtensorMap &m0, const CUtensorMap &m1, const CUtensorMap &mdy, const WgTcArgs &a,
+                     int ctas, cudaStream_t st)
+{
+    constexpr int STO = 2, STS = wg9_stages_stg<BN>();
+    static_assert(STS >= 2, "staging ring");
+    constexpr size_t SMEM = (size_t)STS * wg9_stg_bytes<BN>() + (size_t)STO * wg9_op_bytes<BN>() + WG9_SLACK +
+                            1024 + 256;
+    static_assert(SMEM <= 227 * 1024, "shared memory");
+    auto kern = wgrad_tc9_kernel<BN, STS, STO>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM) != cudaSuccess) return 1;
+    count_launch();
+    kern<<<ctas, WG_THREADS, SMEM, st>>>(m0, m1, mdy, a);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
 // dw[co][r] += sum over splits of part[split][r][co], r = tap * Cin + ci < rows
 __global__ void wgrad_reduce_kernel(const float *__restrict__ part, float *__restrict__ dw, int splits, int rows,
                                     int prow, int Cout)
@@ -786,40 +1019,54 @@ __global__ void wgrad_reduce_kernel(const float *__restrict__ part, float *__res
     }
 }
 
-// dbias[co] += sum over pixels of dy[p][co]: per-block partial sums over a
-// pixel range (256 threads = Cout channels x 256 / Cout pixel lanes, four
-// independent sums each), then a fixed-order sum of the partials
+// dbias[co] += sum over pixels of dy[p][co], in a fixed order: per block a
+// pixel range, each thread eight channels of one pixel lane (16-byte loads,
+// lanes = 256 / (Cout / 8)), lanes summed in shared memory; then one block per
+// channel sums the blocks' partials (a strided per-thread sum and a tree).
 __global__ void __launch_bounds__(256)
 bias_partial_kernel(const bf16 *__restrict__ dy, float *__restrict__ part, long long P, int Cout, long long per)
 {
-    __shared__ float red[256];
-    const int L = 256 / Cout, co = threadIdx.x % Cout, pl = threadIdx.x / Cout;
+    __shared__ float red[256 * 8];
+    const int g8 = Cout / 8, L = 256 / g8, c8 = threadIdx.x % g8, pl = threadIdx.x / g8;
     const long long p0 = (long long)blockIdx.x * per, p1 = p0 + per < P ? p0 + per : P;
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-    long long p = p0 + pl;
-    for (; p + 3LL * L < p1; p += 4LL * L) {
-        a0 += __bfloat162float(dy[p * Cout + co]);
-        a1 += __bfloat162float(dy[(p + L) * Cout + co]);
-        a2 += __bfloat162float(dy[(p + 2LL * L) * Cout + co]);
-        a3 += __bfloat162float(dy[(p + 3LL * L) * Cout + co]);
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (pl < L) {
+        for (long long p = p0 + pl; p < p1; p += L) {
+            const uint4 v = *reinterpret_cast<const uint4 *>(dy + p * Cout + 8 * c8);
+            const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&v);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const float2 f = __bfloat1622float2(h[q]);
+                acc[2 * q] += f.x;
+                acc[2 * q + 1] += f.y;
+            }
+        }
     }
-    for (; p < p1; p += L) a0 += __bfloat162float(dy[p * Cout + co]);
-    red[threadIdx.x] = (a0 + a1) + (a2 + a3);
+#pragma unroll
+    for (int q = 0; q < 8; q++) red[threadIdx.x * 8 + q] = acc[q];
     __syncthreads();
     if (threadIdx.x < Cout) {
+        const int co = threadIdx.x, c = co / 8, q = co % 8;
         float sum = 0.f;
-        for (int l = 0; l < L; ++l) sum += red[l * Cout + threadIdx.x];
-        part[(size_t)blockIdx.x * Cout + threadIdx.x] = sum;
+        for (int l = 0; l < L; ++l) sum += red[(l * g8 + c) * 8 + q];
+        part[(size_t)blockIdx.x * Cout + co] = sum;
     }
 }
 
-__global__ void bias_reduce_kernel(const float *__restrict__ part, float *__restrict__ dbias, int nblk, int Cout)
+__global__ void __launch_bounds__(256) bias_reduce_kernel(const float *__restrict__ part, float *__restrict__ dbias,
+                                                          int nblk, int Cout)
 {
-    const int co = blockIdx.x * blockDim.x + threadIdx.x;
-    if (co >= Cout) return;
+    __shared__ float red[256];
+    const int co = blockIdx.x;
     float acc = 0.f;
-    for (int b = 0; b < nblk; ++b) acc += part[(size_t)b * Cout + co];
-    dbias[co] += acc;
+    for (int b = threadIdx.x; b < nblk; b += 256) acc += part[(size_t)b * Cout + co];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) dbias[co] += red[0];
 }
 
 template <int BN>
@@ -846,13 +1093,13 @@ int launch_wgrad_tc(const CUtensorMap &m0, const CUtensorMap &m1, const CUtensor
 
 // Tensor map of an NHWC activation for the weight gradient: boxes of
 // (bc channels, 64 pixels, 1 row, 1 image), 64-byte (bc 32) or 128-byte (bc 64) swizzled rows.
-bool encode_wg(CUtensorMap *m, const void *ptr, int C, int N, int H, int W, int bc)
+bool encode_wg(CUtensorMap *m, const void *ptr, int C, int N, int H, int W, int bc, int bw = WG_KB)
 {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return false;
     cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
     cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
-    cuuint32_t box[4] = {(cuuint32_t)bc, (cuuint32_t)WG_KB, 1, 1};
+    cuuint32_t box[4] = {(cuuint32_t)bc, (cuuint32_t)bw, 1, 1};
     cuuint32_t es[4] = {1, 1, 1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(ptr), dims, strides, box, es,
                CU_TENSOR_MAP_INTERLEAVE_NONE, bc == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
@@ -880,6 +1127,7 @@ float *wgrad_workspace(int device, size_t floats)
 }  // namespace
 
 void conv3x3_tc_set_halo(int on) { g_halo = on != 0; }
+void conv3x3_wgrad_tc_set_nine(int on) { g_wgrad_nine = on != 0; }
 
 bool conv3x3_tc_supported(int C0, int C1, int W)
 {
@@ -975,6 +1223,10 @@ int conv3x3_wgrad_tc(const void *dy, const void *x0, int C0, const void *x1, int
     if (C0 % 32 || C1 % 32 || C0 <= 0 || W % WG_KB || N < 1 || H < 1) return 2;
     if (!(Cout == 32 || Cout == 64 || Cout == 128 || Cout == 256)) return 2;
     const int Cin = C0 + C1;
+    // Cout <= 128: all nine taps per CTA (one 32-channel input chunk, inputs
+    // staged once per k-block); Cout = 256: 128-row blocks of (tap, channel)
+    // (three accumulators of 256 columns would not fit TMEM)
+    const bool nine = Cout <= 128 && g_wgrad_nine;
     WgTcArgs a;
     a.N = N;
     a.H = H;
@@ -988,38 +1240,51 @@ int conv3x3_wgrad_tc(const void *dy, const void *x0, int C0, const void *x1, int
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    // about two CTAs per SM over all row blocks, at least 8 k-blocks each
-    long long splits = std::max(1LL, (2LL * sms + a.mtiles - 1) / a.mtiles);
+    // one CTA per SM over all work items (shared memory holds one), at least
+    // 8 k-blocks each (nine-tap CTAs); two per SM for the row-block kernel
+    const int items = nine ? Cin / 32 : a.mtiles;
+    long long splits = std::max(1LL, ((nine ? 1LL : 2LL) * sms + items - 1) / items);
     splits = std::min(splits, std::max(1LL, a.kblocks / 8));
     a.kper = (a.kblocks + splits - 1) / splits;
     a.splits = (int)((a.kblocks + a.kper - 1) / a.kper);
     a.err = tc_err_flag(dev);
     const long long P = (long long)N * H * W;
     const int bias_blk = dbias ? (int)std::min<long long>(4 * sms, std::max(1LL, P / 256)) : 0;
-    const size_t part_floats = (size_t)a.splits * a.mtiles * 128 * Cout;
+    const int prow = nine ? 9 * Cin : a.mtiles * 128;
+    const size_t part_floats = (size_t)a.splits * prow * Cout;
     float *ws = wgrad_workspace(dev, part_floats + (size_t)bias_blk * Cout);
     if (!ws) return 1;
     a.part = ws;
     CUtensorMap m0, m1, mdy;
-    if (!encode_wg(&m0, x0, C0, N, H, W, 32)) return 2;
+    const int bw = nine ? WG9_BOX : WG_KB;
+    if (!encode_wg(&m0, x0, C0, N, H, W, 32, bw)) return 2;
     if (C1 > 0) {
-        if (!encode_wg(&m1, x1, C1, N, H, W, 32)) return 2;
+        if (!encode_wg(&m1, x1, C1, N, H, W, 32, bw)) return 2;
     } else {
         m1 = m0;
     }
     if (!encode_wg(&mdy, dy, Cout, N, H, W, Cout == 32 ? 32 : 64)) return 2;
     int rc;
-    switch (Cout) {
-    case 32: rc = launch_wgrad_tc<32>(m0, m1, mdy, a, st); break;
-    case 64: rc = launch_wgrad_tc<64>(m0, m1, mdy, a, st); break;
-    case 128: rc = launch_wgrad_tc<128>(m0, m1, mdy, a, st); break;
-    default: rc = launch_wgrad_tc<256>(m0, m1, mdy, a, st); break;
+    if (nine) {
+        const int ctas = items * a.splits;
+        switch (Cout) {
+        case 32: rc = launch_wgrad_tc9<32>(m0, m1, mdy, a, ctas, st); break;
+        case 64: rc = launch_wgrad_tc9<64>(m0, m1, mdy, a, ctas, st); break;
+        default: rc = launch_wgrad_tc9<128>(m0, m1, mdy, a, ctas, st); break;
+        }
+    } else {
+        switch (Cout) {
+        case 32: rc = launch_wgrad_tc<32>(m0, m1, mdy, a, st); break;
+        case 64: rc = launch_wgrad_tc<64>(m0, m1, mdy, a, st); break;
+        case 128: rc = launch_wgrad_tc<128>(m0, m1, mdy, a, st); break;
+        default: rc = launch_wgrad_tc<256>(m0, m1, mdy, a, st); break;
+        }
     }
     if (rc) return rc;
     const int rows = 9 * Cin;
     count_launch();
     wgrad_reduce_kernel<<<(unsigned)std::min<size_t>(((size_t)rows * Cout + 255) / 256, 148 * 16), 256, 0, st>>>(
-        a.part, dw, a.splits, rows, a.mtiles * 128, Cout);
+        a.part, dw, a.splits, rows, prow, Cout);
     if (cudaGetLastError() != cudaSuccess) return 1;
     if (dbias) {
         float *bp = ws + part_floats;
@@ -1027,7 +1292,7 @@ int conv3x3_wgrad_tc(const void *dy, const void *x0, int C0, const void *x1, int
         count_launch();
         bias_partial_kernel<<<bias_blk, 256, 0, st>>>((const bf16 *)dy, bp, P, Cout, per);
         count_launch();
-        bias_reduce_kernel<<<(Cout + 255) / 256, 256, 0, st>>>(bp, dbias, bias_blk, Cout);
+        bias_reduce_kernel<<<Cout, 256, 0, st>>>(bp, dbias, bias_blk, Cout);
         if (cudaGetLastError() != cudaSuccess) return 1;
     }
     return 0;

@@ -37,8 +37,9 @@ libraft.raft_unet_add.argtypes = [_P, _P, _Z, _P]
 libraft.raft_unet_to_bf16.argtypes = [_P, _P, _Z, _P]
 libraft.raft_unet_set_conv_path.argtypes = [_I]
 libraft.raft_unet_set_conv_halo.argtypes = [_I]
+libraft.raft_unet_set_wgrad_nine.argtypes = [_I]
 libraft.raft_unet_conv_error.argtypes = []
-for _f in ("raft_unet_set_conv_path", "raft_unet_set_conv_halo", "raft_unet_conv_error", "raft_unet_conv_fwd", "raft_unet_conv_wgrad", "raft_unet_flip_weights", "raft_unet_relu_bwd",
+for _f in ("raft_unet_set_conv_path", "raft_unet_set_conv_halo", "raft_unet_set_wgrad_nine", "raft_unet_conv_error", "raft_unet_conv_fwd", "raft_unet_conv_wgrad", "raft_unet_flip_weights", "raft_unet_relu_bwd",
            "raft_unet_pool", "raft_unet_upsample", "raft_unet_input", "raft_unet_head", "raft_unet_mse",
            "raft_unet_adam", "raft_unet_add", "raft_unet_to_bf16"):
     getattr(libraft, _f).restype = _I

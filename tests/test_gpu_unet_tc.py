@@ -148,7 +148,8 @@ def _wgrad(dy, x0, x1, N, H, W, C0, C1, Co, path):
 ])
 def test_tc_wgrad_vs_oracle_and_mma_sync(oracle, N, H, W, C0, C1, Co):
     """Weight and bias gradients on tcgen05 (operands transposed in shared
-    memory, split over the pixels, partials summed in a fixed order) vs the
+    memory, split over the pixels, partials summed in a fixed order; both CTA
+    shapes: all nine taps of a 32-channel chunk, and 128-row blocks) vs the
     FP64 oracle on the BF16 inputs (rel-L2 <= 1e-4, FP32 accumulation of exact
     BF16 products) and vs the mma.sync kernel (<= 1e-5)."""
     import torch
@@ -156,10 +157,17 @@ def test_tc_wgrad_vs_oracle_and_mma_sync(oracle, N, H, W, C0, C1, Co):
     x0 = _bf(torch.randn(N, H, W, C0, device="cuda"))
     x1 = _bf(torch.randn(N, H, W, C1, device="cuda")) if C1 else None
     dy = _bf(torch.randn(N, H, W, Co, device="cuda"))
+    from sscRaft.rafttypes import libraft
     dw_tc, db_tc = _wgrad(dy, x0, x1, N, H, W, C0, C1, Co, 2)
     dw_ms, db_ms = _wgrad(dy, x0, x1, N, H, W, C0, C1, Co, 1)
+    libraft.raft_unet_set_wgrad_nine(0)          # 128-row blocks of (tap, channel) instead of nine-tap CTAs
+    try:
+        dw_rb, _ = _wgrad(dy, x0, x1, N, H, W, C0, C1, Co, 2)
+    finally:
+        libraft.raft_unet_set_wgrad_nine(1)
     xc = _f64(x0) if x1 is None else np.concatenate([_f64(x0), _f64(x1)], axis=-1)
     ref = oracle.conv3x3_wgrad(_f64(dy), xc)
+    assert rel_l2(dw_rb, ref) <= 1e-4, rel_l2(dw_rb, ref)
     assert rel_l2(dw_tc, ref) <= 1e-4, rel_l2(dw_tc, ref)
     assert rel_l2(dw_tc, dw_ms) <= 1e-5, rel_l2(dw_tc, dw_ms)
     ref_db = _f64(dy).sum(axis=(0, 1, 2))
