@@ -958,6 +958,8 @@ def run_ours(args):
     em_result = None if args.no_em else run_tem(local, dev)
     ragged_result = None if args.no_ragged else run_ragged(dev)
     warm_result = None if args.no_warm else run_warm(dev)
+    if warm_result is not None:
+        warm_result["training_step"] = run_unet_train(dev)
     flat_dark_result = None if args.no_flat_dark else run_flat_dark(dev, sino, hbm_peak=hbm_peak)
     temfq_result = None if args.no_temfq else run_temfq(dev)
     aux_result = None if args.no_aux else run_aux(dev, sino)
