@@ -177,15 +177,23 @@ __device__ __forceinline__ int fft_pad(int i) { return i + (i >> 4); }
 // One Stockham pass of radix R from src to dst (Np complex values in shared
 // memory; pin / pout: src / dst stored padded).  Butterfly j = q Ns + k; the
 // thread's (q, k) advance by blockDim.x without a division per butterfly.
+// The twiddle exp(-2 pi i k twstep / Np) is computed only when k changes (for
+// Ns dividing the block size a thread keeps one k for the whole pass).  An SFU
+// __sincosf in place of sincospif measured 0.6 % faster FBP and doubled the
+// filter's error against the FP64 oracle (1.4e-5 for 14400-bin linear rows);
+// not used.
 template <int R>
 __device__ __noinline__ void fft_pass(const float2 *__restrict__ src, float2 *__restrict__ dst, int Np,
                                       int Ns, const float2 *__restrict__ tw, int pin, int pout)
 {
+    (void)tw;
     const int nb = Np / R;
     const int twstep = Np / (Ns * R);
     const int T = blockDim.x;
     int q = threadIdx.x / Ns, k = threadIdx.x - q * Ns;
     const int dq = T / Ns, dk = T - dq * Ns;
+    int kw = -1;
+    float2 w1 = make_float2(1.f, 0.f);
     for (int j = threadIdx.x; j < nb; j += T) {
         float2 v[R];
 #pragma unroll
@@ -196,13 +204,12 @@ __device__ __noinline__ void fft_pass(const float2 *__restrict__ src, float2 *__
         if (k > 0) {
             // w^r, r < R, from w = exp(-2 pi i k twstep / Np) by repeated products
             // (two complex registers live; relative error of w^7 a few 1e-7)
-            float2 w1;
-            {
-                // exp(-2 pi i k twstep / Np) computed in place of a (latency-bound)
-                // table load; sincospif rounds to about one unit in the last place
+            if (k != kw) {
+                // sincospif rounds to about one unit in the last place
                 float sn, cs;
                 sincospif(-2.0f * (float)(k * twstep) / (float)Np, &sn, &cs);
                 w1 = make_float2(cs, sn);
+                kw = k;
             }
             float2 w = w1;
 #pragma unroll

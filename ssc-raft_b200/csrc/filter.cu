@@ -427,7 +427,7 @@ filter_fft_cluster_kernel(const float *__restrict__ sino, int N, int Np, int off
         // no transform: match the conjugation convention of the output step
         for (int i1 = tid; i1 < m; i1 += T) bufA[i1].y = -bufA[i1].y;
     } else {
-    float2 *Y = fft_forward(bufA, bufB, m, rl, nullptr);     // plain order, same buffer in every CTA
+    float2 *Y = fft_forward(bufA, bufB, m, rl, nullptr);   // plain order, same buffer in every CTA
     float2 *Wb = (Y == bufA) ? bufB : bufA;
     cl.sync();
     // middle step for this CTA's block of k1: gather the C values, forward
@@ -459,7 +459,7 @@ filter_fft_cluster_kernel(const float *__restrict__ sino, int N, int Np, int off
         Y[k1] = cl.map_shared_rank(Wb, own)[(k1 - own * kb) * C + rank];
     }
     cl.sync();   // every CTA has read the Wb buffers before they are overwritten
-    R = fft_forward(Y, Wb, m, rl, nullptr);                  // conj of the filtered row, strided order
+    R = fft_forward(Y, Wb, m, rl, nullptr);            // conj of the filtered row, strided order
     }
     cl.sync();
     // output: element u of the filtered row sits in CTA u % C at u / C

@@ -2,7 +2,7 @@
 from the reference's own CUDA sources) in a process of its own, so that its
 exports never meet this repository's libraft.so in one address space.
 
-    python tests/ref_runner.py fbp|bst IN.npz OUT.npz
+    python tests/ref_runner.py fbp|bst|eem IN.npz OUT.npz
 
 IN.npz holds the arguments with the reference's packing (`sino`, `angles`,
 `paramf`, `parami`); OUT.npz receives `out`.  Test infrastructure only."""
@@ -51,10 +51,26 @@ def run_bst(d):
     return obj
 
 
+def run_eem(d):
+    """get_eEM_RT_MultiGPU (em_rt.cu:201-262) on GPU 0 from the uniform start."""
+    lib = ctypes.CDLL(REF_LIB)
+    P, I = ctypes.c_void_p, ctypes.c_int
+    lib.get_eEM_RT_MultiGPU.argtypes = [P, I, P, P, P, P, P]
+    tomo = np.ascontiguousarray(d["tomo"], np.float32)
+    ang = np.ascontiguousarray(d["angles"], np.float32)
+    B, A, N = tomo.shape
+    pi = np.array([N, A, B, N, 0, 0, 0, 1, int(d["iterations"]), 0], np.int32)
+    pf = np.zeros(1, np.float32)
+    obj = np.ones((B, N, N), np.float32)
+    g = np.array([0], np.intc)
+    lib.get_eEM_RT_MultiGPU(_p(g), 1, _p(obj), _p(tomo), _p(ang), _p(pf), _p(pi))
+    return obj
+
+
 def main():
     kind, src, dst = sys.argv[1:4]
     d = np.load(src)
-    out = {"fbp": run_fbp, "bst": run_bst}[kind](d)
+    out = {"fbp": run_fbp, "bst": run_bst, "eem": run_eem}[kind](d)
     np.savez(dst, out=out)
 
 

@@ -18,6 +18,9 @@
   the oracle).  The reference library is not run here: with 64 slices and
   900 angles its tEM reads its flat buffer by angle row beyond what it
   initialised (em_rt.cu:107,134), so its result is undefined.
+* Emission EM at the size of the ragged workload's larger requests (2 slices
+  of 768^2, 720 angles, 5 iterations) vs the reference library's own
+  get_eEM_RT_MultiGPU on the same data: rel-L2 <= 1e-4.
 """
 import os
 import subprocess
@@ -128,3 +131,22 @@ def test_tem_cfg3_vs_oracle(oracle):
     print(f"cfg3 tEM (3 iterations) vs FP64 oracle: rel-L2 {err:.3e}")
     assert np.all(np.isfinite(out))
     assert err <= 1e-3, err
+
+
+def test_eem_768_vs_reference_library(oracle, tmp_path):
+    import sscRaft
+    from sscRaft import synthetic as S
+    if not os.path.exists(REF_LIB):
+        pytest.skip("reference library not built (oracle/build_ref.sh)")
+    N, A, B, it = 768, 720, 2, 5
+    ang = S.uniform_angles(A)
+    imgs = np.stack([S.phantom_image(S.ellipse_params(4_000_000 + k, 20), N) for k in range(B)])
+    tomo = oracle.em_forward(imgs.astype(np.float64), ang, N).astype(np.float32)
+    out = sscRaft.em(tomo.copy(), angles=ang, dic={"gpu": [0], "method": "eEMRT", "iterations": it})
+    src, dst = tmp_path / "in.npz", tmp_path / "out.npz"
+    np.savez(src, tomo=tomo, angles=ang, iterations=it)
+    subprocess.run([sys.executable, os.path.join(REPO, "tests", "ref_runner.py"), "eem", str(src), str(dst)],
+                   check=True, timeout=600)
+    err = rel_l2(out, np.load(dst)["out"])
+    print(f"eEM 768^2 x 720 (5 iterations) vs reference library: rel-L2 {err:.3e}")
+    assert err <= 1e-4, err

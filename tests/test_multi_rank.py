@@ -113,3 +113,13 @@ def test_two_rank_slab_split_reconstruction_equals_whole():
     whole = oracle.fbp(sino, ang, oracle.MODE_LIN, 5, 2)
     for _, vol in res:
         np.testing.assert_array_equal(vol, whole)
+
+
+def test_bench_inputs_do_not_import_the_package():
+    """The reference arm makes its inputs with synthetic.py loaded by path, so
+    that process maps no library of this repository."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys; sys.path.insert(0, %r); import bench; S = bench.synthetic_module(); "
+            "S.ellipse_params(1, 3); assert 'sscRaft' not in sys.modules, sorted(sys.modules)" % root)
+    subprocess.run([sys.executable, "-c", code], check=True, timeout=120)
