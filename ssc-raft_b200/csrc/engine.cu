@@ -194,22 +194,31 @@ static void run_pipeline(DeviceState &ds, int nslices, int chunk, size_t in_ps, 
         if (!pin_dst) pout[b] = ds.pin_out[b].get(out_ps * chunk);
     }
     // Chunk schedule: the first chunk's upload and the last chunk's download
-    // overlap no compute, so with enough slices both are kept small (four
-    // slices, a whole group of the four-slice backprojector) and the rest
-    // goes in full chunks.
+    // overlap no compute, so with enough slices the chunks ramp up from four
+    // slices (a whole group of the four-slice backprojector), doubling, to
+    // full size, and ramp down the same way at the end: each upload then
+    // hides behind the compute of a chunk half its size, and the exposed
+    // ends are four slices' copies.
     std::vector<int> cs0, cns;
     {
-        const int edge = (chunk >= 8 && nslices > 2 * chunk) ? 4 : 0;
+        std::vector<int> ramp;
+        for (int e = 4; e < chunk && 4 * e <= nslices; e *= 2) ramp.push_back(e);
+        int edge_total = 0;
+        for (int e : ramp) edge_total += 2 * e;
+        if (chunk < 8 || nslices <= edge_total + chunk) {
+            ramp.clear();
+            edge_total = 0;
+        }
         int s = 0;
         auto add = [&](int n) {
             cs0.push_back(s);
             cns.push_back(n);
             s += n;
         };
-        if (edge) add(edge);
-        const int mid_end = nslices - edge;
+        for (int e : ramp) add(e);
+        const int mid_end = nslices - edge_total / 2;
         while (s < mid_end) add(std::min(chunk, mid_end - s));
-        if (edge) add(edge);
+        for (int k = (int)ramp.size() - 1; k >= 0; --k) add(ramp[k]);
     }
     const int nch = (int)cs0.size();
     auto finalize = [&](int c) {
