@@ -264,6 +264,155 @@ __device__ __forceinline__ float2 *fft_forward(float2 *a, float2 *b, int Np, con
 }
 
 
+// ------------------------------------------------ compile-time length --
+// The same transform for a length known at compile time: the passes are
+// unrolled, so every shared-memory address is the thread's padded index plus
+// an immediate offset, and a pass whose twiddle index k is the same in every
+// iteration of a thread computes its twiddle once.  Radix order, twiddle
+// expressions and butterflies are those of fft_pass; only the compiler's
+// choice of fused multiply-adds may differ, so the results agree with
+// fft_forward's to rounding (rel-L2 about 2e-7).  The first pass's loads and the last pass's
+// stores are functors, so callers can read the input from global memory and
+// consume the output in registers.
+struct CRadices {
+    int n;
+    int r[24];
+};
+__host__ __device__ constexpr CRadices c_factorize(int n)
+{
+    CRadices o{};
+    int e2 = 0;
+    while (n % 2 == 0) { n /= 2; e2++; }
+    while (e2 >= 3) { o.r[o.n++] = 8; e2 -= 3; }
+    if (e2 == 2) o.r[o.n++] = 4;
+    if (e2 == 1) o.r[o.n++] = 2;
+    while (n % 3 == 0) { n /= 3; o.r[o.n++] = 3; }
+    while (n % 5 == 0) { n /= 5; o.r[o.n++] = 5; }
+    while (n % 7 == 0) { n /= 7; o.r[o.n++] = 7; }
+    if (n != 1) o.n = -1;
+    return o;
+}
+__host__ __device__ constexpr int c_fft_threads(int n)
+{
+    return ((n / 16 + 31) / 32) * 32 < 128 ? 128 : (((n / 16 + 31) / 32) * 32 > 512 ? 512 : ((n / 16 + 31) / 32) * 32);
+}
+
+// Shared-memory source of pass (R, NS): element j + r nb, stored padded or plain.
+template <int NP, int T, int R, bool PIN>
+struct CSmemIn {
+    const float2 *s;
+    int base;   // padded (or plain) index of threadIdx.x
+    __device__ __forceinline__ CSmemIn(const float2 *s_) : s(s_), base(PIN ? fft_pad(threadIdx.x) : threadIdx.x) {}
+    __device__ __forceinline__ float2 operator()(int j, int it, int r) const
+    {
+        constexpr int nb = NP / R;
+        static_assert(!PIN || (T % 16 == 0 && nb % 16 == 0), "padded source needs 16 | T and 16 | nb");
+        (void)j;
+        return PIN ? s[base + it * (T + T / 16) + r * (nb + nb / 16)] : s[base + it * T + r * nb];
+    }
+};
+// Shared-memory destination of pass (R, NS): element q NS R + k + r NS.
+template <int NP, int R, int NS, bool POUT>
+struct CSmemOut {
+    float2 *d;
+    __device__ __forceinline__ void operator()(int q, int k, const float2 (&v)[R]) const
+    {
+        const int b = q * NS * R + k;
+        constexpr bool small = (16 % (NS * R)) == 0;
+        constexpr bool split = (NS * R) % 16 == 0 && (NS % 16 == 0 || 16 % NS == 0);
+        if (!POUT) {
+#pragma unroll
+            for (int r = 0; r < R; r++) d[b + r * NS] = v[r];
+        } else if (small || split) {
+            // pad(b + r NS) = pad(b) + r NS (+ r NS / 16 when 16 | NS R)
+            const int pb = fft_pad(b);
+#pragma unroll
+            for (int r = 0; r < R; r++) d[pb + r * NS + (small ? 0 : (r * NS) / 16)] = v[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) d[fft_pad(b + r * NS)] = v[r];
+        }
+    }
+};
+
+// One pass of radix R over NP points with T threads: v[r] = in(j, it, r)
+// (element j + r NP/R of the pass input), twiddles, R-point DFT,
+// out(q, k, v) (elements q NS R + k + r NS of the pass output).
+template <int NP, int T, int R, int NS, class In, class Out>
+__device__ __forceinline__ void cfft_pass(const In &in, const Out &out)
+{
+    constexpr int nb = NP / R;
+    constexpr int twstep = NP / (NS * R);
+    constexpr int ITER = (nb + T - 1) / T;
+    constexpr bool kfix = T % NS == 0;   // k = threadIdx.x % NS in every iteration
+    float2 wfix = make_float2(1.f, 0.f);
+    if (kfix && NS > 1) {
+        const int k = threadIdx.x % NS;
+        if (k > 0) {
+            float sn, cs;
+            sincospif(-2.0f * (float)(k * twstep) / (float)NP, &sn, &cs);
+            wfix = make_float2(cs, sn);
+        }
+    }
+#pragma unroll
+    for (int it = 0; it < ITER; it++) {
+        const int j = threadIdx.x + it * T;
+        if (nb % T != 0 && j >= nb) break;
+        const int q = j / NS, k = j - q * NS;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = in(j, it, r);
+        if (NS > 1 && k > 0) {
+            float2 w1 = wfix;
+            if (!kfix) {
+                float sn, cs;
+                sincospif(-2.0f * (float)(k * twstep) / (float)NP, &sn, &cs);
+                w1 = make_float2(cs, sn);
+            }
+            float2 w = w1;
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                v[r] = cmul(v[r], w);
+                if (r + 1 < R) w = cmul(w, w1);
+            }
+        }
+        Dft<R>::run(v);
+        out(q, k, v);
+    }
+}
+
+// Passes P.. of the NP-point transform from buffer a (b the other buffer);
+// pass 0 reads through `first`, the last pass writes through `last`; the
+// passes in between ping-pong through shared memory with a barrier after each.
+// (NS: product of the radices of the passes before P.)
+template <int NP, int P, int NS, class First, class Last>
+__device__ __forceinline__ void cfft_passes(float2 *a, float2 *b, const First &first, const Last &last)
+{
+    constexpr CRadices rl = c_factorize(NP);
+    constexpr int T = c_fft_threads(NP);
+    static_assert(rl.n > 0 && fft_padded(NP), "compile-time transforms take 7-smooth lengths up to 12288");
+    if constexpr (P < rl.n) {
+        constexpr int R = rl.r[P];
+        constexpr bool pout = P + 1 < rl.n;
+        if constexpr (P == 0 && P + 1 == rl.n) {
+            cfft_pass<NP, T, R, NS>(first, last.template at<R, NS>());
+        } else if constexpr (P == 0) {
+            cfft_pass<NP, T, R, NS>(first, CSmemOut<NP, R, NS, pout>{b});
+        } else if constexpr (P + 1 == rl.n) {
+            cfft_pass<NP, T, R, NS>(CSmemIn<NP, T, R, true>(a), last.template at<R, NS>());
+        } else {
+            cfft_pass<NP, T, R, NS>(CSmemIn<NP, T, R, true>(a), CSmemOut<NP, R, NS, pout>{b});
+        }
+        if constexpr (P + 1 < rl.n) {
+            __syncthreads();
+            cfft_passes<NP, P + 1, NS * R>(b, a, first, last);
+        }
+    }
+}
+// Buffer (0: a, 1: b) the last pass of an NP-point cfft_passes from a writes.
+template <int NP>
+__host__ __device__ constexpr int cfft_out_buffer() { return c_factorize(NP).n % 2 == 1 ? 1 : 0; }
+
 // ------------------------------------------------------- any length --
 // A forward DFT of any length n held in shared memory: directly when n has
 // only the prime factors 2, 3, 5, 7, otherwise by Bluestein's chirp-z

@@ -343,6 +343,202 @@ filter_fft_kernel(const float *__restrict__ sino, int N, int Np, int off, int ns
     if (has1) pack_row(z, rp.k, rp.a0 + 1, 1, pk);
 }
 
+// ====================================== kernel: FFT filter, fixed length
+// The same filter for the common padded lengths, with the transform length a
+// compile-time constant (cfft_passes): the first forward pass reads the two
+// sinogram rows straight from global memory (edge-replicating pad included),
+// the spectral multiply and conjugation sit in the last forward pass, and for
+// single-float window rows the last inverse pass stores the window elements
+// from registers (other row formats go through shared memory and pack_row).
+// The arithmetic of filter_fft_kernel; the results agree with it to rounding
+// (the compiler may fuse multiply-adds differently in the unrolled passes).
+template <int NP, int R0>
+struct FxRowsIn {
+    const float *s0, *s1;
+    int N, off;
+    bool has1;
+    __device__ __forceinline__ float2 operator()(int j, int it, int r) const
+    {
+        (void)it;
+        int i = j + r * (NP / R0) - off;
+        i = i < 0 ? 0 : (i > N - 1 ? N - 1 : i);
+        return make_float2(__ldg(&s0[i]), has1 ? __ldg(&s1[i]) : 0.f);
+    }
+};
+template <int R, int NS>
+struct FxSpecOut {
+    float2 *d;
+    const float2 *H;
+    __device__ __forceinline__ void operator()(int q, int k, const float2 (&v)[R]) const
+    {
+        (void)q;   // the last pass: NS R = NP, q = 0
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int i = k + r * NS;
+            const float2 g = cmul(v[r], __ldg(&H[i]));
+            d[i] = make_float2(g.x, -g.y);
+        }
+    }
+};
+struct FxSpecLast {
+    float2 *d;
+    const float2 *H;
+    template <int R, int NS> __device__ __forceinline__ FxSpecOut<R, NS> at() const { return {d, H}; }
+};
+template <int R, int NS>
+struct FxPlainOut {
+    float2 *d;
+    __device__ __forceinline__ void operator()(int q, int k, const float2 (&v)[R]) const
+    {
+        (void)q;
+#pragma unroll
+        for (int r = 0; r < R; r++) d[k + r * NS] = v[r];
+    }
+};
+struct FxPlainLast {
+    float2 *d;
+    template <int R, int NS> __device__ __forceinline__ FxPlainOut<R, NS> at() const { return {d}; }
+};
+// window element e = u - wlo of both rows, from filtered sample u (registers)
+struct FxWindow {
+    float *out;
+    size_t base0, base1;   // element 0 of the two window rows
+    int stride, wlo, Wg;
+    float w0, w1;
+    bool has1;
+};
+template <int R, int NS>
+struct FxWinOut {
+    FxWindow w;
+    __device__ __forceinline__ void operator()(int q, int k, const float2 (&v)[R]) const
+    {
+        (void)q;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int e = k + r * NS - w.wlo;
+            if ((unsigned)e < (unsigned)w.Wg) {
+                w.out[w.base0 + (size_t)e * w.stride] = v[r].x * w.w0;
+                if (w.has1) w.out[w.base1 + (size_t)e * w.stride] = (-v[r].y) * w.w1;
+            }
+        }
+    }
+};
+struct FxWinLast {
+    FxWindow w;
+    template <int R, int NS> __device__ __forceinline__ FxWinOut<R, NS> at() const { return {w}; }
+};
+
+__host__ __device__ constexpr int fixed_filter_min_blocks(int NP)
+{
+    return (220 * 1024) / (2 * fft_span(NP) * 8) < 1 ? 1
+         : ((220 * 1024) / (2 * fft_span(NP) * 8) > 2048 / c_fft_threads(NP) ? 2048 / c_fft_threads(NP)
+                                                                            : (220 * 1024) / (2 * fft_span(NP) * 8));
+}
+
+template <int NP, bool IL, bool FUSED>
+__global__ void __launch_bounds__(c_fft_threads(NP), fixed_filter_min_blocks(NP))
+filter_fixed_kernel(const float *__restrict__ sino, int N, int off, int nslices, const float2 *__restrict__ H,
+                    PackArgs pk)
+{
+    constexpr CRadices rl = c_factorize(NP);
+    constexpr int T = c_fft_threads(NP);
+    extern __shared__ float2 smem_fft[];
+    float2 *A = smem_fft, *B = smem_fft + fft_span(NP);
+    const RowPair rp = row_pair(blockIdx.x, pk.nangles, IL);
+    if (rp.k >= nslices) {
+        zero_rows(rp.k, rp.a0, pk);
+        return;
+    }
+    const int r0 = rp.k * pk.nangles + rp.a0, r1 = r0 + 1;
+    const bool has1 = rp.a0 + 1 < pk.nangles;
+    // forward transform of the two edge-padded rows, times H, conjugated
+    const FxRowsIn<NP, rl.r[0]> rows{sino + (size_t)r0 * N, sino + (size_t)r1 * N, N, off, has1};
+    float2 *X = cfft_out_buffer<NP>() ? B : A, *Y = (X == A) ? B : A;
+    cfft_passes<NP, 0, 1>(A, B, rows, FxSpecLast{X, H});
+    __syncthreads();
+    // inverse transform (forward transform of the conjugate; conjugated on output)
+    const CSmemIn<NP, T, rl.r[0], false> spec(X);
+    if constexpr (FUSED) {
+        FxWindow w;
+        w.out = reinterpret_cast<float *>(pk.out);
+        w.stride = IL ? 4 : 1;
+        w.base0 = IL ? ((size_t)(rp.k >> 2) * pk.nangles + rp.a0) * pk.Wg * 4 + (rp.k & 3)
+                     : ((size_t)rp.k * pk.nangles + rp.a0) * pk.Wg;
+        w.base1 = w.base0 + (size_t)pk.Wg * w.stride;
+        w.wlo = pk.wlo;
+        w.Wg = pk.Wg;
+        w.w0 = pk.wt ? pk.wt[rp.a0] : 1.f;
+        w.w1 = (pk.wt && has1) ? pk.wt[rp.a0 + 1] : 1.f;
+        w.has1 = has1;
+        cfft_passes<NP, 0, 1>(X, Y, spec, FxWinLast{w});
+        // window elements outside the padded row
+        const int lo = min(pk.Wg, max(0, -pk.wlo)), hi = max(0, NP - pk.wlo);
+        for (int e = threadIdx.x; e < pk.Wg; e += T) {
+            if (e >= lo && e < hi) continue;
+            w.out[w.base0 + (size_t)e * w.stride] = 0.f * w.w0;
+            if (has1) w.out[w.base1 + (size_t)e * w.stride] = 0.f * w.w1;
+        }
+    } else {
+        float2 *Z = cfft_out_buffer<NP>() ? Y : X;
+        cfft_passes<NP, 0, 1>(X, Y, spec, FxPlainLast{Z});
+        __syncthreads();
+        pack_row(Z, rp.k, rp.a0, 0, pk);
+        if (has1) pack_row(Z, rp.k, rp.a0 + 1, 1, pk);
+    }
+}
+
+static bool g_fixed_filter = true;
+
+template <int NP, bool IL, bool FUSED>
+static void launch_fixed_one(const FilterPlan &plan, const FilterLaunch &fl, const PackArgs &pk, int nsl,
+                             cudaStream_t st)
+{
+    static thread_local int configured_dev = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t smem = 2 * (size_t)fft_span(NP) * sizeof(float2);
+    if (configured_dev != dev) {
+        RAFT_CUDA(cudaFuncSetAttribute(filter_fixed_kernel<NP, IL, FUSED>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        RAFT_CUDA(cudaFuncSetAttribute(filter_fixed_kernel<NP, IL, FUSED>,
+                                       cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        configured_dev = dev;
+    }
+    ProfScope ps(PROF_FILTER, st);
+    filter_fixed_kernel<NP, IL, FUSED><<<(unsigned)row_pairs(nsl, fl.nangles, IL), c_fft_threads(NP), smem, st>>>(
+        fl.sino, plan.N, plan.off, nsl, plan.d_H, pk);
+}
+
+template <int NP>
+static void launch_fixed_np(const FilterPlan &plan, const FilterLaunch &fl, const PackArgs &pk, int nsl,
+                            cudaStream_t st)
+{
+    const bool f32 = fl.store == STORE_F32;
+    if (fl.interleaved) {
+        if (f32) launch_fixed_one<NP, true, true>(plan, fl, pk, nsl, st);
+        else launch_fixed_one<NP, true, false>(plan, fl, pk, nsl, st);
+    } else {
+        if (f32) launch_fixed_one<NP, false, true>(plan, fl, pk, nsl, st);
+        else launch_fixed_one<NP, false, false>(plan, fl, pk, nsl, st);
+    }
+}
+
+// Runs the fixed-length filter when one is compiled for plan.Np.
+static bool launch_fixed_filter(const FilterPlan &plan, const FilterLaunch &fl, const PackArgs &pk, int nsl,
+                                cudaStream_t st)
+{
+    if (!g_fixed_filter) return false;
+    switch (plan.Np) {
+    case 2048: launch_fixed_np<2048>(plan, fl, pk, nsl, st); return true;
+    case 3072: launch_fixed_np<3072>(plan, fl, pk, nsl, st); return true;
+    case 4096: launch_fixed_np<4096>(plan, fl, pk, nsl, st); return true;
+    case 6144: launch_fixed_np<6144>(plan, fl, pk, nsl, st); return true;
+    case 8192: launch_fixed_np<8192>(plan, fl, pk, nsl, st); return true;
+    case 12288: launch_fixed_np<12288>(plan, fl, pk, nsl, st); return true;
+    default: return false;
+    }
+}
+
 // ============================================ kernel: cluster FFT filter
 // Padded rows too long for one CTA's shared memory (two ping-pong buffers of
 // Np complex values) are filtered by a cluster of C CTAs (thread-block
@@ -616,6 +812,10 @@ void launch_filter(const FilterPlan &plan, const FilterLaunch &fl, cudaStream_t 
         }
         return;
     }
+    if (plan.fft && !plan.skip && !lp && plan.bs_M <= 0 && launch_fixed_filter(plan, fl, pk, nsl, st)) {
+        RAFT_CUDA(cudaGetLastError());
+        return;
+    }
     if (plan.fft || plan.skip) {
         FftPlan P;
         P.n = plan.Np;
@@ -672,3 +872,13 @@ bool filter_plan_shape(FilterPlan &plan, int ftype, int N, int pad)
 }
 
 }  // namespace raft
+
+extern "C" {
+// 1 (default): padded lengths 2048, 3072, 4096, 6144, 8192 and 12288 run the
+// compile-time-length filter kernel; 0: every length runs the generic one.
+int raft_filter_set_fixed(int on)
+{
+    raft::g_fixed_filter = on != 0;
+    return 0;
+}
+}

@@ -569,44 +569,59 @@ __global__ void head_bwd_kernel(const bf16 *h, const float *w, const float *g, b
     if ((threadIdx.x & 31) == 0) atomicAdd(db, lb);
 }
 
-// The same with a pixel's C channels (C % 8 == 0, C <= 64) moved as 16-byte vectors.
-__global__ void head_bwd_v8_kernel(const bf16 *h, const float *w, const float *g, bf16 *dh, float *dw, float *db,
-                                   int N, int HW, int C)
+// The same with 16-byte vectors: a thread owns one 8-channel group of a pixel
+// (G = C / 8 groups per pixel, G a power of two <= 8), so its weights and
+// partial sums stay in registers; the grid stride is a multiple of 256 and so
+// of G, which keeps each thread on one group.  Partial sums meet in shared
+// memory before one atomic per channel per block.
+__global__ void __launch_bounds__(256) head_bwd_v8_kernel(const uint4 *h, const float *w, const float *g, uint4 *dh,
+                                                          float *dw, float *db, size_t npix, int G)
 {
-    const size_t n = (size_t)N * HW;
-    float lw[64];
-    for (int c = 0; c < C; c++) lw[c] = 0.f;
+    __shared__ float part[8][65];
+    const int lg = __ffs(G) - 1;
+    const size_t e0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x, n = npix << lg;
+    const int c8 = threadIdx.x & (G - 1), lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float wr[8], lw[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        wr[j] = w[8 * c8 + j];
+        lw[j] = 0.f;
+    }
     float lb = 0.f;
-    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
-        const float gp = g[p];
-        lb += gp;
-        const uint4 *hv = reinterpret_cast<const uint4 *>(h + p * C);
-        uint4 *dv = reinterpret_cast<uint4 *>(dh + p * C);
-        for (int c8 = 0; c8 < C / 8; c8++) {
-            const uint4 v = hv[c8];
-            const __nv_bfloat162 *hh = reinterpret_cast<const __nv_bfloat162 *>(&v);
-            uint4 o;
-            __nv_bfloat162 *oo = reinterpret_cast<__nv_bfloat162 *>(&o);
+    for (size_t e = e0; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const float gp = g[e >> lg];
+        if (c8 == 0) lb += gp;
+        const uint4 v = h[e];
+        const __nv_bfloat162 *hh = reinterpret_cast<const __nv_bfloat162 *>(&v);
+        uint4 o;
+        __nv_bfloat162 *oo = reinterpret_cast<__nv_bfloat162 *>(&o);
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int c = 8 * c8 + 2 * q;
-                const float2 f = __bfloat1622float2(hh[q]);
-                lw[c] += gp * f.x;
-                lw[c + 1] += gp * f.y;
-                oo[q] = __floats2bfloat162_rn(gp * w[c], gp * w[c + 1]);
-            }
-            dv[c8] = o;
+        for (int q = 0; q < 4; q++) {
+            const float2 f = __bfloat1622float2(hh[q]);
+            lw[2 * q] += gp * f.x;
+            lw[2 * q + 1] += gp * f.y;
+            oo[q] = __floats2bfloat162_rn(gp * wr[2 * q], gp * wr[2 * q + 1]);
         }
+        dh[e] = o;
     }
-    for (int c = 0; c < C; c++) {
-        float v = lw[c];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((threadIdx.x & 31) == 0) atomicAdd(&dw[c], v);
-    }
+    for (int j = 0; j < 8; j++)
+        for (int o = G; o < 32; o <<= 1) lw[j] += __shfl_xor_sync(0xffffffffu, lw[j], o);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lb += __shfl_xor_sync(0xffffffffu, lb, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(db, lb);
+    if (lane < G) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) part[warp][8 * lane + j] = lw[j];
+    }
+    if (lane == 0) part[warp][64] = lb;
+    __syncthreads();
+    const int C = 8 * G, nw = blockDim.x >> 5;
+    if (threadIdx.x <= C) {
+        const int c = threadIdx.x < C ? threadIdx.x : 64;
+        float v = 0.f;
+        for (int k = 0; k < nw; k++) v += part[k][c];
+        atomicAdd(threadIdx.x < C ? &dw[c] : db, v);
+    }
 }
 
 // Adam on FP32 master weights; writes the BF16 compute copy (wb may be null)
@@ -830,9 +845,9 @@ int raft_unet_head(int backward, const void *h, const float *w, const float *b, 
     if (!backward)
         head_fwd_kernel<<<grid_for((size_t)N * HW), 256, 0, (cudaStream_t)stream>>>((const bf16 *)h, w, b, img, scale,
                                                                                     out_or_grad, N, HW, C);
-    else if (C % 8 == 0 && C <= 64 && ((uintptr_t)h | (uintptr_t)dh) % 16 == 0)
-        head_bwd_v8_kernel<<<grid_for((size_t)N * HW), 256, 0, (cudaStream_t)stream>>>((const bf16 *)h, w, out_or_grad,
-                                                                                       (bf16 *)dh, dw, db, N, HW, C);
+    else if (C % 8 == 0 && C <= 64 && ((C / 8) & (C / 8 - 1)) == 0 && ((uintptr_t)h | (uintptr_t)dh) % 16 == 0)
+        head_bwd_v8_kernel<<<grid_for((size_t)N * HW * (C / 8)), 256, 0, (cudaStream_t)stream>>>(
+            (const uint4 *)h, w, out_or_grad, (uint4 *)dh, dw, db, (size_t)N * HW, C / 8);
     else
         head_bwd_kernel<<<grid_for((size_t)N * HW), 256, 0, (cudaStream_t)stream>>>((const bf16 *)h, w, out_or_grad,
                                                                                     (bf16 *)dh, dw, db, N, HW, C);

@@ -91,6 +91,8 @@ libraft.raft_profile_enable.argtypes = [_I]
 libraft.raft_profile_enable.restype = None
 libraft.raft_profile_read.argtypes = [_P, _P, _I]
 libraft.raft_profile_read.restype = _I
+libraft.raft_filter_set_fixed.argtypes = [_I]
+libraft.raft_filter_set_fixed.restype = _I
 
 libraft.raft_slab_partition.argtypes = [_I, _I, _P, _P]
 libraft.raft_slab_partition.restype = _I

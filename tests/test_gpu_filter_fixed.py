@@ -1,0 +1,87 @@
+"""The filter kernels compiled for fixed padded lengths (2048, 3072, 4096,
+6144, 8192, 12288) against the generic filter kernel, through the C ABI.
+
+The fixed-length kernel keeps the generic kernel's radix order, twiddle
+expressions and butterflies; only the compiler's choice of fused multiply-adds
+may differ between the two, so whole FBP reconstructions with
+raft_filter_set_fixed(1) and (0) must agree to rel-L2 <= 1e-6 with FP32 rows
+(measured 2e-7) and <= 1e-4 with BF16 rows (measured 1-3e-5: a one-ulp FP32
+difference now and then moves a BF16 rounding); a misplaced element or
+twiddle shows as 1e-3 or more.  Every row format the filter writes is run: single floats in the four-slice interleaved layout (nearest operator),
+the same in the planar layout (nearest, backprojector forced to S = 2), FP32
+(mid, diff) pairs (linear) and BF16 pairs in the interleaved layout (linear).
+An odd angle count leaves a single row in each slice's last pair, five slices
+leave three zero slices in the last group of four, jittered angles make the
+angle weights unequal, and padding 0 with an axis offset puts window elements
+outside the padded row."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    # N, pad -> padded length
+    (1024, 1),   # 2048
+    (2048, 0),   # 2048, window beyond the row
+    (1024, 2),   # 3072
+    (2048, 1),   # 4096
+    (2048, 2),   # 6144
+    (4096, 1),   # 8192
+    (4096, 2),   # 12288
+]
+FORMATS = [
+    # geometry, store, RAFT_BP_TUNE
+    (0, 0, None),      # nearest, single floats, interleaved rows
+    (0, 0, "2,16"),    # nearest, single floats, planar rows
+    (1, 1, None),      # linear, FP32 pairs, planar rows
+    (1, 2, None),      # linear, BF16 pairs, interleaved rows
+]
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+@pytest.fixture
+def restore():
+    from sscRaft.rafttypes import libraft
+    old = os.environ.get("RAFT_BP_TUNE")
+    yield
+    libraft.raft_filter_set_fixed(1)
+    if old is None:
+        os.environ.pop("RAFT_BP_TUNE", None)
+    else:
+        os.environ["RAFT_BP_TUNE"] = old
+
+
+@pytest.mark.parametrize("N,pad", CASES)
+def test_fixed_length_filter_bit_identical_to_generic(N, pad, restore):
+    import torch
+    from sscRaft.rafttypes import _ptr, libraft
+    A, n = 21, 5
+    rng = np.random.default_rng(N + pad)
+    ang = np.sort((np.arange(A) + rng.uniform(-0.3, 0.3, A)) * (np.pi / A)).astype(np.float32)
+    sino = torch.from_numpy(rng.standard_normal((n, A, N)).astype(np.float32)).cuda()
+    pf = np.array([0, 0, 1, 0, 1, 1, 3.5], np.float32)
+    pi = np.array([N, A, n, N, pad, 0, 0, 5, 0, 0], np.int32)
+    for geometry, store, tune in FORMATS:
+        if tune is None:
+            os.environ.pop("RAFT_BP_TUNE", None)
+        else:
+            os.environ["RAFT_BP_TUNE"] = tune
+        outs = []
+        for fixed in (1, 0):
+            libraft.raft_filter_set_fixed(fixed)
+            out = torch.empty((n, N, N), device="cuda")
+            assert libraft.raft_fbp_device(0, _p(out), _p(sino), _ptr(ang), _ptr(pf), _ptr(pi), geometry, store,
+                                           None) == 0
+            outs.append(out)
+        assert torch.isfinite(outs[0]).all()
+        d = (outs[0] - outs[1]).double()
+        err = float(d.norm() / outs[1].double().norm())
+        print(f"Np={N * (1 + pad)} geometry={geometry} store={store} tune={tune}: "
+              f"rel-L2 {err:.2e}, max |diff| {float(d.abs().max()):.2e}")
+        assert err <= (1e-4 if store == 2 else 1e-6), (N, pad, geometry, store, tune, err)

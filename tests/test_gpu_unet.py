@@ -65,6 +65,33 @@ def test_conv_kernels_vs_oracle(oracle):
     assert rel_l2(_f64(d1), ref_dx[..., C0:]) <= 1e-2
 
 
+@pytest.mark.parametrize("C", [32, 8, 24])
+def test_head_backward_vs_fp64(C):
+    """raft_unet_head backward: dh[p][c] = bf16(g[p] * w[c]) bit for bit (one
+    FP32 product, rounded to nearest even), dw[c] = sum_p g[p] h[p][c] and
+    db = sum_p g[p] within 1e-5 of FP64.  C = 32 and 8 take the 16-byte-vector
+    kernel (8-channel groups per thread), C = 24 the scalar one."""
+    import torch
+    from sscRaft import warmstart as ws
+    from sscRaft.rafttypes import libraft
+    torch.manual_seed(C)
+    N, HW = 3, 257 * 129
+    h = _bf(torch.randn(N, HW, C, device="cuda"))
+    w = torch.randn(C, device="cuda")
+    g = torch.randn(N, HW, device="cuda")
+    dh = torch.empty_like(h)
+    dw = torch.zeros(C, device="cuda")
+    db = torch.zeros(1, device="cuda")
+    assert libraft.raft_unet_head(1, ws._p(h), ws._p(w), None, None, None, ws._p(g), ws._p(dh), ws._p(dw),
+                                  ws._p(db), N, HW, C, None) == 0
+    torch.cuda.synchronize()
+    want_dh = (g[..., None] * w).to(torch.bfloat16)
+    assert torch.equal(dh.view(torch.int16), want_dh.view(torch.int16))
+    gd, hd = _f64(g), _f64(h)
+    assert rel_l2(_f64(dw), np.einsum("np,npc->c", gd, hd)) <= 1e-5
+    assert abs(float(db.item()) - gd.sum()) <= 1e-5 * np.abs(gd).sum()
+
+
 def _torch_unet(net, img, scale):
     """The same network in plain PyTorch FP32 (NCHW), for the gradient check."""
     import torch
