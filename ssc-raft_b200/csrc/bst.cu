@@ -64,6 +64,20 @@ struct BstArgs {
     float scale;
 };
 
+// The transforms of the three kernels: NF > 0 is the compile-time length
+// that every transform of the launch has (cfft_smem), 0 the plans' lengths.
+template <int NF>
+__device__ __forceinline__ float2 *bst_fft(float2 *a, float2 *b, const FftPlan &P)
+{
+    if constexpr (NF > 0) {
+        (void)P;
+        return cfft_smem<NF>(a, b);
+    } else {
+        return fft_run(a, b, P);
+    }
+}
+
+template <int NF>
 __global__ void __launch_bounds__(512) bst_rows_kernel(const BstArgs p)
 {
     extern __shared__ float2 sm_bst[];
@@ -80,14 +94,14 @@ __global__ void __launch_bounds__(512) bst_rows_kernel(const BstArgs p)
     __syncthreads();
     float sgn1 = 1.f;   // the second row is sgn1 * z.y
     if (p.G) {
-        float2 *r = fft_run(z, sm_bst + p.M, p.pN);
+        float2 *r = bst_fft<NF>(z, sm_bst + p.M, p.pN);
         for (int k = threadIdx.x; k < p.Np; k += blockDim.x) {
             const float2 g = cmul(r[k], __ldg(&p.G[k]));
             r[k] = make_float2(g.x, -g.y);
         }
         __syncthreads();
         // forward transform of the conjugate = conjugate of the inverse
-        z = fft_run(r, r == sm_bst ? sm_bst + p.M : sm_bst, p.pN);
+        z = bst_fft<NF>(r, r == sm_bst ? sm_bst + p.M : sm_bst, p.pN);
         sgn1 = -1.f;
     }
     // two buffers of M elements: the filtered pair z, and the other one.  The
@@ -117,7 +131,7 @@ __global__ void __launch_bounds__(512) bst_rows_kernel(const BstArgs p)
             fa[idx] = h;
         }
         __syncthreads();
-        const float2 *H = fft_run(fa, fb, p.pL);
+        const float2 *H = bst_fft<NF>(fa, fb, p.pL);
         float2 *frow = p.polar + pb + (size_t)(a0 + r) * p.Lh;           // left half-ray (theta + pi)
         float2 *rrow = p.polar + pb + (size_t)(p.A + a0 + r) * p.Lh;     // right half-ray (theta)
         for (int k = threadIdx.x; k < p.Lh; k += blockDim.x) {
@@ -134,6 +148,7 @@ __global__ void __launch_bounds__(512) bst_rows_kernel(const BstArgs p)
     }
 }
 
+template <int NF>
 __global__ void __launch_bounds__(512) bst_regrid_kernel(const BstArgs p)
 {
     extern __shared__ float2 sm_bst[];
@@ -168,13 +183,14 @@ __global__ void __launch_bounds__(512) bst_regrid_kernel(const BstArgs p)
         sm_bst[X] = make_float2(v.x * sgn, -v.y * sgn);   // conjugated: see bst_cols_kernel
     }
     __syncthreads();
-    const float2 *r = fft_run(sm_bst, sm_bst + fft_plan_span(p.pS), p.pS);
+    const float2 *r = bst_fft<NF>(sm_bst, sm_bst + fft_plan_span(p.pS), p.pS);
     float2 *trow = p.T + ((size_t)slice * S + Y) * p.N;
     for (int i = threadIdx.x; i < p.N; i += blockDim.x) trow[i] = r[p.off + i];
 }
 
 // T holds conj(IFFT_x(grid)); its forward transform along y is the conjugate
 // of the 2-D inverse transform, whose real part is the image.
+template <int NF>
 __global__ void __launch_bounds__(512) bst_cols_kernel(const BstArgs p)
 {
     extern __shared__ float2 sm_bst[];
@@ -182,7 +198,7 @@ __global__ void __launch_bounds__(512) bst_cols_kernel(const BstArgs p)
     const float2 *tcol = p.T + (size_t)slice * p.S * p.N + i;
     for (int Y = threadIdx.x; Y < p.S; Y += blockDim.x) sm_bst[Y] = tcol[(size_t)Y * p.N];
     __syncthreads();
-    const float2 *r = fft_run(sm_bst, sm_bst + fft_plan_span(p.pS), p.pS);
+    const float2 *r = bst_fft<NF>(sm_bst, sm_bst + fft_plan_span(p.pS), p.pS);
     float *o = p.obj + (size_t)slice * p.N * p.N + i;
     for (int j = threadIdx.x; j < p.N; j += blockDim.x) o[(size_t)j * p.N] = r[p.off + j].x / p.scale;
 }
@@ -359,6 +375,33 @@ size_t bst_core_workspace_bytes(const BstCore &c, int nslices)
     return ((polar + 255) & ~(size_t)255) + T;
 }
 
+template <int NF>
+static void launch_bst_kernels(const BstArgs &a, const BstCore &c, int nslices, int threads, size_t sm3, size_t sm2,
+                               cudaStream_t st)
+{
+    RAFT_CHECK(NF == 0 || threads == c_fft_threads(NF), "BST: thread count of the compile-time transforms");
+    static thread_local int configured = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured != dev) {
+        RAFT_CUDA(cudaFuncSetAttribute(bst_rows_kernel<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kBstSmemMax));
+        RAFT_CUDA(cudaFuncSetAttribute(bst_regrid_kernel<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kBstSmemMax));
+        RAFT_CUDA(cudaFuncSetAttribute(bst_cols_kernel<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kBstSmemMax));
+        configured = dev;
+    }
+    bst_rows_kernel<NF><<<dim3((c.A + 1) / 2, nslices), threads, sm3, st>>>(a);
+    RAFT_CUDA(cudaGetLastError());
+    count_launch();
+    bst_regrid_kernel<NF><<<dim3(c.S, nslices), threads, sm2, st>>>(a);
+    RAFT_CUDA(cudaGetLastError());
+    count_launch();
+    bst_cols_kernel<NF><<<dim3(c.N, nslices), threads, sm2, st>>>(a);
+    RAFT_CUDA(cudaGetLastError());
+}
+
 void bst_run(int device, const BstCore &c, const float *d_tomo, float *d_obj, int nslices, void *workspace,
              cudaStream_t st)
 {
@@ -387,24 +430,20 @@ void bst_run(int device, const BstCore &c, const float *d_tomo, float *d_obj, in
     a.scale = c.scale;
     const int threads = fft_threads(std::max({c.M, a.pN.M, a.pL.M, a.pS.M}));
     const size_t sm3 = 2 * (size_t)a.M * sizeof(float2), sm2 = 2 * (size_t)fft_plan_span(a.pS) * sizeof(float2);
-    static thread_local int configured = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured != dev) {
-        RAFT_CUDA(cudaFuncSetAttribute(bst_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBstSmemMax));
-        RAFT_CUDA(cudaFuncSetAttribute(bst_regrid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBstSmemMax));
-        RAFT_CUDA(cudaFuncSetAttribute(bst_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBstSmemMax));
-        configured = dev;
-    }
+    // one compile-time length for every transform of the launch, when it is one of those compiled
+    const bool same = (!c.G || (a.pN.n == c.S && a.pN.M == c.S)) && a.pL.n == c.S && a.pL.M == c.S &&
+                      a.pS.n == c.S && a.pS.M == c.S && threads == c_fft_threads(c.S) &&
+                      fixed_transforms_enabled();
     ProfScope ps(PROF_OTHER, st);   // counts the first of the three launches
-    bst_rows_kernel<<<dim3((c.A + 1) / 2, nslices), threads, sm3, st>>>(a);
-    RAFT_CUDA(cudaGetLastError());
-    count_launch();
-    bst_regrid_kernel<<<dim3(c.S, nslices), threads, sm2, st>>>(a);
-    RAFT_CUDA(cudaGetLastError());
-    count_launch();
-    bst_cols_kernel<<<dim3(c.N, nslices), threads, sm2, st>>>(a);
-    RAFT_CUDA(cudaGetLastError());
+    switch (same ? c.S : 0) {
+    case 2048: launch_bst_kernels<2048>(a, c, nslices, threads, sm3, sm2, st); break;
+    case 3072: launch_bst_kernels<3072>(a, c, nslices, threads, sm3, sm2, st); break;
+    case 4096: launch_bst_kernels<4096>(a, c, nslices, threads, sm3, sm2, st); break;
+    case 6144: launch_bst_kernels<6144>(a, c, nslices, threads, sm3, sm2, st); break;
+    case 8192: launch_bst_kernels<8192>(a, c, nslices, threads, sm3, sm2, st); break;
+    case 12288: launch_bst_kernels<12288>(a, c, nslices, threads, sm3, sm2, st); break;
+    default: launch_bst_kernels<0>(a, c, nslices, threads, sm3, sm2, st); break;
+    }
 }
 
 void launch_bst(int device, const FbpConfig &cfg, const float *d_tomo, float *d_obj, int nslices, void *workspace,

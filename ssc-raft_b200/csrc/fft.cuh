@@ -413,6 +413,35 @@ __device__ __forceinline__ void cfft_passes(float2 *a, float2 *b, const First &f
 template <int NP>
 __host__ __device__ constexpr int cfft_out_buffer() { return c_factorize(NP).n % 2 == 1 ? 1 : 0; }
 
+// Plain-order shared-memory output of the last pass (NS R = NP: q = 0).
+template <int R, int NS>
+struct CPlainOut {
+    float2 *d;
+    __device__ __forceinline__ void operator()(int q, int k, const float2 (&v)[R]) const
+    {
+        (void)q;
+#pragma unroll
+        for (int r = 0; r < R; r++) d[k + r * NS] = v[r];
+    }
+};
+struct CPlainLast {
+    float2 *d;
+    template <int R, int NS> __device__ __forceinline__ CPlainOut<R, NS> at() const { return {d}; }
+};
+
+// fft_forward for a compile-time length with blockDim.x == c_fft_threads(NP):
+// the NP values in a (plain order) are transformed, the result (plain order)
+// is left in the returned buffer, a or b, after a barrier.
+template <int NP>
+__device__ __forceinline__ float2 *cfft_smem(float2 *a, float2 *b)
+{
+    constexpr CRadices rl = c_factorize(NP);
+    float2 *out = cfft_out_buffer<NP>() ? b : a;
+    cfft_passes<NP, 0, 1>(a, b, CSmemIn<NP, c_fft_threads(NP), rl.r[0], false>(a), CPlainLast{out});
+    __syncthreads();
+    return out;
+}
+
 // ------------------------------------------------------- any length --
 // A forward DFT of any length n held in shared memory: directly when n has
 // only the prime factors 2, 3, 5, 7, otherwise by Bluestein's chirp-z

@@ -385,20 +385,6 @@ struct FxSpecLast {
     const float2 *H;
     template <int R, int NS> __device__ __forceinline__ FxSpecOut<R, NS> at() const { return {d, H}; }
 };
-template <int R, int NS>
-struct FxPlainOut {
-    float2 *d;
-    __device__ __forceinline__ void operator()(int q, int k, const float2 (&v)[R]) const
-    {
-        (void)q;
-#pragma unroll
-        for (int r = 0; r < R; r++) d[k + r * NS] = v[r];
-    }
-};
-struct FxPlainLast {
-    float2 *d;
-    template <int R, int NS> __device__ __forceinline__ FxPlainOut<R, NS> at() const { return {d}; }
-};
 // window element e = u - wlo of both rows, from filtered sample u (registers)
 struct FxWindow {
     float *out;
@@ -480,7 +466,7 @@ filter_fixed_kernel(const float *__restrict__ sino, int N, int off, int nslices,
         }
     } else {
         float2 *Z = cfft_out_buffer<NP>() ? Y : X;
-        cfft_passes<NP, 0, 1>(X, Y, spec, FxPlainLast{Z});
+        cfft_passes<NP, 0, 1>(X, Y, spec, CPlainLast{Z});
         __syncthreads();
         pack_row(Z, rp.k, rp.a0, 0, pk);
         if (has1) pack_row(Z, rp.k, rp.a0 + 1, 1, pk);
@@ -488,6 +474,7 @@ filter_fixed_kernel(const float *__restrict__ sino, int N, int off, int nslices,
 }
 
 static bool g_fixed_filter = true;
+bool fixed_transforms_enabled() { return g_fixed_filter; }
 
 template <int NP, bool IL, bool FUSED>
 static void launch_fixed_one(const FilterPlan &plan, const FilterLaunch &fl, const PackArgs &pk, int nsl,
@@ -874,8 +861,9 @@ bool filter_plan_shape(FilterPlan &plan, int ftype, int N, int pad)
 }  // namespace raft
 
 extern "C" {
-// 1 (default): padded lengths 2048, 3072, 4096, 6144, 8192 and 12288 run the
-// compile-time-length filter kernel; 0: every length runs the generic one.
+// 1 (default): transforms of 2048, 3072, 4096, 6144, 8192 and 12288 points
+// (FBP filter rows, BST) run the compile-time-length kernels; 0: every length
+// runs the generic ones.
 int raft_filter_set_fixed(int on)
 {
     raft::g_fixed_filter = on != 0;

@@ -296,6 +296,8 @@ struct BstCore {
     float w_half = 4.0f, scale = 1.0f;
 };
 bool bst_core_ok(const BstCore &c);
+// Compile-time-length transform kernels in use (raft_filter_set_fixed).
+bool fixed_transforms_enabled();
 size_t bst_core_workspace_bytes(const BstCore &c, int nslices);
 void bst_run(int device, const BstCore &c, const float *d_tomo, float *d_obj, int nslices, void *workspace,
              cudaStream_t st);

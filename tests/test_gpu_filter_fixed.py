@@ -1,5 +1,6 @@
-"""The filter kernels compiled for fixed padded lengths (2048, 3072, 4096,
-6144, 8192, 12288) against the generic filter kernel, through the C ABI.
+"""The transform kernels compiled for fixed lengths (2048, 3072, 4096, 6144,
+8192, 12288 points: FBP filter rows and BST) against the generic ones,
+through the C ABI.
 
 The fixed-length kernel keeps the generic kernel's radix order, twiddle
 expressions and butterflies; only the compiler's choice of fused multiply-adds
@@ -13,7 +14,9 @@ the same in the planar layout (nearest, backprojector forced to S = 2), FP32
 An odd angle count leaves a single row in each slice's last pair, five slices
 leave three zero slices in the last group of four, jittered angles make the
 angle weights unequal, and padding 0 with an axis offset puts window elements
-outside the padded row."""
+outside the padded row.  BST (rows, half-rays and grid all of the padded
+length) must agree to rel-L2 <= 1e-6 as well, filtered and with the 'none'
+filter."""
 import ctypes
 import os
 
@@ -85,3 +88,28 @@ def test_fixed_length_filter_bit_identical_to_generic(N, pad, restore):
         print(f"Np={N * (1 + pad)} geometry={geometry} store={store} tune={tune}: "
               f"rel-L2 {err:.2e}, max |diff| {float(d.abs().max()):.2e}")
         assert err <= (1e-4 if store == 2 else 1e-6), (N, pad, geometry, store, tune, err)
+
+
+@pytest.mark.parametrize("N,pad,ftype", [(1024, 1, 7), (1024, 2, 5), (2048, 1, 5), (2048, 2, 5), (2048, 2, 0),
+                                         (4096, 1, 7)])
+def test_fixed_length_bst_matches_generic(N, pad, ftype, restore):
+    from sscRaft.rafttypes import check_error, libraft
+    A, n = 33, 2
+    rng = np.random.default_rng(N + pad + ftype)
+    sino = np.ascontiguousarray(rng.standard_normal((n, A, N)).astype(np.float32))
+    ang = np.linspace(0, np.pi, A, endpoint=False).astype(np.float32)
+    pi = np.array([N, A, n, N, pad, 0, 0, ftype, 0, 0], np.int32)
+    pf = np.array([0, 0, 1, 0, 1, 1, 2.0], np.float32)
+    g = np.array([0], np.intc)
+    outs = []
+    for fixed in (1, 0):
+        libraft.raft_filter_set_fixed(fixed)
+        obj = np.zeros((n, N, N), np.float32)
+        libraft.getBSTMultiGPU(g.ctypes.data, 1, obj.ctypes.data, sino.ctypes.data, ang.ctypes.data,
+                               pf.ctypes.data, pi.ctypes.data, 0)
+        check_error("bst")
+        outs.append(obj)
+    assert np.all(np.isfinite(outs[0]))
+    err = float(np.linalg.norm((outs[0] - outs[1]).astype(np.float64)) / np.linalg.norm(outs[1].astype(np.float64)))
+    print(f"BST Np={N * (1 + pad)} ftype={ftype}: rel-L2 {err:.2e}")
+    assert err <= 1e-6, (N, pad, ftype, err)
