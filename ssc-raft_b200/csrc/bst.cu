@@ -436,6 +436,8 @@ void bst_run(int device, const BstCore &c, const float *d_tomo, float *d_obj, in
                       fixed_transforms_enabled();
     ProfScope ps(PROF_OTHER, st);   // counts the first of the three launches
     switch (same ? c.S : 0) {
+    case 1024: launch_bst_kernels<1024>(a, c, nslices, threads, sm3, sm2, st); break;
+    case 1536: launch_bst_kernels<1536>(a, c, nslices, threads, sm3, sm2, st); break;
     case 2048: launch_bst_kernels<2048>(a, c, nslices, threads, sm3, sm2, st); break;
     case 3072: launch_bst_kernels<3072>(a, c, nslices, threads, sm3, sm2, st); break;
     case 4096: launch_bst_kernels<4096>(a, c, nslices, threads, sm3, sm2, st); break;

@@ -414,11 +414,16 @@ struct FxWinLast {
     template <int R, int NS> __device__ __forceinline__ FxWinOut<R, NS> at() const { return {w}; }
 };
 
+// CTAs per SM the launch bounds ask for: as many as shared memory and the
+// thread limit allow, but no fewer than 64 registers per thread.
+__host__ __device__ constexpr int cmin(int a, int b) { return a < b ? a : b; }
 __host__ __device__ constexpr int fixed_filter_min_blocks(int NP)
 {
-    return (220 * 1024) / (2 * fft_span(NP) * 8) < 1 ? 1
-         : ((220 * 1024) / (2 * fft_span(NP) * 8) > 2048 / c_fft_threads(NP) ? 2048 / c_fft_threads(NP)
-                                                                            : (220 * 1024) / (2 * fft_span(NP) * 8));
+    return cmin(cmin((220 * 1024) / (2 * fft_span(NP) * 8), 2048 / c_fft_threads(NP)),
+                65536 / (64 * c_fft_threads(NP))) < 1
+               ? 1
+               : cmin(cmin((220 * 1024) / (2 * fft_span(NP) * 8), 2048 / c_fft_threads(NP)),
+                      65536 / (64 * c_fft_threads(NP)));
 }
 
 template <int NP, bool IL, bool FUSED>
@@ -516,6 +521,8 @@ static bool launch_fixed_filter(const FilterPlan &plan, const FilterLaunch &fl, 
 {
     if (!g_fixed_filter) return false;
     switch (plan.Np) {
+    case 1024: launch_fixed_np<1024>(plan, fl, pk, nsl, st); return true;
+    case 1536: launch_fixed_np<1536>(plan, fl, pk, nsl, st); return true;
     case 2048: launch_fixed_np<2048>(plan, fl, pk, nsl, st); return true;
     case 3072: launch_fixed_np<3072>(plan, fl, pk, nsl, st); return true;
     case 4096: launch_fixed_np<4096>(plan, fl, pk, nsl, st); return true;
@@ -861,7 +868,7 @@ bool filter_plan_shape(FilterPlan &plan, int ftype, int N, int pad)
 }  // namespace raft
 
 extern "C" {
-// 1 (default): transforms of 2048, 3072, 4096, 6144, 8192 and 12288 points
+// 1 (default): transforms of 1024, 1536, 2048, 3072, 4096, 6144, 8192 and 12288 points
 // (FBP filter rows, BST) run the compile-time-length kernels; 0: every length
 // runs the generic ones.
 int raft_filter_set_fixed(int on)

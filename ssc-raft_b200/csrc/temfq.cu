@@ -48,8 +48,22 @@ struct FstArgs {
     float scale;
 };
 
+// The L-point transforms: NL > 0 is L as a compile-time constant (cfft_smem,
+// launched with c_fft_threads(NL) threads), 0 the plan's length.
+template <int NL>
+__device__ __forceinline__ const float2 *fst_fft(float2 *a, float2 *b, const FftPlan &P)
+{
+    if constexpr (NL > 0) {
+        (void)P;
+        return cfft_smem<NL>(a, b);
+    } else {
+        return fft_run(a, b, P);
+    }
+}
+
 // Grid row q (q < N/2: row q; else row q + L - N) holds row q of the
 // fftshifted image in its first N/2 and last N/2 columns.
+template <int NL>
 __global__ void __launch_bounds__(512) fst_rows_kernel(const FstArgs p)
 {
     extern __shared__ float2 sm_fst[];
@@ -63,11 +77,12 @@ __global__ void __launch_bounds__(512) fst_rows_kernel(const FstArgs p)
         sm_fst[c] = make_float2(v, 0.f);
     }
     __syncthreads();
-    const float2 *r = fft_run(sm_fst, sm_fst + fft_plan_span(p.pL), p.pL);
+    const float2 *r = fst_fft<NL>(sm_fst, sm_fst + fft_plan_span(p.pL), p.pL);
     float2 *dst = p.rows + ((size_t)b * N + q) * L;
     for (int c = threadIdx.x; c < L; c += blockDim.x) dst[c] = r[c];
 }
 
+template <int NL>
 __global__ void __launch_bounds__(512) fst_cols_kernel(const FstArgs p)
 {
     extern __shared__ float2 sm_fst[];
@@ -78,7 +93,7 @@ __global__ void __launch_bounds__(512) fst_cols_kernel(const FstArgs p)
     const float2 *col = p.rows + (size_t)b * N * L + c;
     for (int q = threadIdx.x; q < N; q += blockDim.x) sm_fst[q < h ? q : q + L - N] = col[(size_t)q * L];
     __syncthreads();
-    const float2 *r = fft_run(sm_fst, sm_fst + fft_plan_span(p.pL), p.pL);
+    const float2 *r = fst_fft<NL>(sm_fst, sm_fst + fft_plan_span(p.pL), p.pL);
     float2 *dst = p.spec + ((size_t)b * L + c) * L;
     for (int y = threadIdx.x; y < L; y += blockDim.x) dst[y] = r[y];
 }
@@ -94,6 +109,7 @@ __device__ __forceinline__ float2 shifted_spec(const float2 *spec, int L, long l
     return spec[(size_t)x * L + y];
 }
 
+template <int NL>
 __global__ void __launch_bounds__(512) fst_sino_kernel(const FstArgs p)
 {
     extern __shared__ float2 sm_fst[];
@@ -138,7 +154,7 @@ __global__ void __launch_bounds__(512) fst_sino_kernel(const FstArgs p)
         sm_fst[qq] = make_float2(v.x, -v.y);               // conjugate: inverse = conj(forward(conj))
     }
     __syncthreads();
-    const float2 *H = fft_run(sm_fst, sm_fst + fft_plan_span(p.pL), p.pL);
+    const float2 *H = fst_fft<NL>(sm_fst, sm_fst + fft_plan_span(p.pL), p.pL);
     const float *fl = p.flat + (size_t)b * N;
     float *out = p.model + ((size_t)b * p.A + a) * N;
     for (int i = threadIdx.x; i < N; i += blockDim.x) {
@@ -146,6 +162,22 @@ __global__ void __launch_bounds__(512) fst_sino_kernel(const FstArgs p)
         const float proj = H[m].x * p.scale;               // real part (conjugation keeps it)
         out[i] = proj < 0.f ? fl[i] : fl[i] * __expf(-proj);
     }
+}
+
+template <int NL>
+static void launch_fst(const FstArgs &f, int nslices, int threads, size_t sm, cudaStream_t st)
+{
+    RAFT_CUDA(cudaFuncSetAttribute(fst_rows_kernel<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    RAFT_CUDA(cudaFuncSetAttribute(fst_cols_kernel<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    RAFT_CUDA(cudaFuncSetAttribute(fst_sino_kernel<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    fst_rows_kernel<NL><<<dim3(f.N, nslices), threads, sm, st>>>(f);
+    RAFT_CUDA(cudaGetLastError());
+    count_launch();
+    fst_cols_kernel<NL><<<dim3(f.L, nslices), threads, sm, st>>>(f);
+    RAFT_CUDA(cudaGetLastError());
+    count_launch();
+    fst_sino_kernel<NL><<<dim3(f.A, nslices), threads, sm, st>>>(f);
+    RAFT_CUDA(cudaGetLastError());
 }
 
 // calc_reciprocal_element_wise: 1.0 / x in double, stored as float
@@ -262,20 +294,23 @@ void temfq_run(int device, const TemfqConfig &cfg, float *d_obj, const float *d_
     f.scale = cfg.dx > 0.f ? cfg.dx / (float)L : (float)(1.0 / (float)L);
     const size_t sm = 2 * (size_t)fft_plan_span(f.pL) * sizeof(float2);
     const int threads = fft_threads(f.pL.M);
-    RAFT_CUDA(cudaFuncSetAttribute(fst_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    RAFT_CUDA(cudaFuncSetAttribute(fst_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    RAFT_CUDA(cudaFuncSetAttribute(fst_sino_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    // L as a compile-time length when it is one of those compiled
+    const int fixedL = (f.pL.n == L && f.pL.M == L && threads == c_fft_threads(L) && fixed_transforms_enabled())
+                           ? L : 0;
     for (int k = 0; k < cfg.niter; k++) {
         {
             ProfScope ps(PROF_PROJECT, st);   // counts the first of the three FST launches
-            fst_rows_kernel<<<dim3(N, nslices), threads, sm, st>>>(f);
-            RAFT_CUDA(cudaGetLastError());
-            count_launch();
-            fst_cols_kernel<<<dim3(L, nslices), threads, sm, st>>>(f);
-            RAFT_CUDA(cudaGetLastError());
-            count_launch();
-            fst_sino_kernel<<<dim3(A, nslices), threads, sm, st>>>(f);
-            RAFT_CUDA(cudaGetLastError());
+            switch (fixedL) {
+            case 1024: launch_fst<1024>(f, nslices, threads, sm, st); break;
+            case 1536: launch_fst<1536>(f, nslices, threads, sm, st); break;
+            case 2048: launch_fst<2048>(f, nslices, threads, sm, st); break;
+            case 3072: launch_fst<3072>(f, nslices, threads, sm, st); break;
+            case 4096: launch_fst<4096>(f, nslices, threads, sm, st); break;
+            case 6144: launch_fst<6144>(f, nslices, threads, sm, st); break;
+            case 8192: launch_fst<8192>(f, nslices, threads, sm, st); break;
+            case 12288: launch_fst<12288>(f, nslices, threads, sm, st); break;
+            default: launch_fst<0>(f, nslices, threads, sm, st); break;
+            }
         }
         bst_run(device, core, sino, back, nslices, bst_ws, st);
         count_launch();

@@ -1,5 +1,5 @@
-"""The transform kernels compiled for fixed lengths (2048, 3072, 4096, 6144,
-8192, 12288 points: FBP filter rows and BST) against the generic ones,
+"""The transform kernels compiled for fixed lengths (1024, 1536, 2048, 3072,
+4096, 6144, 8192, 12288 points: FBP filter rows, BST, tEMFQ) against the generic ones,
 through the C ABI.
 
 The fixed-length kernel keeps the generic kernel's radix order, twiddle
@@ -16,7 +16,9 @@ leave three zero slices in the last group of four, jittered angles make the
 angle weights unequal, and padding 0 with an axis offset puts window elements
 outside the padded row.  BST (rows, half-rays and grid all of the padded
 length) must agree to rel-L2 <= 1e-6 as well, filtered and with the 'none'
-filter."""
+filter, and tEMFQ (Fourier-slice projector transforms of L = N (1 + zpad)
+points; two EM iterations, which multiply the rounding into the object) to
+rel-L2 <= 1e-5."""
 import ctypes
 import os
 
@@ -27,6 +29,8 @@ pytestmark = pytest.mark.gpu
 
 CASES = [
     # N, pad -> padded length
+    (512, 1),    # 1024
+    (512, 2),    # 1536
     (1024, 1),   # 2048
     (2048, 0),   # 2048, window beyond the row
     (1024, 2),   # 3072
@@ -90,7 +94,7 @@ def test_fixed_length_filter_bit_identical_to_generic(N, pad, restore):
         assert err <= (1e-4 if store == 2 else 1e-6), (N, pad, geometry, store, tune, err)
 
 
-@pytest.mark.parametrize("N,pad,ftype", [(1024, 1, 7), (1024, 2, 5), (2048, 1, 5), (2048, 2, 5), (2048, 2, 0),
+@pytest.mark.parametrize("N,pad,ftype", [(512, 2, 5), (1024, 1, 7), (1024, 2, 5), (2048, 1, 5), (2048, 2, 5), (2048, 2, 0),
                                          (4096, 1, 7)])
 def test_fixed_length_bst_matches_generic(N, pad, ftype, restore):
     from sscRaft.rafttypes import check_error, libraft
@@ -113,3 +117,28 @@ def test_fixed_length_bst_matches_generic(N, pad, ftype, restore):
     err = float(np.linalg.norm((outs[0] - outs[1]).astype(np.float64)) / np.linalg.norm(outs[1].astype(np.float64)))
     print(f"BST Np={N * (1 + pad)} ftype={ftype}: rel-L2 {err:.2e}")
     assert err <= 1e-6, (N, pad, ftype, err)
+
+
+@pytest.mark.parametrize("N,zpad,interp", [(512, 2, 1), (1024, 1, 1), (1024, 2, 1), (1024, 2, 0), (2048, 1, 1)])
+def test_fixed_length_temfq_matches_generic(N, zpad, interp, restore):
+    from sscRaft.rafttypes import check_error, libraft
+    A, B, niter, dx = 45, 2, 2, 0.02
+    rng = np.random.default_rng(N + zpad + interp)
+    flat = np.ascontiguousarray(1e4 * (1 + 0.05 * rng.random((B, N))), np.float32)
+    counts = np.ascontiguousarray(rng.poisson(flat[:, None, :] * np.exp(-rng.random((B, A, N)))), np.float32)
+    ang = (np.arange(A) * (np.pi / A)).astype(np.float32)
+    pi = np.array([N, A, B, N, zpad, 0, 0, B, niter, interp, 0], np.int32)
+    pf = np.array([dx, dx, 0.0], np.float32)
+    g = np.array([0], np.intc)
+    outs = []
+    for fixed in (1, 0):
+        libraft.raft_filter_set_fixed(fixed)
+        obj = np.ones((B, N, N), np.float32)
+        libraft.get_tEM_FQ_MultiGPU(g.ctypes.data, 1, counts.ctypes.data, obj.ctypes.data, ang.ctypes.data,
+                                    flat.ctypes.data, pf.ctypes.data, pi.ctypes.data)
+        check_error("temfq")
+        outs.append(obj)
+    assert np.all(np.isfinite(outs[0]))
+    err = float(np.linalg.norm((outs[0] - outs[1]).astype(np.float64)) / np.linalg.norm(outs[1].astype(np.float64)))
+    print(f"tEMFQ L={N * (1 + zpad)} interp={interp}: rel-L2 {err:.2e}")
+    assert err <= 1e-5, (N, zpad, interp, err)
