@@ -25,37 +25,38 @@
 #include "profile.hpp"
 
 #include <cstdlib>
+#include <type_traits>
 
 namespace raft {
 
 constexpr int PJ_WARPS = 8;   // 256 threads per block
 
-// Thread -> (ray, angle) shapes.  A warp covers RW neighbouring rays at 32/RW
-// neighbouring angles; a block covers BR rays x BA angles.  The lanes of a
-// warp load their samples together.  With one angle per warp (RW = 32) the
-// 32 pixels lie on a line across the ray direction, one pixel apart: along an
-// image row near 0 degrees, but on ~23 different rows (23 cache lines) near
-// 45 degrees.  Rays of neighbouring angles at the same detector position
-// sample points only |s| * dtheta apart (s = distance from the rotation
-// centre), so a warp of a few rays at several angles touches far fewer lines.
-// That is what limits single-slice projection (one 4-byte pixel per lane: the
-// L1 tag stage, one line per cycle); eight interleaved slices per lane (32
-// bytes) are bound by the L1 data stage instead, where one angle per warp
-// measured fastest.  Each thread still sums its own ray's samples in order,
-// so every shape gives the same bits.
-template <int RW> struct PjShape {
-    static constexpr int AW = 32 / RW;            // angles per warp
-    static constexpr int BR = RW >= 4 ? 32 : 16;  // rays per block
-    static constexpr int BA = 256 / BR;           // angles per block
+// Thread -> (ray, angle, sample phase) shapes.  A warp covers RW neighbouring
+// rays at AW = 32 / (RW PH) neighbouring angles, each ray's samples split over
+// PH lanes (lane ph sums samples m = ph, ph + PH, ... in order; the PH partial
+// sums are then combined by a fixed butterfly of warp shuffles, so the
+// summation order depends on PH alone, not on the slice count, the layout or
+// the ray/angle shape); a block covers BR rays x BA angles.  The lanes of a
+// warp load their samples together.  With one angle and one phase per warp
+// (RW = 32) the 32 pixels lie on a line across the ray direction, one pixel
+// apart: along an image row near 0 degrees, but on ~23 different rows near 45
+// degrees.  A few rays x a few consecutive samples cover a compact
+// parallelogram instead (about 12 cache lines per warp load of 32-byte pixels
+// against 15-17 for the line, averaged over angles).  Measured (B200, 512 x
+// 1024^2 x 900): interleaved 8-slice images four rays x four phases x two
+// angles, Radon 5096 GUPS against 4655 for one angle x 32 rays, tEM 176.7
+// against 182.1 ms per iteration; planar single-slice projection (instruction
+// issue bound) is best sequential (ragged batch 1863 GUPS) and costs 3.7 % at
+// PH = 4 (eight rays x four phases, 1795 GUPS), kept so that every slice count
+// sums in the same order.
+template <int RW, int PH, int BRS> struct PjShape {
+    static_assert(32 % (RW * PH) == 0, "a warp holds whole (ray, phase) groups");
+    static constexpr int AW = 32 / (RW * PH);     // angles per warp
+    static constexpr int BR = BRS;                // rays per block
+    static constexpr int BA = 256 / (BR * PH);    // angles per block
     static constexpr int WR = BR / RW;            // warps along the rays
+    static_assert(BR % RW == 0 && BA % AW == 0 && WR * (BA / AW) == 8, "eight warps per block");
 };
-
-__device__ __forceinline__ double warp_sum(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 
 // S slices per thread share every sample's position and pixel index (the
 // geometry is the same for all slices).  Warps whose angle is steeper than
@@ -72,22 +73,24 @@ __device__ __forceinline__ void ldg_v8(const float *p, float (&w)[8])
                  : "l"(p));
 }
 
-template <int EM, int EPI, int S, int IL, int RW>
+template <int EM, int EPI, int S, int IL, int RW, int PH, int BRS>
 __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx, const int by, const int bz)
 {
     static_assert(!IL || S == 8, "interleaved images hold groups of 8 slices");
-    using Sh = PjShape<RW>;
+    using Sh = PjShape<RW, PH, BRS>;
     const int w = threadIdx.y, lane = threadIdx.x;
-    const int i = bx * Sh::BR + (w % Sh::WR) * RW + lane % RW;     // ray
-    const int j = by * Sh::BA + (w / Sh::WR) * Sh::AW + lane / RW;  // angle
+    const int ph = lane / (RW * Sh::AW);                                      // sample phase
+    const int i = bx * Sh::BR + (w % Sh::WR) * RW + lane % RW;                // ray
+    const int j = by * Sh::BA + (w / Sh::WR) * Sh::AW + (lane / RW) % Sh::AW;  // angle
     const int k0 = bz * S;                        // first slice
     const int nsl = min(S, p.nslices - k0);
     const bool valid = (i < p.nrays) && (j < p.nangles);
     const int nx = p.nx, ny = p.ny;
     const size_t plane = (size_t)nx * ny;
-    float value[S];
+    float value[S], linesum[S];
+    float step = 0.f;
 #pragma unroll
-    for (int q = 0; q < S; q++) value[q] = 0.f;
+    for (int q = 0; q < S; q++) value[q] = linesum[q] = 0.f;
     if (valid) {
         const float ang = p.angles[j];
         const float ctheta = __cosf(ang);
@@ -97,20 +100,17 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
                               : (steep ? p.imgT : p.img) + (size_t)k0 * plane;
         // address = Y*nx + X (row-major) or X*ny + Y (transposed)
         const int sy = steep ? 1 : nx, sx = steep ? ny : 1;
-        float linesum[S];
-#pragma unroll
-        for (int q = 0; q < S; q++) linesum[q] = 0.f;
-        // Samples are processed four at a time: the four positions and pixel
-        // loads are issued together (independent, so their latency overlaps),
-        // then added in sample order, exactly as the reference's sequential sum.
+        // This lane's samples (m = ph, ph + PH, ...) are processed four at a
+        // time: the four positions and pixel loads are issued together
+        // (independent, so their latency overlaps), then added in sample order.
         auto sample_loop = [&](const float t, const float d0, const float ay0, const float ddx,
                                const float ddy, const int nsamp, const int limx, const int limy) {
-            int m = 0;
-            for (; m + 4 <= nsamp; m += 4) {
+            int m = ph;
+            for (; m + 3 * PH < nsamp; m += 4 * PH) {
                 float v[4][S];
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
-                    const float s = __fmaf_rn((float)(m + u), d0, -ay0);
+                    const float s = __fmaf_rn((float)(m + u * PH), d0, -ay0);
                     const float x = __fmaf_rn(t, ctheta, -__fmul_rn(s, stheta));
                     const float y = __fmaf_rn(t, stheta, __fmul_rn(s, ctheta));
                     const int X = (int)((x + 1) / ddx);
@@ -141,7 +141,7 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
 #pragma unroll
                     for (int q = 0; q < S; q++) linesum[q] += v[u][q];
             }
-            for (; m < nsamp; m++) {
+            for (; m < nsamp; m += PH) {
                 const float s = __fmaf_rn((float)m, d0, -ay0);
                 const float x = __fmaf_rn(t, ctheta, -__fmul_rn(s, stheta));
                 const float y = __fmaf_rn(t, stheta, __fmul_rn(s, ctheta));
@@ -169,25 +169,34 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
             const float dt = (float)(2.0 * a / (p.nrays - 1));
             const float t = __fmaf_rn((float)i, dt, -a);
             sample_loop(t, dt, a, dt, dt, p.nrays, nx, nx);
-#pragma unroll
-            for (int q = 0; q < S; q++) value[q] = linesum[q] * dt;
+            step = dt;
         } else {
             const float dx = 2.0f * p.ax / (float)(unsigned)(nx - 1);
             const float dy = 2.0f * p.ay / (float)(unsigned)(ny - 1);
             const float t = __fmaf_rn((float)i, dx, -p.ax);
             sample_loop(t, dy, p.ay, dx, dy, ny, nx, ny);
-#pragma unroll
-            for (int q = 0; q < S; q++) value[q] = linesum[q] * dy;
+            step = dy;
         }
     }
-
-    double r2[S], y2[S], nll[S];
+    // combine the PH partial sums of each ray (every lane of the warp takes
+    // part; the lanes of one ray share its validity, invalid rays sum zeros):
+    // ((p0 + p1) + (p2 + p3)) for PH = 4, the same in every lane of the ray
 #pragma unroll
-    for (int q = 0; q < S; q++) r2[q] = y2[q] = nll[q] = 0.0;
+    for (int o = RW * Sh::AW; o < 32; o <<= 1)
+#pragma unroll
+        for (int q = 0; q < S; q++) linesum[q] += __shfl_xor_sync(0xffffffffu, linesum[q], o);
+#pragma unroll
+    for (int q = 0; q < S; q++) value[q] = linesum[q] * step;
+
+    // FP64 metric terms of this lane's slices q = ph + PH u (slot u = q / PH)
+    constexpr int U = (S + PH - 1) / PH;
+    double r2[U], y2[U], nll[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) r2[u] = y2[u] = nll[u] = 0.0;
 #pragma unroll
     for (int q = 0; q < S; q++) {
         const int k = k0 + q;
-        if (!valid || q >= nsl) continue;
+        if (!valid || q >= nsl || q % PH != ph) continue;   // phase lane ph writes slices q = ph mod PH
         const size_t vox = ((size_t)k * p.nangles + j) * p.nrays + i;
         float out = value[q];
         if constexpr (EPI == 1) {
@@ -197,9 +206,9 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
             if (p.metrics) {
                 const double y = p.data[vox];
                 const double m = fl * exp(-(double)value[q]);
-                r2[q] = (m - y) * (m - y);
-                y2[q] = y * y;
-                nll[q] = m + y * (double)value[q];
+                r2[q / PH] = (m - y) * (m - y);
+                y2[q / PH] = y * y;
+                nll[q / PH] = m + y * (double)value[q];
             }
         } else if constexpr (EPI == 2) {
             // eEM ratio, APPROXINVX(value, 1e-4) = SIGN/sqrtf(SQR(e)+SQR(x)) (configs.hpp:30-32)
@@ -210,9 +219,9 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
             if (out < 0) out = 0.0f;
             if (p.metrics) {
                 const double yd = y, m = value[q];
-                r2[q] = (m - yd) * (m - yd);
-                y2[q] = yd * yd;
-                nll[q] = (m > 0) ? m - yd * log(m) : 0.0;
+                r2[q / PH] = (m - yd) * (m - yd);
+                y2[q / PH] = yd * yd;
+                nll[q / PH] = (m > 0) ? m - yd * log(m) : 0.0;
             }
         }
         if (p.windowed) {
@@ -224,12 +233,21 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
     }
     if constexpr (EPI != 0) {
         if (p.metrics) {
-            // FP64 per-slice sums: warp shuffle, then across the block's warps
+            // FP64 per-slice sums: over the warp's lanes of one sample phase
+            // (the lanes holding slice q), then across the block's warps
             __shared__ double red[3][S][PJ_WARPS];
+            constexpr int G = RW * Sh::AW;   // lanes of one phase
 #pragma unroll
-            for (int q = 0; q < S; q++) {
-                const double a0 = warp_sum(r2[q]), a1 = warp_sum(y2[q]), a2 = warp_sum(nll[q]);
-                if (threadIdx.x == 0) {
+            for (int u = 0; u < U; u++) {
+                double a0 = r2[u], a1 = y2[u], a2 = nll[u];
+#pragma unroll
+                for (int o = 1; o < G; o <<= 1) {
+                    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+                    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+                    a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+                }
+                const int q = ph + PH * u;
+                if (threadIdx.x % G == 0 && q < S) {
                     red[0][q][threadIdx.y] = a0;
                     red[1][q][threadIdx.y] = a1;
                     red[2][q][threadIdx.y] = a2;
@@ -248,36 +266,53 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
     }
 }
 
-template <int EM, int EPI, int S, int IL, int RW>
+template <int EM, int EPI, int S, int IL, int RW, int PH, int BRS>
 __global__ void __launch_bounds__(32 * PJ_WARPS)
 project_kernel(const ProjLaunch p)
 {
-    project_block<EM, EPI, S, IL, RW>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    project_block<EM, EPI, S, IL, RW, PH, BRS>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
-// Shapes: eight interleaved slices per thread one angle per warp, fewer
-// slices (planar images, the ragged projector) four rays at eight angles per
-// warp.  RAFT_PJ_RW=32/16/8/4/2 forces one shape for the planar launches.
-constexpr int kPjRwIl = 32, kPjRwPlanar = 4;
-static int pj_rw_planar()
+// Launch shapes (rays per warp RW, sample phases PH, rays per block BR): by
+// default four rays x four phases x two angles per warp on interleaved images
+// and eight rays x four phases on planar ones, 32 rays per block (blocks of
+// 16, 8 or 4 rays at more angles measured 8-10 % slower on the interleaved
+// images, the same on planar ones); RAFT_PJ_SEQUENTIAL=1 sums every ray in one
+// lane in sample order (the reference's order; 32 rays at one angle, or four
+// rays at eight angles per warp).  Read at every launch.
+struct PjChoice {
+    int rw, ph, br;
+};
+static bool pj_sequential()
 {
-    static const int rw = [] {
-        const char *e = getenv("RAFT_PJ_RW");
-        const int v = e ? atoi(e) : kPjRwPlanar;
-        return (v == 32 || v == 16 || v == 8 || v == 4 || v == 2) ? v : kPjRwPlanar;
-    }();
-    return rw;
+    const char *e = getenv("RAFT_PJ_SEQUENTIAL");
+    return e && atoi(e) == 1;
+}
+static PjChoice pj_il() { return pj_sequential() ? PjChoice{32, 1, 32} : PjChoice{4, 4, 32}; }
+static PjChoice pj_pl() { return pj_sequential() ? PjChoice{4, 1, 32} : PjChoice{8, 4, 32}; }
+template <class F>
+static void pj_dispatch(PjChoice c, F &&f)
+{
+    using std::integral_constant;
+    if (c.rw == 32) f(integral_constant<int, 32>{}, integral_constant<int, 1>{}, integral_constant<int, 32>{});
+    else if (c.ph == 1) f(integral_constant<int, 4>{}, integral_constant<int, 1>{}, integral_constant<int, 32>{});
+    else if (c.rw == 4) f(integral_constant<int, 4>{}, integral_constant<int, 4>{}, integral_constant<int, 32>{});
+    else f(integral_constant<int, 8>{}, integral_constant<int, 4>{}, integral_constant<int, 32>{});
 }
 
 int project_blocks_per_slice(int nrays, int nangles)
 {
-    using Sh = PjShape<kPjRwPlanar>;
-    return ((nrays + Sh::BR - 1) / Sh::BR) * ((nangles + Sh::BA - 1) / Sh::BA);
+    int n = 0;
+    pj_dispatch(pj_pl(), [&](auto rw, auto ph, auto br) {
+        using Sh = PjShape<decltype(rw)::value, decltype(ph)::value, decltype(br)::value>;
+        n = ((nrays + Sh::BR - 1) / Sh::BR) * ((nangles + Sh::BA - 1) / Sh::BA);
+    });
+    return n;
 }
 
 // Ragged projector: one launch over many single-slice requests of different
 // sizes; block b belongs to the request r with blk_start[r] <= b < blk_start[r+1].
-template <int EM, int EPI>
+template <int EM, int EPI, int RW, int PH, int BRS>
 __global__ void __launch_bounds__(32 * PJ_WARPS)
 project_ragged_kernel(const ProjLaunch *__restrict__ reqs, const int *__restrict__ blk_start, int nreq)
 {
@@ -295,8 +330,23 @@ project_ragged_kernel(const ProjLaunch *__restrict__ reqs, const int *__restrict
     const int r = s_r;
     const ProjLaunch &p = reqs[r];
     const int local = blockIdx.x - blk_start[r];
-    const int nbx = (p.nrays + PjShape<kPjRwPlanar>::BR - 1) / PjShape<kPjRwPlanar>::BR;
-    project_block<EM, EPI, 1, 0, kPjRwPlanar>(p, local % nbx, local / nbx, 0);
+    const int nbx = (p.nrays + PjShape<RW, PH, BRS>::BR - 1) / PjShape<RW, PH, BRS>::BR;
+    project_block<EM, EPI, 1, 0, RW, PH, BRS>(p, local % nbx, local / nbx, 0);
+}
+
+template <int RW, int PH, int BRS>
+static void launch_ragged_shape(const ProjLaunch *d_reqs, const int *d_blk_start, int nreq, int total_blocks,
+                                int em, int epilogue, cudaStream_t st)
+{
+    dim3 block(32, PJ_WARPS);
+    if (!em)
+        project_ragged_kernel<0, 0, RW, PH, BRS><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
+    else if (epilogue == 1)
+        project_ragged_kernel<1, 1, RW, PH, BRS><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
+    else if (epilogue == 2)
+        project_ragged_kernel<1, 2, RW, PH, BRS><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
+    else
+        project_ragged_kernel<1, 0, RW, PH, BRS><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
 }
 
 void launch_project_ragged(const ProjLaunch *d_reqs, const int *d_blk_start, int nreq, int total_blocks, int em,
@@ -304,11 +354,10 @@ void launch_project_ragged(const ProjLaunch *d_reqs, const int *d_blk_start, int
 {
     if (nreq <= 0 || total_blocks <= 0) return;
     ProfScope ps(PROF_PROJECT, st);
-    dim3 block(32, PJ_WARPS);
-    if (!em) project_ragged_kernel<0, 0><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
-    else if (epilogue == 1) project_ragged_kernel<1, 1><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
-    else if (epilogue == 2) project_ragged_kernel<1, 2><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
-    else project_ragged_kernel<1, 0><<<total_blocks, block, 0, st>>>(d_reqs, d_blk_start, nreq);
+    pj_dispatch(pj_pl(), [&](auto rw, auto ph, auto br) {
+        launch_ragged_shape<decltype(rw)::value, decltype(ph)::value, decltype(br)::value>(
+            d_reqs, d_blk_start, nreq, total_blocks, em, epilogue, st);
+    });
     RAFT_CUDA(cudaGetLastError());
 }
 
@@ -417,34 +466,30 @@ void stage_proj_images(ProjLaunch &pl, void *scratch, cudaStream_t st)
     }
 }
 
-template <int EM, int EPI, int S, int IL, int RW>
+template <int EM, int EPI, int S, int IL, int RW, int PH, int BRS>
 static void launch_project_shape(const ProjLaunch &pl, cudaStream_t st)
 {
-    using Sh = PjShape<RW>;
+    using Sh = PjShape<RW, PH, BRS>;
     dim3 grid((pl.nrays + Sh::BR - 1) / Sh::BR, (pl.nangles + Sh::BA - 1) / Sh::BA, (pl.nslices + S - 1) / S);
-    project_kernel<EM, EPI, S, IL, RW><<<grid, dim3(32, PJ_WARPS), 0, st>>>(pl);
-}
-
-template <int EM, int EPI, int S>
-static void launch_project_planar(const ProjLaunch &pl, cudaStream_t st)
-{
-    switch (pj_rw_planar()) {
-    case 32: launch_project_shape<EM, EPI, S, 0, 32>(pl, st); break;
-    case 16: launch_project_shape<EM, EPI, S, 0, 16>(pl, st); break;
-    case 8: launch_project_shape<EM, EPI, S, 0, 8>(pl, st); break;
-    case 2: launch_project_shape<EM, EPI, S, 0, 2>(pl, st); break;
-    default: launch_project_shape<EM, EPI, S, 0, 4>(pl, st); break;
-    }
+    project_kernel<EM, EPI, S, IL, RW, PH, BRS><<<grid, dim3(32, PJ_WARPS), 0, st>>>(pl);
 }
 
 template <int EM, int EPI>
 static void launch_project_s(const ProjLaunch &pl, int S, cudaStream_t st)
 {
     ProfScope ps(PROF_PROJECT, st);
-    if (S == 8) launch_project_shape<EM, EPI, 8, 1, kPjRwIl>(pl, st);
-    else if (S == 4) launch_project_planar<EM, EPI, 4>(pl, st);
-    else if (S == 2) launch_project_planar<EM, EPI, 2>(pl, st);
-    else launch_project_planar<EM, EPI, 1>(pl, st);
+    if (S == 8) {
+        pj_dispatch(pj_il(), [&](auto rw, auto ph, auto br) {
+            launch_project_shape<EM, EPI, 8, 1, decltype(rw)::value, decltype(ph)::value, decltype(br)::value>(pl, st);
+        });
+    } else {
+        pj_dispatch(pj_pl(), [&](auto rw, auto ph, auto br) {
+            constexpr int RW = decltype(rw)::value, PH = decltype(ph)::value, BR = decltype(br)::value;
+            if (S == 4) launch_project_shape<EM, EPI, 4, 0, RW, PH, BR>(pl, st);
+            else if (S == 2) launch_project_shape<EM, EPI, 2, 0, RW, PH, BR>(pl, st);
+            else launch_project_shape<EM, EPI, 1, 0, RW, PH, BR>(pl, st);
+        });
+    }
     RAFT_CUDA(cudaGetLastError());
 }
 

@@ -117,11 +117,27 @@ def test_em_graph_equals_stream_and_metrics(oracle):
         x = oracle.tem(counts, flat, ang, 1, obj=x, fwd_trig=F(ang), bp_trig=B(ang))
 
 
-def test_interleaved_projector_bit_identical():
+@pytest.fixture
+def pj_order(request):
+    old = os.environ.get("RAFT_PJ_SEQUENTIAL")
+    if request.param:
+        os.environ["RAFT_PJ_SEQUENTIAL"] = "1"
+    else:
+        os.environ.pop("RAFT_PJ_SEQUENTIAL", None)
+    yield request.param
+    if old is None:
+        os.environ.pop("RAFT_PJ_SEQUENTIAL", None)
+    else:
+        os.environ["RAFT_PJ_SEQUENTIAL"] = old
+
+
+@pytest.mark.parametrize("pj_order", [False, True], indirect=True, ids=["phases", "sequential"])
+def test_interleaved_projector_bit_identical(pj_order):
     """8 or more slices run the projector on slice-interleaved copies (groups of
     8, a partial last group zero-filled); fewer run it on planar images.  The
-    samples and their summation order are the same, so 11 slices at once must
-    equal 4 + 7 slices bit for bit: Radon, tEM (with metrics) and eEM."""
+    samples and their summation order are the same (four sample phases per ray
+    by default, one sequential sum with RAFT_PJ_SEQUENTIAL=1), so 11 slices at
+    once must equal 4 + 7 slices bit for bit: Radon, tEM (with metrics) and eEM."""
     import ctypes
     import torch
     from sscRaft import synthetic as S
@@ -157,3 +173,45 @@ def test_interleaved_projector_bit_identical():
         torch.cuda.synchronize()
         assert torch.equal(o_full, o_part), kind
         assert torch.allclose(m_full, m_part, rtol=1e-12, atol=0), kind
+
+
+def test_projector_phases_agree_with_sequential_sums():
+    """Each ray's samples summed over four lane phases and combined by a fixed
+    butterfly (the default) against one sequential sum per ray (the
+    reference's order, RAFT_PJ_SEQUENTIAL=1): rounding only.  Two FP32 orders
+    of a 300-term sum differ by about sqrt(300) x 6e-8 = 1e-6 (measured 1.2e-6),
+    so rel-L2 <= 5e-6 for the Radon transform of 9 slices (interleaved) and of
+    1 slice (planar); a misplaced sample shows as 1e-3 or more."""
+    import ctypes
+    import torch
+    from sscRaft import synthetic as S
+    from sscRaft.rafttypes import _ptr, libraft
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    N, A = 300, 200
+    ang = (np.arange(A) * (np.pi / A)).astype(np.float32)
+    img = torch.stack([S.phantom_image(S.ellipse_params(900 + k, 8), N, xp=torch, device="cuda")
+                       for k in range(9)]).contiguous()
+    old = os.environ.get("RAFT_PJ_SEQUENTIAL")
+    try:
+        outs = {}
+        for seq in (False, True):
+            if seq:
+                os.environ["RAFT_PJ_SEQUENTIAL"] = "1"
+            else:
+                os.environ.pop("RAFT_PJ_SEQUENTIAL", None)
+            for n in (9, 1):
+                o = torch.empty((n, A, N), device="cuda")
+                assert libraft.raft_radon_device(0, p(o), p(img[:n].contiguous()), _ptr(ang), N, N, N, A, n, 1.0, 1.0,
+                                                 None) == 0
+                outs[(seq, n)] = o
+        torch.cuda.synchronize()
+    finally:
+        if old is None:
+            os.environ.pop("RAFT_PJ_SEQUENTIAL", None)
+        else:
+            os.environ["RAFT_PJ_SEQUENTIAL"] = old
+    for n in (9, 1):
+        a, b = outs[(False, n)].double(), outs[(True, n)].double()
+        err = float((a - b).norm() / b.norm())
+        print(f"Radon {n} slices, phases vs sequential: rel-L2 {err:.2e}")
+        assert err <= 5e-6, (n, err)
