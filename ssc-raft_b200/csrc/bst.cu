@@ -46,6 +46,7 @@
 #include <memory>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 namespace raft {
@@ -375,26 +376,53 @@ size_t bst_core_workspace_bytes(const BstCore &c, int nslices)
     return ((polar + 255) & ~(size_t)255) + T;
 }
 
-template <int NF>
-static void launch_bst_kernels(const BstArgs &a, const BstCore &c, int nslices, int threads, size_t sm3, size_t sm2,
-                               cudaStream_t st)
+// Calls f(integral_constant<int, n>) when n is one of the compiled transform
+// lengths, f(integral_constant<int, 0>) otherwise.
+template <class F>
+static void with_fixed_length(int n, F &&f)
 {
-    RAFT_CHECK(NF == 0 || threads == c_fft_threads(NF), "BST: thread count of the compile-time transforms");
+    using std::integral_constant;
+    switch (n) {
+    case 1024: f(integral_constant<int, 1024>{}); break;
+    case 1536: f(integral_constant<int, 1536>{}); break;
+    case 2048: f(integral_constant<int, 2048>{}); break;
+    case 3072: f(integral_constant<int, 3072>{}); break;
+    case 4096: f(integral_constant<int, 4096>{}); break;
+    case 6144: f(integral_constant<int, 6144>{}); break;
+    case 8192: f(integral_constant<int, 8192>{}); break;
+    case 12288: f(integral_constant<int, 12288>{}); break;
+    default: f(integral_constant<int, 0>{}); break;
+    }
+}
+
+template <int NF>
+static void launch_bst_rows(const BstArgs &a, const BstCore &c, int nslices, int threads, size_t sm3, cudaStream_t st)
+{
     static thread_local int configured = -1;
     int dev = 0;
     cudaGetDevice(&dev);
     if (configured != dev) {
         RAFT_CUDA(cudaFuncSetAttribute(bst_rows_kernel<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kBstSmemMax));
+        configured = dev;
+    }
+    bst_rows_kernel<NF><<<dim3((c.A + 1) / 2, nslices), threads, sm3, st>>>(a);
+    RAFT_CUDA(cudaGetLastError());
+}
+
+template <int NF>
+static void launch_bst_grid(const BstArgs &a, const BstCore &c, int nslices, int threads, size_t sm2, cudaStream_t st)
+{
+    static thread_local int configured = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured != dev) {
         RAFT_CUDA(cudaFuncSetAttribute(bst_regrid_kernel<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kBstSmemMax));
         RAFT_CUDA(cudaFuncSetAttribute(bst_cols_kernel<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kBstSmemMax));
         configured = dev;
     }
-    bst_rows_kernel<NF><<<dim3((c.A + 1) / 2, nslices), threads, sm3, st>>>(a);
-    RAFT_CUDA(cudaGetLastError());
-    count_launch();
     bst_regrid_kernel<NF><<<dim3(c.S, nslices), threads, sm2, st>>>(a);
     RAFT_CUDA(cudaGetLastError());
     count_launch();
@@ -430,22 +458,23 @@ void bst_run(int device, const BstCore &c, const float *d_tomo, float *d_obj, in
     a.scale = c.scale;
     const int threads = fft_threads(std::max({c.M, a.pN.M, a.pL.M, a.pS.M}));
     const size_t sm3 = 2 * (size_t)a.M * sizeof(float2), sm2 = 2 * (size_t)fft_plan_span(a.pS) * sizeof(float2);
-    // one compile-time length for every transform of the launch, when it is one of those compiled
-    const bool same = (!c.G || (a.pN.n == c.S && a.pN.M == c.S)) && a.pL.n == c.S && a.pL.M == c.S &&
-                      a.pS.n == c.S && a.pS.M == c.S && threads == c_fft_threads(c.S) &&
-                      fixed_transforms_enabled();
+    // compile-time lengths where the plans are direct: the rows kernel's
+    // transforms (the filter's, when there is one, and the half-rays') and the
+    // grid transforms of the regrid and column kernels; each kernel then runs
+    // with the thread count of its length
+    const bool en = fixed_transforms_enabled();
+    const int nrow = (en && a.pL.n == a.pL.M && (!c.G || (a.pN.n == a.pL.n && a.pN.M == a.pN.n))) ? a.pL.n : 0;
+    const int ngrid = (en && a.pS.n == a.pS.M) ? a.pS.n : 0;
     ProfScope ps(PROF_OTHER, st);   // counts the first of the three launches
-    switch (same ? c.S : 0) {
-    case 1024: launch_bst_kernels<1024>(a, c, nslices, threads, sm3, sm2, st); break;
-    case 1536: launch_bst_kernels<1536>(a, c, nslices, threads, sm3, sm2, st); break;
-    case 2048: launch_bst_kernels<2048>(a, c, nslices, threads, sm3, sm2, st); break;
-    case 3072: launch_bst_kernels<3072>(a, c, nslices, threads, sm3, sm2, st); break;
-    case 4096: launch_bst_kernels<4096>(a, c, nslices, threads, sm3, sm2, st); break;
-    case 6144: launch_bst_kernels<6144>(a, c, nslices, threads, sm3, sm2, st); break;
-    case 8192: launch_bst_kernels<8192>(a, c, nslices, threads, sm3, sm2, st); break;
-    case 12288: launch_bst_kernels<12288>(a, c, nslices, threads, sm3, sm2, st); break;
-    default: launch_bst_kernels<0>(a, c, nslices, threads, sm3, sm2, st); break;
-    }
+    with_fixed_length(nrow, [&](auto nf) {
+        constexpr int NF = decltype(nf)::value;
+        launch_bst_rows<NF>(a, c, nslices, NF ? c_fft_threads(NF) : threads, sm3, st);
+    });
+    count_launch();
+    with_fixed_length(ngrid, [&](auto nf) {
+        constexpr int NF = decltype(nf)::value;
+        launch_bst_grid<NF>(a, c, nslices, NF ? c_fft_threads(NF) : threads, sm2, st);
+    });
 }
 
 void launch_bst(int device, const FbpConfig &cfg, const float *d_tomo, float *d_obj, int nslices, void *workspace,
