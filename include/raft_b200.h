@@ -263,9 +263,8 @@ void raft_profile_enable(int on);
 int raft_profile_read(double *ms, long long *counts, int nclasses);
 /* Transform kernel selection (no reference counterpart): 1 (default) = FBP filter
  * rows, BST and tEMFQ transforms of 1024, 1536, 2048, 3072, 4096, 6144, 8192 and
- * 12288 points run kernels compiled for that length (the same arithmetic as the
- * generic kernels; results agree to rounding, rel-L2 about 2e-7 to 6e-7); 0 = the
- * generic kernels for all lengths. */
+ * 12288 points run kernels compiled for that length (bit for bit the results of
+ * the generic kernels); 0 = the generic kernels for all lengths. */
 int raft_filter_set_fixed(int on);
 
 /* Learned warm start: tensor-core kernels of the U-Net (no reference counterpart).

@@ -64,12 +64,28 @@ static inline int fft_threads(int n)
 }
 
 // -------------------------------------------------------------- device --
+// Complex arithmetic with every rounding explicit (the compiler may not fuse
+// or split any of it), so a transform gives the same bits in every kernel it
+// is inlined into: the compile-time-length passes and fft_pass agree bit for
+// bit.  (The packed two-lane FP32 instructions give the same bits; they
+// measured 3 % slower in the 6144-point filter and are not used.)
+__device__ __forceinline__ float2 add2(float2 a, float2 b)
+{
+    return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
+{
+    return make_float2(__fmaf_rn(a.x, b.x, c.x), __fmaf_rn(a.y, b.y, c.y));
+}
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return make_float2(__fmaf_rn(a.x, b.x, -__fmul_rn(a.y, b.y)), __fmaf_rn(a.x, b.y, __fmul_rn(a.y, b.x)));
 }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return add2(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b)
+{
+    return make_float2(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y));
+}
 // multiply by -i
 __device__ __forceinline__ float2 cmni(float2 a) { return make_float2(a.y, -a.x); }
 
@@ -87,8 +103,10 @@ template <> struct Dft<2> {
 template <> struct Dft<4> {
     static __device__ __forceinline__ void run(float2 *v)
     {
-        float2 s0 = cadd(v[0], v[2]), d0 = csub(v[0], v[2]);
-        float2 s1 = cadd(v[1], v[3]), d1 = cmni(csub(v[1], v[3]));
+        const float2 s0 = cadd(v[0], v[2]), d0 = csub(v[0], v[2]);
+        const float2 s1 = cadd(v[1], v[3]);
+        // -i (v1 - v3)
+        const float2 d1 = make_float2(__fsub_rn(v[1].y, v[3].y), __fsub_rn(v[3].x, v[1].x));
         v[0] = cadd(s0, s1);
         v[2] = csub(s0, s1);
         v[1] = cadd(d0, d1);
@@ -103,18 +121,20 @@ template <> struct Dft<8> {
         float2 o[4] = {v[1], v[3], v[5], v[7]};
         Dft<4>::run(e);
         Dft<4>::run(o);
-        // twiddles exp(-2 pi i k/8), k = 0..3
-        float2 t1 = make_float2(r * (o[1].x + o[1].y), r * (o[1].y - o[1].x));
-        float2 t2 = cmni(o[2]);
-        float2 t3 = make_float2(r * (o[3].y - o[3].x), -r * (o[3].x + o[3].y));
+        // twiddles exp(-2 pi i k/8), k = 0..3:
+        //   o1 w1 = r (o1.x + o1.y, o1.y - o1.x), o2 w2 = -i o2,
+        //   o3 w3 = r (o3.y - o3.x, -(o3.x + o3.y))
+        const float2 rr = make_float2(r, r), nr = make_float2(-r, -r);
+        const float2 s1 = make_float2(__fadd_rn(o[1].x, o[1].y), __fsub_rn(o[1].y, o[1].x));
+        const float2 s3 = make_float2(__fsub_rn(o[3].y, o[3].x), -__fadd_rn(o[3].x, o[3].y));
         v[0] = cadd(e[0], o[0]);
         v[4] = csub(e[0], o[0]);
-        v[1] = cadd(e[1], t1);
-        v[5] = csub(e[1], t1);
-        v[2] = cadd(e[2], t2);
-        v[6] = csub(e[2], t2);
-        v[3] = cadd(e[3], t3);
-        v[7] = csub(e[3], t3);
+        v[1] = fma2(rr, s1, e[1]);
+        v[5] = fma2(nr, s1, e[1]);
+        v[2] = make_float2(__fadd_rn(e[2].x, o[2].y), __fsub_rn(e[2].y, o[2].x));
+        v[6] = make_float2(__fsub_rn(e[2].x, o[2].y), __fadd_rn(e[2].y, o[2].x));
+        v[3] = fma2(rr, s3, e[3]);
+        v[7] = fma2(nr, s3, e[3]);
     }
 };
 // odd radices: direct sum with constant roots cos/sin(2 pi m / R)
@@ -150,19 +170,23 @@ template <> struct Roots<7> {
 template <int R> struct DftOdd {
     static __device__ __forceinline__ void run(float2 *v)
     {
-        float2 in[R];
+        float2 in[R], sw[R];
 #pragma unroll
-        for (int r = 0; r < R; r++) in[r] = v[r];
+        for (int r = 0; r < R; r++) {
+            in[r] = v[r];
+            sw[r] = make_float2(v[r].y, v[r].x);
+        }
 #pragma unroll
         for (int q = 0; q < R; q++) {
             float2 acc = in[0];
 #pragma unroll
             for (int r = 1; r < R; r++) {
                 const int m = (r * q) % R;
-                // exp(-2 pi i m / R) = c(m) - i s(m)
+                // in[r] exp(-2 pi i m / R) = in[r] (c(m) - i s(m)):
+                // (x c + y s, y c - x s), two packed fmas
                 const float c = Roots<R>::c(m), s = Roots<R>::s(m);
-                acc.x += in[r].x * c + in[r].y * s;
-                acc.y += in[r].y * c - in[r].x * s;
+                acc = fma2(in[r], make_float2(c, c), acc);
+                acc = fma2(sw[r], make_float2(s, -s), acc);
             }
             v[q] = acc;
         }
@@ -269,9 +293,9 @@ __device__ __forceinline__ float2 *fft_forward(float2 *a, float2 *b, int Np, con
 // unrolled, so every shared-memory address is the thread's padded index plus
 // an immediate offset, and a pass whose twiddle index k is the same in every
 // iteration of a thread computes its twiddle once.  Radix order, twiddle
-// expressions and butterflies are those of fft_pass; only the compiler's
-// choice of fused multiply-adds may differ, so the results agree with
-// fft_forward's to rounding (rel-L2 about 2e-7).  The first pass's loads and the last pass's
+// expressions and butterflies are those of fft_pass, with every rounding
+// explicit, so the results are bit for bit fft_forward's.  The first pass's
+// loads and the last pass's
 // stores are functors, so callers can read the input from global memory and
 // consume the output in registers.
 struct CRadices {

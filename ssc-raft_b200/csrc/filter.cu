@@ -350,8 +350,7 @@ filter_fft_kernel(const float *__restrict__ sino, int N, int Np, int off, int ns
 // the spectral multiply and conjugation sit in the last forward pass, and for
 // single-float window rows the last inverse pass stores the window elements
 // from registers (other row formats go through shared memory and pack_row).
-// The arithmetic of filter_fft_kernel; the results agree with it to rounding
-// (the compiler may fuse multiply-adds differently in the unrolled passes).
+// Bit for bit the results of filter_fft_kernel.
 template <int NP, int R0>
 struct FxRowsIn {
     const float *s0, *s1;
