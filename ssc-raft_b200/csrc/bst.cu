@@ -161,7 +161,9 @@ __global__ void __launch_bounds__(512) bst_regrid_kernel(const BstArgs p)
     const float2 *pol = p.polar + (size_t)slice * twoA * p.Lh;
     const int rmax = p.L / 2 - 1;
     for (int X = threadIdx.x; X < S; X += blockDim.x) {
-        const int tx = (X - h + S) % S;
+        // (X - h + S) % S, X < S: one conditional add (integer modulos by
+        // run-time values cost about twenty instructions each)
+        const int tx = X - h < 0 ? X - h + S : X - h;
         const float posx = (float)(tx - h);
         const float rho = (float)p.L * hypotf(posx, posy) / (float)S;
         const float angle = (float)twoA * (0.5f * atan2f(posy, posx) / (float)M_PI + 0.5f);
@@ -171,8 +173,10 @@ __global__ void __launch_bounds__(512) bst_regrid_kernel(const BstArgs p)
         if (irho < rmax) {
             const float pfrac = rho - (float)irho;
             const float tfrac = (float)iarc - angle;
-            iarc = iarc % twoA;
-            const int uarc = (iarc + 1) % twoA;
+            // angle lies in [0, twoA] (truncation keeps iarc >= 0): iarc % twoA
+            // and (iarc + 1) % twoA as conditional subtractions
+            iarc = iarc >= twoA ? iarc - twoA : iarc;
+            const int uarc = iarc + 1 >= twoA ? iarc + 1 - twoA : iarc + 1;
             const float2 *q0 = pol + (size_t)iarc * p.Lh + irho;
             const float2 *q1 = pol + (size_t)uarc * p.Lh + irho;
             const float2 c00 = __ldg(q0), c01 = __ldg(q0 + 1), c10 = __ldg(q1), c11 = __ldg(q1 + 1);
@@ -180,7 +184,7 @@ __global__ void __launch_bounds__(512) bst_regrid_kernel(const BstArgs p)
             const float2 i1 = make_float2(c10.x * (1.f - pfrac) + c11.x * pfrac, c10.y * (1.f - pfrac) + c11.y * pfrac);
             v = make_float2(i0.x * tfrac + i1.x * (1.f - tfrac), i0.y * tfrac + i1.y * (1.f - tfrac));
         }
-        const float sgn = sy * ((float)(tx % 2) - 0.5f);
+        const float sgn = sy * ((float)(tx & 1) - 0.5f);
         sm_bst[X] = make_float2(v.x * sgn, -v.y * sgn);   // conjugated: see bst_cols_kernel
     }
     __syncthreads();
