@@ -19,6 +19,29 @@ from helpers import fbp_params, sino_case
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("N,pad", [(4096, 2), (4096, 1)])
+def test_fbp_largest_compiled_lengths_vs_oracle(N, pad, oracle):
+    """4096^2 images with 12288- and 8192-point rows (the largest filter
+    lengths compiled for their length), 2 slices, Hann, axis offset 1.5:
+    nearest vs the FP64 oracle given the fast-intrinsic sin/cos <= 2e-5,
+    linear FP32 rows <= 1e-5, linear BF16 rows <= 4e-3."""
+    from sscRaft.rafttypes import fast_sincos
+    A, B, ftype, offset = 64, 2, 5, 1.5
+    sino, ang = sino_case(N, A, B, seed=N + pad, n_ell=12)
+    pf, pi = fbp_params(N, A, B, pad=pad, ftype=ftype, offset=offset)
+    out = _fbp(sino, ang, pf, pi)
+    ref = oracle.fbp(sino, ang, oracle.MODE_REF, ftype, pad, offset=offset, trig=fast_sincos(ang, 0))
+    err = rel_l2(out, ref)
+    print(f"N={N} pad={pad} nearest vs oracle: {err:.3e}")
+    assert err <= 2e-5, err
+    ref = oracle.fbp(sino, ang, oracle.MODE_LIN, ftype, pad, offset=offset)
+    err32 = rel_l2(_fbp(sino, ang, pf, pi, 1, 1), ref)
+    err16 = rel_l2(_fbp(sino, ang, pf, pi, 1, 2), ref)
+    print(f"N={N} pad={pad} linear vs oracle: FP32 {err32:.3e}, BF16 {err16:.3e}")
+    assert err32 <= 1e-5, err32
+    assert err16 <= 4e-3, err16
+
+
 def _fbp(sino, ang, pf, pi, geometry=0, store=0):
     from sscRaft.rafttypes import _ptr, check_error, libraft
     No = int(pi[3])
