@@ -535,9 +535,11 @@ def run_warm(dev, samples=256):
 
 
 def unet_flops_per_image(net, H=512, W=512):
-    """2 * 9 * Cin * Cout * pixels summed over the 3x3 convolutions."""
+    """2 * 9 * Cin * Cout * pixels summed over the 3x3 convolutions; the first
+    layer counted with its one real input channel (its packed input's other
+    31 channels are zero, and inference convolves the image directly)."""
     level = {"0": 1, "1": 2, "2": 4, "3": 8}
-    return sum(2.0 * 9 * (c0 + c1) * co * (H // level[name[1]]) * (W // level[name[1]])
+    return sum(2.0 * 9 * (1 if name == "e0a" else c0 + c1) * co * (H // level[name[1]]) * (W // level[name[1]])
                for name, c0, c1, co in net.LAYERS)
 
 

@@ -294,6 +294,11 @@ int raft_unet_relu_bwd(const void *y, const void *dy, void *dpre, size_t n, void
 int raft_unet_pool(int backward, const void *src, void *dst, int N, int H, int W, int C, void *stream);
 int raft_unet_upsample(int backward, const void *src, void *dst, int N, int H, int W, int C, void *stream);
 int raft_unet_input(const float *img, const float *scale, void *x, int N, int H, int W, int C, void *stream);
+/* First layer for inference, from the one-channel input: y = ReLU(bias + 3x3 conv of
+ * bf16(img x scale)) with the layer's weights [32][3][3][Cin] (channel 0 of each tap;
+ * the packed input's other channels are zero), 32 BF16 output channels, NHWC. */
+int raft_unet_input_conv(const float *img, const float *scale, const void *w, int Cin, const float *bias, void *y,
+                         int N, int H, int W, void *stream);
 int raft_unet_head(int backward, const void *h, const float *w, const float *b, const float *img,
                    const float *scale, float *out_or_grad, void *dh, float *dw, float *db, int N, int HW,
                    int C, void *stream);

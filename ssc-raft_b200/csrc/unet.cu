@@ -478,6 +478,58 @@ __global__ void input_pack_v8_kernel(const float *img, const float *scale, bf16 
     }
 }
 
+// The network's first layer for inference, from the image itself: the input
+// has one channel (image x scale, rounded to BF16 as the packed input is),
+// so the 3x3 convolution to 32 channels with bias and ReLU is nine FP32
+// multiply-adds per output channel -- no 32-channel input of which 31 are
+// zero, no tensor-core pass over them.  Weights [32][3][3][Cin]: channel 0 of
+// each tap is used (the others multiply zero inputs).  One CTA per 32 x 8
+// output pixels and image; one thread per pixel, 32 channels, 64-byte stores.
+__global__ void __launch_bounds__(256) input_conv_kernel(const float *__restrict__ img,
+                                                         const float *__restrict__ scale, const bf16 *__restrict__ w,
+                                                         const float *__restrict__ b, bf16 *__restrict__ y, int H,
+                                                         int W, int Cin)
+{
+    __shared__ float xs[10][34];   // input rows y0-1 .. y0+8, columns x0-1 .. x0+32
+    __shared__ float ws[9][32];    // w[co][tap][0]
+    __shared__ float bs[32];
+    const int n = blockIdx.z, x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
+    const float sc = scale[n];
+    for (int i = threadIdx.x; i < 10 * 34; i += blockDim.x) {
+        const int r = i / 34, c = i - r * 34, gy = y0 + r - 1, gx = x0 + c - 1;
+        float v = 0.f;
+        if (gy >= 0 && gy < H && gx >= 0 && gx < W)
+            v = __bfloat162float(__float2bfloat16(img[((size_t)n * H + gy) * W + gx] * sc));
+        xs[r][c] = v;
+    }
+    for (int i = threadIdx.x; i < 9 * 32; i += blockDim.x) {
+        const int t = i >> 5, co = i & 31;
+        ws[t][co] = __bfloat162float(w[((size_t)co * 9 + t) * Cin]);
+    }
+    if (threadIdx.x < 32) bs[threadIdx.x] = b[threadIdx.x];
+    __syncthreads();
+    const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+    const int gx = x0 + lx, gy = y0 + ly;
+    if (gx >= W || gy >= H) return;
+    float xv[9];
+#pragma unroll
+    for (int t = 0; t < 9; t++) xv[t] = xs[ly + t / 3][lx + t % 3];
+    uint4 *dst = reinterpret_cast<uint4 *>(y + (((size_t)n * H + gy) * W + gx) * 32);
+#pragma unroll
+    for (int g = 0; g < 4; g++) {
+        float f[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int co = 8 * g + j;
+            float acc = 0.f;
+#pragma unroll
+            for (int t = 0; t < 9; t++) acc = fmaf(xv[t], ws[t][co], acc);
+            f[j] = fmaxf(acc + bs[co], 0.f);
+        }
+        dst[g] = f_to_bf8(f);
+    }
+}
+
 // head, one thread per pixel with 16-byte channel loads (C <= 64, weights in shared memory)
 __global__ void head_fwd_v8_kernel(const bf16 *h, const float *w, const float *b, const float *img,
                                    const float *scale, float *out, int N, int HW, int C)
@@ -828,6 +880,17 @@ int raft_unet_input(const float *img, const float *scale, void *x, int N, int H,
     }
     input_pack_kernel<<<grid_for((size_t)N * H * W * C), 256, 0, (cudaStream_t)stream>>>(img, scale, (bf16 *)x, N, H,
                                                                                         W, C);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+int raft_unet_input_conv(const float *img, const float *scale, const void *w, int Cin, const float *bias, void *y,
+                         int N, int H, int W, void *stream)
+{
+    if (N <= 0 || H <= 0 || W <= 0 || Cin < 1 || ((uintptr_t)y % 16) != 0) return 1;
+    count_launch();
+    const dim3 grid((W + 31) / 32, (H + 7) / 8, N);
+    input_conv_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(img, scale, (const bf16 *)w, bias, (bf16 *)y, H, W,
+                                                              Cin);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 

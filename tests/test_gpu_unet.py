@@ -65,6 +65,43 @@ def test_conv_kernels_vs_oracle(oracle):
     assert rel_l2(_f64(d1), ref_dx[..., C0:]) <= 1e-2
 
 
+def test_input_conv_equals_packed_first_layer(oracle):
+    """Inference's first layer straight from the one-channel image
+    (raft_unet_input_conv) against the training path's packed 32-channel input
+    + tensor-core convolution, and against the FP64 oracle on the BF16-rounded
+    input: BF16 outputs within rel-L2 1e-2 of the oracle and 2e-3 of the
+    packed path (the two sum nine exact products in different orders); the
+    whole network's inference output within 1e-2 of the training forward."""
+    import torch
+    from sscRaft import warmstart as ws
+    from sscRaft.rafttypes import libraft
+    torch.manual_seed(5)
+    N, H, W = 2, 128, 160
+    img = torch.rand(N, H, W, device="cuda")
+    scale = torch.tensor([3.0, 0.5], device="cuda")
+    w = _bf(torch.randn(32, 3, 3, 32, device="cuda") * 0.3)
+    w[..., 1:] = 0
+    b = torch.randn(32, device="cuda") * 0.1
+    y = torch.empty(N, H, W, 32, dtype=torch.bfloat16, device="cuda")
+    assert libraft.raft_unet_input_conv(ws._p(img), ws._p(scale), ws._p(w), 32, ws._p(b), ws._p(y), N, H, W, None) == 0
+    x = torch.empty(N, H, W, 32, dtype=torch.bfloat16, device="cuda")
+    assert libraft.raft_unet_input(ws._p(img), ws._p(scale), ws._p(x), N, H, W, 32, None) == 0
+    yp = torch.empty_like(y)
+    assert libraft.raft_unet_conv_fwd(ws._p(x), 32, None, 0, ws._p(w), ws._p(b), ws._p(yp), None, 0,
+                                      N, H, W, 32, 1, None) == 0
+    ref = oracle.conv3x3(_f64(x), _f64(w), _f64(b), relu=True)
+    e_or, e_pk = rel_l2(_f64(y), ref), rel_l2(_f64(y), _f64(yp))
+    print(f"input conv vs oracle {e_or:.2e}, vs packed tensor-core layer {e_pk:.2e}")
+    assert e_or <= 1e-2, e_or
+    assert e_pk <= 2e-3, e_pk
+    net = ws.UNet(torch.device("cuda", 0), seed=3)
+    sc = torch.ones(N, device="cuda")
+    o_inf = net.forward(img * 0.01, sc)
+    o_trn = net.forward(img * 0.01, sc, keep=True)
+    e_net = rel_l2(_f64(o_inf), _f64(o_trn))
+    print(f"network inference vs training forward {e_net:.2e}")
+    assert e_net <= 1e-2, e_net
+
 @pytest.mark.parametrize("C", [32, 8, 24])
 def test_head_backward_vs_fp64(C):
     """raft_unet_head backward: dh[p][c] = bf16(g[p] * w[c]) bit for bit (one
