@@ -167,18 +167,10 @@ __global__ void __launch_bounds__(512) fst_sino_kernel(const FstArgs p)
 template <int NL>
 static void launch_fst(const FstArgs &f, int nslices, int threads, size_t sm, cudaStream_t st)
 {
-    // the shared-memory limit is raised once per device (and again for a larger request)
-    static thread_local int configured_dev = -1;
-    static thread_local size_t configured_sm = 0;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_dev != dev || sm > configured_sm) {
-        RAFT_CUDA(cudaFuncSetAttribute(fst_rows_kernel<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        RAFT_CUDA(cudaFuncSetAttribute(fst_cols_kernel<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        RAFT_CUDA(cudaFuncSetAttribute(fst_sino_kernel<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        configured_dev = dev;
-        configured_sm = sm;
-    }
+    // set on every launch (a few microseconds per iteration)
+    RAFT_CUDA(cudaFuncSetAttribute(fst_rows_kernel<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    RAFT_CUDA(cudaFuncSetAttribute(fst_cols_kernel<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    RAFT_CUDA(cudaFuncSetAttribute(fst_sino_kernel<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     fst_rows_kernel<NL><<<dim3(f.N, nslices), threads, sm, st>>>(f);
     RAFT_CUDA(cudaGetLastError());
     count_launch();
