@@ -167,7 +167,10 @@ __global__ void __launch_bounds__(512) fst_sino_kernel(const FstArgs p)
 template <int NL>
 static void launch_fst(const FstArgs &f, int nslices, int threads, size_t sm, cudaStream_t st)
 {
-    // set on every launch (a few microseconds per iteration)
+    // Set on every launch (a few microseconds per iteration): the limit belongs
+    // to the kernel, shared by all host threads, and sm varies with L, so a
+    // thread's memory of the last value it set can be undercut by another
+    // thread setting a smaller one (the slab split runs one thread per entry).
     RAFT_CUDA(cudaFuncSetAttribute(fst_rows_kernel<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     RAFT_CUDA(cudaFuncSetAttribute(fst_cols_kernel<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     RAFT_CUDA(cudaFuncSetAttribute(fst_sino_kernel<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
