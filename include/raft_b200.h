@@ -299,6 +299,12 @@ int raft_unet_input(const float *img, const float *scale, void *x, int N, int H,
  * the packed input's other channels are zero), 32 BF16 output channels, NHWC. */
 int raft_unet_input_conv(const float *img, const float *scale, const void *w, int Cin, const float *bias, void *y,
                          int N, int H, int W, void *stream);
+/* First layer's gradients in training, from the one-channel input: dw[co][tap][0]
+ * (dw is [32][3][3][Cin]; the other channels are left as they are) and db[co] from
+ * dpre [N][H][W][32] BF16 (the ReLU-masked output gradient); work holds N*H*320
+ * floats of per-row partial sums, reduced in a fixed order. */
+int raft_unet_input_wgrad(const float *img, const float *scale, const void *dpre, float *dw, int Cin, float *db,
+                          float *work, size_t work_floats, int N, int H, int W, void *stream);
 int raft_unet_head(int backward, const void *h, const float *w, const float *b, const float *img,
                    const float *scale, float *out_or_grad, void *dh, float *dw, float *db, int N, int HW,
                    int C, void *stream);

@@ -530,6 +530,67 @@ __global__ void __launch_bounds__(256) input_conv_kernel(const float *__restrict
     }
 }
 
+// The first layer's weight and bias gradients in training, from the image
+// itself: only channel 0 of its input carries data, so
+//   dw[co][tap][0] = sum_p dpre[p][co] x[p + tap],   db[co] = sum_p dpre[p][co]
+// with x = bf16(img x scale) (zero outside the image).  Pass 1: one CTA per
+// image row, 320 threads = 288 (tap, channel) sums + 32 bias sums over the
+// row's pixels, staged in shared memory; partial sums [row][320].  Pass 2:
+// one CTA per output, the rows' partials summed in a fixed order, so the
+// result does not depend on scheduling.
+__global__ void __launch_bounds__(320) input_wgrad_rows_kernel(const float *__restrict__ img,
+                                                               const float *__restrict__ scale,
+                                                               const bf16 *__restrict__ dpre, float *__restrict__ part,
+                                                               int H, int W)
+{
+    extern __shared__ __align__(16) unsigned char smem_iw[];
+    bf16 *ds = reinterpret_cast<bf16 *>(smem_iw);                          // [W][32]
+    float *xs = reinterpret_cast<float *>(smem_iw + (size_t)W * 64);      // [3][W + 2]
+    const int y = blockIdx.x, n = blockIdx.y, W2 = W + 2;
+    const float sc = scale[n];
+    const uint4 *src = reinterpret_cast<const uint4 *>(dpre + ((size_t)n * H + y) * W * 32);
+    uint4 *dst = reinterpret_cast<uint4 *>(ds);
+    for (int i = threadIdx.x; i < W * 4; i += blockDim.x) dst[i] = src[i];
+    for (int i = threadIdx.x; i < 3 * W2; i += blockDim.x) {
+        const int r = i / W2, c = i - r * W2, gy = y + r - 1, gx = c - 1;
+        float v = 0.f;
+        if (gy >= 0 && gy < H && gx >= 0 && gx < W)
+            v = __bfloat162float(__float2bfloat16(img[((size_t)n * H + gy) * W + gx] * sc));
+        xs[i] = v;
+    }
+    __syncthreads();
+    const int t = threadIdx.x, co = t & 31;
+    float acc = 0.f;
+    if (t < 288) {
+        const int tap = t >> 5, ky = tap / 3, kx = tap - 3 * ky;
+        const float *xr = xs + ky * W2 + kx;
+        for (int px = 0; px < W; px++) acc = fmaf(__bfloat162float(ds[px * 32 + co]), xr[px], acc);
+    } else {
+        for (int px = 0; px < W; px++) acc += __bfloat162float(ds[px * 32 + co]);
+    }
+    part[((size_t)n * H + y) * 320 + t] = acc;
+}
+
+__global__ void __launch_bounds__(256) input_wgrad_reduce_kernel(const float *__restrict__ part, int nrows,
+                                                                 float *__restrict__ dw, int Cin,
+                                                                 float *__restrict__ db)
+{
+    __shared__ float red[256];
+    const int t = blockIdx.x;   // output: (tap, channel) t < 288, bias t - 288
+    float s = 0.f;
+    for (int r = threadIdx.x; r < nrows; r += blockDim.x) s += part[(size_t)r * 320 + t];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (t < 288) dw[((size_t)(t & 31) * 9 + (t >> 5)) * Cin] = red[0];
+        else db[t - 288] = red[0];
+    }
+}
+
 // head, one thread per pixel with 16-byte channel loads (C <= 64, weights in shared memory)
 __global__ void head_fwd_v8_kernel(const bf16 *h, const float *w, const float *b, const float *img,
                                    const float *scale, float *out, int N, int HW, int C)
@@ -891,6 +952,25 @@ int raft_unet_input_conv(const float *img, const float *scale, const void *w, in
     const dim3 grid((W + 31) / 32, (H + 7) / 8, N);
     input_conv_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(img, scale, (const bf16 *)w, bias, (bf16 *)y, H, W,
                                                               Cin);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+int raft_unet_input_wgrad(const float *img, const float *scale, const void *dpre, float *dw, int Cin, float *db,
+                          float *work, size_t work_floats, int N, int H, int W, void *stream)
+{
+    const size_t rows = (size_t)N * H, smem = (size_t)W * 64 + (size_t)3 * (W + 2) * sizeof(float);
+    if (N <= 0 || H <= 0 || W <= 0 || Cin < 1 || work_floats < rows * 320 || smem > 200 * 1024 ||
+        ((uintptr_t)dpre % 16) != 0)
+        return 1;
+    // set at every call: the size depends on W
+    if (cudaFuncSetAttribute(input_wgrad_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return 1;
+    count_launch();
+    input_wgrad_rows_kernel<<<dim3(H, N), 320, smem, (cudaStream_t)stream>>>(img, scale, (const bf16 *)dpre, work, H,
+                                                                          W);
+    count_launch();
+    input_wgrad_reduce_kernel<<<320, 256, 0, (cudaStream_t)stream>>>(work, (int)rows, dw, Cin, db);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 

@@ -31,6 +31,7 @@ libraft.raft_unet_pool.argtypes = [_I, _P, _P, _I, _I, _I, _I, _P]
 libraft.raft_unet_upsample.argtypes = [_I, _P, _P, _I, _I, _I, _I, _P]
 libraft.raft_unet_input.argtypes = [_P, _P, _P, _I, _I, _I, _I, _P]
 libraft.raft_unet_input_conv.argtypes = [_P, _P, _P, _I, _P, _P, _I, _I, _I, _P]
+libraft.raft_unet_input_wgrad.argtypes = [_P, _P, _P, _P, _I, _P, _P, _Z, _I, _I, _I, _P]
 libraft.raft_unet_head.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _P]
 libraft.raft_unet_mse.argtypes = [_P, _P, _P, _P, _P, _I, _I, _P]
 libraft.raft_unet_adam.argtypes = [_P, _P, _P, _P, _P, _Z, _F, _F, _F, _F, _I, _P]
@@ -41,7 +42,8 @@ libraft.raft_unet_set_conv_halo.argtypes = [_I]
 libraft.raft_unet_set_wgrad_nine.argtypes = [_I]
 libraft.raft_unet_conv_error.argtypes = []
 for _f in ("raft_unet_set_conv_path", "raft_unet_set_conv_halo", "raft_unet_set_wgrad_nine", "raft_unet_conv_error", "raft_unet_conv_fwd", "raft_unet_conv_wgrad", "raft_unet_flip_weights", "raft_unet_relu_bwd",
-           "raft_unet_pool", "raft_unet_upsample", "raft_unet_input", "raft_unet_input_conv", "raft_unet_head",
+           "raft_unet_pool", "raft_unet_upsample", "raft_unet_input", "raft_unet_input_conv", "raft_unet_input_wgrad",
+           "raft_unet_head",
            "raft_unet_mse",
            "raft_unet_adam", "raft_unet_add", "raft_unet_to_bf16"):
     getattr(libraft, _f).restype = _I
@@ -123,17 +125,11 @@ class UNet:
         H, W must be multiples of 8."""
         torch = self.torch
         N, H, W = img.shape
-        if keep:
-            # training: the first layer's weight gradient needs the packed input
-            x = torch.empty((N, H, W, 32), dtype=torch.bfloat16, device=self.dev)
-            _ok(libraft.raft_unet_input(_p(img), _p(scale), _p(x), N, H, W, 32, self._st()), "input")
-            A = {"x": x}
-            A["e0a"] = self._conv("e0a", x, None, N, H, W)
-        else:
-            # inference: the first layer straight from the one-channel image
-            A = {"e0a": torch.empty((N, H, W, 32), dtype=torch.bfloat16, device=self.dev)}
-            _ok(libraft.raft_unet_input_conv(_p(img), _p(scale), _p(self.wb["e0a"]), 32, _p(self.b["e0a"]),
-                                             _p(A["e0a"]), N, H, W, self._st()), "input_conv")
+        # the first layer straight from the one-channel image (bit-identical to
+        # convolving a packed 32-channel input whose other channels are zero)
+        A = {"e0a": torch.empty((N, H, W, 32), dtype=torch.bfloat16, device=self.dev)}
+        _ok(libraft.raft_unet_input_conv(_p(img), _p(scale), _p(self.wb["e0a"]), 32, _p(self.b["e0a"]),
+                                         _p(A["e0a"]), N, H, W, self._st()), "input_conv")
         A["s0"] = self._conv("e0b", A["e0a"], None, N, H, W)
         A["p0"] = self._pool(A["s0"], N, H, W, 32)
         h1, w1 = H // 2, W // 2
@@ -226,7 +222,12 @@ class UNet:
         g, _ = self._conv_bwd("e1a", A["p0"], None, A["e1a"], g, N, h1, w1)
         g = self._add(self._poolb(g, N, H, W, 32), g_s0)
         g, _ = self._conv_bwd("e0b", A["e0a"], None, A["s0"], g, N, H, W)
-        self._conv_bwd("e0a", A["x"], None, A["e0a"], g, N, H, W, need_dx=False)
+        # first layer: weight (channel 0) and bias gradients from the image itself
+        dpre = torch.empty_like(g)
+        _ok(libraft.raft_unet_relu_bwd(_p(A["e0a"]), _p(g), _p(dpre), g.numel(), st), "relu_bwd")
+        work = torch.empty(N * H * 320, dtype=torch.float32, device=self.dev)
+        _ok(libraft.raft_unet_input_wgrad(_p(img), _p(scale), _p(dpre), _p(self.gw["e0a"]), 32, _p(self.gb["e0a"]),
+                                          _p(work), work.numel(), N, H, W, st), "wgrad e0a")
 
     def adam_step(self, lr, b1=0.9, b2=0.999, eps=1e-8):
         self.step_count += 1
