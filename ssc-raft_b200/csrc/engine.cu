@@ -718,11 +718,17 @@ void em_chunk(DeviceState &ds, const EmPrepared &ep, int kind, const float *d_da
     pl.flat = d_flat;
     pl.data = d_data;
     pl.wt = wt;
-    pl.windowed = 1;
+    // the projector writes the window rows interleaved by slice, as the
+    // four-slice backprojector stages them: no separate interleave pass per
+    // iteration (margins and slices past the batch stay zero from this clear)
+    pl.windowed = 2;
+    pl.out = static_cast<float *>(bl.il_ws);
+    RAFT_CUDA(cudaMemsetAsync(bl.il_ws, 0, bp_il_bytes(nslices, A, win.Wg, 4), st));
     pl.wlo = win.wlo;
     pl.Wg = win.Wg;
     bl.img = d_obj;
     bl.den = den;
+    bl.il_ready = 1;
     if (d_metrics)
         RAFT_CUDA(cudaMemsetAsync(d_metrics, 0, sizeof(double) * 3 * nslices * (size_t)c.niter, st));
 

@@ -226,7 +226,13 @@ __device__ __forceinline__ void project_block(const ProjLaunch &p, const int bx,
         }
         if (p.windowed) {
             const float w = p.wt ? p.wt[j] : 1.f;
-            p.out[((size_t)k * p.nangles + j) * p.Wg + (i - p.wlo)] = out * w;
+            const size_t e = (size_t)(i - p.wlo);
+            // 2: rows interleaved by slice in groups of four, the layout the
+            // four-slice backprojector stages (the four phase lanes of a ray
+            // write the four floats of one 16-byte element)
+            const size_t o = p.windowed == 2 ? ((((size_t)(k >> 2) * p.nangles + j) * p.Wg + e) << 2) + (k & 3)
+                                             : ((size_t)k * p.nangles + j) * p.Wg + e;
+            p.out[o] = out * w;
         } else {
             p.out[vox] = out;
         }

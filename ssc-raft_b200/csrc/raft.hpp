@@ -216,7 +216,7 @@ struct ProjLaunch {
     const float *flat = nullptr;    // tEM: [nslices][nrays]
     const float *data = nullptr;    // tEM counts / eEM tomogram [nslices][nangles][nrays]
     const float *wt = nullptr;      // per-angle weight applied when writing window rows
-    int windowed = 0, wlo = 0, Wg = 0;
+    int windowed = 0, wlo = 0, Wg = 0;   // windowed: 1 rows [slice][angle][Wg], 2 [slice/4][angle][Wg][4]
     double *metrics = nullptr;      // optional FP64 sums [nslices][3]
 };
 
